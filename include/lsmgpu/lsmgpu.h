@@ -1,0 +1,361 @@
+/*
+ * lsmgpu.h -- C ABI of the B200 level-set toolbox library (liblsmgpu.so).
+ *
+ * Part 1 declares drop-in replacements for the Fortran-77 routines of the
+ * LSMLIB 3D toolbox.  Each keeps the reference's symbol (lower-case Fortran
+ * name with a trailing underscore, as the reference's header macros expand
+ * them) and its argument list: every argument by pointer, each array followed
+ * by the six bounds of its ghost box (ilo, ihi, jlo, jhi, klo, khi), then the
+ * fill box, then the grid spacing and scalars.  Arrays are column-major with
+ * i fastest.  LSMLIB_REAL is double (the reference's default FP64 build).
+ *
+ * Semantics beyond the reference:
+ *  - array arguments may be device (cudaMalloc / managed) pointers, used in
+ *    place on the calling thread's stream (lsmgpu_set_stream), or host
+ *    pointers, staged through device buffers; a call with a staged array or a
+ *    host scalar output (dt, max_norm_diff) returns after the work finishes;
+ *    calls on device arrays return immediately unless lsmgpu_set_sync(1);
+ *  - scalar inputs (dx, dt, cfl_number, box bounds) are host pointers;
+ *  - scratch arrays (D1, D2, D3) are accepted and never touched: the
+ *    undivided differences are formed on the fly in registers;
+ *  - boxes are validated before launch; an invalid call computes nothing and
+ *    records an error readable with lsmgpu_get_last_error().
+ *
+ * Part 2 is the extension API (prefix lsmgpu_): error and stream control,
+ * device memory helpers, fused TVD Runge-Kutta stages, FP32 storage, batched
+ * grids and the discrete adjoint.
+ */
+#ifndef LSMGPU_H
+#define LSMGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* every declaration below is exported from liblsmgpu.so */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifndef LSMLIB_REAL
+#define LSMLIB_REAL double
+#endif
+
+/* six ghost-box (or fill-box) bound pointers */
+#define LSMGPU_BOX6(p)                                                     \
+  const int *ilo_##p, const int *ihi_##p, const int *jlo_##p,              \
+      const int *jhi_##p, const int *klo_##p, const int *khi_##p
+
+/* ======================================================================== */
+/* Part 1 -- reference-compatible routines                                   */
+/* ======================================================================== */
+
+/* ---- spatial derivatives: src/toolbox/spatial_derivatives/
+ *      lsm_spatial_derivatives3d.h ---------------------------------------- */
+
+/* replaces LSM3D_HJ_ENO1, lsm_spatial_derivatives3d.h:83 */
+void lsm3dhjeno1_(LSMLIB_REAL *phi_x_plus, LSMLIB_REAL *phi_y_plus,
+                  LSMLIB_REAL *phi_z_plus, LSMGPU_BOX6(grad_phi_plus_gb),
+                  LSMLIB_REAL *phi_x_minus, LSMLIB_REAL *phi_y_minus,
+                  LSMLIB_REAL *phi_z_minus, LSMGPU_BOX6(grad_phi_minus_gb),
+                  const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb), LSMLIB_REAL *D1,
+                  LSMGPU_BOX6(D1_gb), LSMGPU_BOX6(fb), const LSMLIB_REAL *dx,
+                  const LSMLIB_REAL *dy, const LSMLIB_REAL *dz);
+/* replaces LSM3D_HJ_ENO2, lsm_spatial_derivatives3d.h:159 */
+void lsm3dhjeno2_(LSMLIB_REAL *phi_x_plus, LSMLIB_REAL *phi_y_plus,
+                  LSMLIB_REAL *phi_z_plus, LSMGPU_BOX6(grad_phi_plus_gb),
+                  LSMLIB_REAL *phi_x_minus, LSMLIB_REAL *phi_y_minus,
+                  LSMLIB_REAL *phi_z_minus, LSMGPU_BOX6(grad_phi_minus_gb),
+                  const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb), LSMLIB_REAL *D1,
+                  LSMGPU_BOX6(D1_gb), LSMLIB_REAL *D2, LSMGPU_BOX6(D2_gb),
+                  LSMGPU_BOX6(fb), const LSMLIB_REAL *dx,
+                  const LSMLIB_REAL *dy, const LSMLIB_REAL *dz);
+/* replaces LSM3D_HJ_ENO3, lsm_spatial_derivatives3d.h:243 */
+void lsm3dhjeno3_(LSMLIB_REAL *phi_x_plus, LSMLIB_REAL *phi_y_plus,
+                  LSMLIB_REAL *phi_z_plus, LSMGPU_BOX6(grad_phi_plus_gb),
+                  LSMLIB_REAL *phi_x_minus, LSMLIB_REAL *phi_y_minus,
+                  LSMLIB_REAL *phi_z_minus, LSMGPU_BOX6(grad_phi_minus_gb),
+                  const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb), LSMLIB_REAL *D1,
+                  LSMGPU_BOX6(D1_gb), LSMLIB_REAL *D2, LSMGPU_BOX6(D2_gb),
+                  LSMLIB_REAL *D3, LSMGPU_BOX6(D3_gb), LSMGPU_BOX6(fb),
+                  const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+                  const LSMLIB_REAL *dz);
+/* replaces LSM3D_HJ_WENO5, lsm_spatial_derivatives3d.h:332 */
+void lsm3dhjweno5_(LSMLIB_REAL *phi_x_plus, LSMLIB_REAL *phi_y_plus,
+                   LSMLIB_REAL *phi_z_plus, LSMGPU_BOX6(grad_phi_plus_gb),
+                   LSMLIB_REAL *phi_x_minus, LSMLIB_REAL *phi_y_minus,
+                   LSMLIB_REAL *phi_z_minus, LSMGPU_BOX6(grad_phi_minus_gb),
+                   const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb),
+                   LSMLIB_REAL *D1, LSMGPU_BOX6(D1_gb), LSMGPU_BOX6(fb),
+                   const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+                   const LSMLIB_REAL *dz);
+/* replaces LSM3D_UPWIND_HJ_ENO1, lsm_spatial_derivatives3d.h:395 */
+void lsm3dupwindhjeno1_(LSMLIB_REAL *phi_x, LSMLIB_REAL *phi_y,
+                        LSMLIB_REAL *phi_z, LSMGPU_BOX6(grad_phi_gb),
+                        const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb),
+                        const LSMLIB_REAL *vel_x, const LSMLIB_REAL *vel_y,
+                        const LSMLIB_REAL *vel_z, LSMGPU_BOX6(vel_gb),
+                        LSMLIB_REAL *D1, LSMGPU_BOX6(D1_gb), LSMGPU_BOX6(fb),
+                        const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+                        const LSMLIB_REAL *dz);
+/* replaces LSM3D_UPWIND_HJ_ENO2, lsm_spatial_derivatives3d.h:459 */
+void lsm3dupwindhjeno2_(LSMLIB_REAL *phi_x, LSMLIB_REAL *phi_y,
+                        LSMLIB_REAL *phi_z, LSMGPU_BOX6(grad_phi_gb),
+                        const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb),
+                        const LSMLIB_REAL *vel_x, const LSMLIB_REAL *vel_y,
+                        const LSMLIB_REAL *vel_z, LSMGPU_BOX6(vel_gb),
+                        LSMLIB_REAL *D1, LSMGPU_BOX6(D1_gb), LSMLIB_REAL *D2,
+                        LSMGPU_BOX6(D2_gb), LSMGPU_BOX6(fb),
+                        const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+                        const LSMLIB_REAL *dz);
+/* replaces LSM3D_UPWIND_HJ_ENO3, lsm_spatial_derivatives3d.h:531 */
+void lsm3dupwindhjeno3_(LSMLIB_REAL *phi_x, LSMLIB_REAL *phi_y,
+                        LSMLIB_REAL *phi_z, LSMGPU_BOX6(grad_phi_gb),
+                        const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb),
+                        const LSMLIB_REAL *vel_x, const LSMLIB_REAL *vel_y,
+                        const LSMLIB_REAL *vel_z, LSMGPU_BOX6(vel_gb),
+                        LSMLIB_REAL *D1, LSMGPU_BOX6(D1_gb), LSMLIB_REAL *D2,
+                        LSMGPU_BOX6(D2_gb), LSMLIB_REAL *D3,
+                        LSMGPU_BOX6(D3_gb), LSMGPU_BOX6(fb),
+                        const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+                        const LSMLIB_REAL *dz);
+/* replaces LSM3D_UPWIND_HJ_WENO5, lsm_spatial_derivatives3d.h:608 */
+void lsm3dupwindhjweno5_(LSMLIB_REAL *phi_x, LSMLIB_REAL *phi_y,
+                         LSMLIB_REAL *phi_z, LSMGPU_BOX6(grad_phi_gb),
+                         const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb),
+                         const LSMLIB_REAL *vel_x, const LSMLIB_REAL *vel_y,
+                         const LSMLIB_REAL *vel_z, LSMGPU_BOX6(vel_gb),
+                         LSMLIB_REAL *D1, LSMGPU_BOX6(D1_gb), LSMGPU_BOX6(fb),
+                         const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+                         const LSMLIB_REAL *dz);
+
+/* ---- level set equation RHS: src/toolbox/level_set_evolution/
+ *      lsm_level_set_evolution3d.h ---------------------------------------- */
+
+/* replaces LSM3D_ZERO_OUT_LEVEL_SET_EQN_RHS, lsm_level_set_evolution3d.h:64 */
+void lsm3dzerooutlevelseteqnrhs_(LSMLIB_REAL *lse_rhs,
+                                 LSMGPU_BOX6(lse_rhs_gb));
+/* replaces LSM3D_ADD_ADVECTION_TERM_TO_LSE_RHS,
+ * lsm_level_set_evolution3d.h:94 */
+void lsm3daddadvectiontermtolserhs_(
+    LSMLIB_REAL *lse_rhs, LSMGPU_BOX6(lse_rhs_gb), const LSMLIB_REAL *phi_x,
+    const LSMLIB_REAL *phi_y, const LSMLIB_REAL *phi_z,
+    LSMGPU_BOX6(grad_phi_gb), const LSMLIB_REAL *vel_x,
+    const LSMLIB_REAL *vel_y, const LSMLIB_REAL *vel_z, LSMGPU_BOX6(vel_gb),
+    LSMGPU_BOX6(fb));
+/* replaces LSM3D_ADD_NORMAL_VEL_TERM_TO_LSE_RHS,
+ * lsm_level_set_evolution3d.h:151 */
+void lsm3daddnormalveltermtolserhs_(
+    LSMLIB_REAL *lse_rhs, LSMGPU_BOX6(lse_rhs_gb),
+    const LSMLIB_REAL *phi_x_plus, const LSMLIB_REAL *phi_y_plus,
+    const LSMLIB_REAL *phi_z_plus, LSMGPU_BOX6(grad_phi_plus_gb),
+    const LSMLIB_REAL *phi_x_minus, const LSMLIB_REAL *phi_y_minus,
+    const LSMLIB_REAL *phi_z_minus, LSMGPU_BOX6(grad_phi_minus_gb),
+    const LSMLIB_REAL *vel_n, LSMGPU_BOX6(vel_gb), LSMGPU_BOX6(fb));
+/* replaces LSM3D_ADD_CONST_NORMAL_VEL_TERM_TO_LSE_RHS,
+ * lsm_level_set_evolution3d.h:217 */
+void lsm3daddconstnormalveltermtolserhs_(
+    LSMLIB_REAL *lse_rhs, LSMGPU_BOX6(lse_rhs_gb),
+    const LSMLIB_REAL *phi_x_plus, const LSMLIB_REAL *phi_y_plus,
+    const LSMLIB_REAL *phi_z_plus, LSMGPU_BOX6(grad_phi_plus_gb),
+    const LSMLIB_REAL *phi_x_minus, const LSMLIB_REAL *phi_y_minus,
+    const LSMLIB_REAL *phi_z_minus, LSMGPU_BOX6(grad_phi_minus_gb),
+    const LSMLIB_REAL *vel_n, LSMGPU_BOX6(fb));
+
+/* ---- reinitialization: src/toolbox/reinitialization/
+ *      lsm_reinitialization3d.h:77 ----------------------------------------- */
+void lsm3dcomputereinitializationeqnrhs_(
+    LSMLIB_REAL *reinit_rhs, LSMGPU_BOX6(rhs_gb), const LSMLIB_REAL *phi,
+    LSMGPU_BOX6(phi_gb), const LSMLIB_REAL *phi0, LSMGPU_BOX6(phi0_gb),
+    const LSMLIB_REAL *phi_x_plus, const LSMLIB_REAL *phi_y_plus,
+    const LSMLIB_REAL *phi_z_plus, LSMGPU_BOX6(grad_phi_plus_gb),
+    const LSMLIB_REAL *phi_x_minus, const LSMLIB_REAL *phi_y_minus,
+    const LSMLIB_REAL *phi_z_minus, LSMGPU_BOX6(grad_phi_minus_gb),
+    LSMGPU_BOX6(fb), const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+    const LSMLIB_REAL *dz, const int *use_phi0_for_sgn);
+
+/* ---- field extension: src/toolbox/field_extension/
+ *      lsm_field_extension3d.h:65 ------------------------------------------ */
+void lsm3dcomputefieldextensioneqnrhs_(
+    LSMLIB_REAL *rhs, LSMGPU_BOX6(rhs_gb), const LSMLIB_REAL *S,
+    LSMGPU_BOX6(S_gb), const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb),
+    const LSMLIB_REAL *S_x_upwind, const LSMLIB_REAL *S_y_upwind,
+    const LSMLIB_REAL *S_z_upwind, LSMGPU_BOX6(grad_S_upwind_gb),
+    const LSMLIB_REAL *signed_normal_x, const LSMLIB_REAL *signed_normal_y,
+    const LSMLIB_REAL *signed_normal_z, LSMGPU_BOX6(signed_normal_gb),
+    LSMGPU_BOX6(fb), const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+    const LSMLIB_REAL *dz);
+
+/* ---- signed unit normal (supplies the extension "velocity"):
+ *      src/toolbox/geometry/lsm_geometry3d.h:127 --------------------------- */
+void lsm3dcomputesignedunitnormal_(
+    LSMLIB_REAL *normal_x, LSMLIB_REAL *normal_y, LSMLIB_REAL *normal_z,
+    LSMGPU_BOX6(normal_gb), const LSMLIB_REAL *phi_x,
+    const LSMLIB_REAL *phi_y, const LSMLIB_REAL *phi_z,
+    LSMGPU_BOX6(grad_phi_gb), const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb),
+    LSMGPU_BOX6(fb), const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+    const LSMLIB_REAL *dz);
+
+/* ---- TVD Runge-Kutta: src/toolbox/time_integration/
+ *      lsm_tvd_runge_kutta3d.h ----------------------------------------------- */
+
+/* replaces LSM3D_RK1_STEP, lsm_tvd_runge_kutta3d.h:59 */
+void lsm3drk1step_(LSMLIB_REAL *u_next, LSMGPU_BOX6(u_next_gb),
+                   const LSMLIB_REAL *u_cur, LSMGPU_BOX6(u_cur_gb),
+                   const LSMLIB_REAL *rhs, LSMGPU_BOX6(rhs_gb),
+                   LSMGPU_BOX6(fb), const LSMLIB_REAL *dt);
+/* replaces LSM3D_TVD_RK2_STAGE1, lsm_tvd_runge_kutta3d.h:108 */
+void lsm3dtvdrk2stage1_(LSMLIB_REAL *u_stage1, LSMGPU_BOX6(u_stage1_gb),
+                        const LSMLIB_REAL *u_cur, LSMGPU_BOX6(u_cur_gb),
+                        const LSMLIB_REAL *rhs, LSMGPU_BOX6(rhs_gb),
+                        LSMGPU_BOX6(fb), const LSMLIB_REAL *dt);
+/* replaces LSM3D_TVD_RK2_STAGE2, lsm_tvd_runge_kutta3d.h:154 */
+void lsm3dtvdrk2stage2_(LSMLIB_REAL *u_next, LSMGPU_BOX6(u_next_gb),
+                        const LSMLIB_REAL *u_stage1, LSMGPU_BOX6(u_stage1_gb),
+                        const LSMLIB_REAL *u_cur, LSMGPU_BOX6(u_cur_gb),
+                        const LSMLIB_REAL *rhs, LSMGPU_BOX6(rhs_gb),
+                        LSMGPU_BOX6(fb), const LSMLIB_REAL *dt);
+/* replaces LSM3D_TVD_RK3_STAGE1, lsm_tvd_runge_kutta3d.h:210 */
+void lsm3dtvdrk3stage1_(LSMLIB_REAL *u_stage1, LSMGPU_BOX6(u_stage1_gb),
+                        const LSMLIB_REAL *u_cur, LSMGPU_BOX6(u_cur_gb),
+                        const LSMLIB_REAL *rhs, LSMGPU_BOX6(rhs_gb),
+                        LSMGPU_BOX6(fb), const LSMLIB_REAL *dt);
+/* replaces LSM3D_TVD_RK3_STAGE2, lsm_tvd_runge_kutta3d.h:256 */
+void lsm3dtvdrk3stage2_(LSMLIB_REAL *u_stage2, LSMGPU_BOX6(u_stage2_gb),
+                        const LSMLIB_REAL *u_stage1, LSMGPU_BOX6(u_stage1_gb),
+                        const LSMLIB_REAL *u_cur, LSMGPU_BOX6(u_cur_gb),
+                        const LSMLIB_REAL *rhs, LSMGPU_BOX6(rhs_gb),
+                        LSMGPU_BOX6(fb), const LSMLIB_REAL *dt);
+/* replaces LSM3D_TVD_RK3_STAGE3, lsm_tvd_runge_kutta3d.h:309 */
+void lsm3dtvdrk3stage3_(LSMLIB_REAL *u_next, LSMGPU_BOX6(u_next_gb),
+                        const LSMLIB_REAL *u_stage2, LSMGPU_BOX6(u_stage2_gb),
+                        const LSMLIB_REAL *u_cur, LSMGPU_BOX6(u_cur_gb),
+                        const LSMLIB_REAL *rhs, LSMGPU_BOX6(rhs_gb),
+                        LSMGPU_BOX6(fb), const LSMLIB_REAL *dt);
+
+/* ---- utilities: src/toolbox/utilities/lsm_utilities3d.h ------------------ */
+
+/* replaces LSM3D_MAX_NORM_DIFF, lsm_utilities3d.h:87 */
+void lsm3dmaxnormdiff_(LSMLIB_REAL *max_norm_diff, const LSMLIB_REAL *field1,
+                       LSMGPU_BOX6(field1_gb), const LSMLIB_REAL *field2,
+                       LSMGPU_BOX6(field2_gb), LSMGPU_BOX6(ib));
+/* replaces LSM3D_COMPUTE_STABLE_ADVECTION_DT, lsm_utilities3d.h:221 */
+void lsm3dcomputestableadvectiondt_(
+    LSMLIB_REAL *dt, const LSMLIB_REAL *vel_x, const LSMLIB_REAL *vel_y,
+    const LSMLIB_REAL *vel_z, LSMGPU_BOX6(vel_gb), LSMGPU_BOX6(ib),
+    const LSMLIB_REAL *dx, const LSMLIB_REAL *dy, const LSMLIB_REAL *dz,
+    const LSMLIB_REAL *cfl_number);
+/* replaces LSM3D_COMPUTE_STABLE_NORMAL_VEL_DT, lsm_utilities3d.h:268 */
+void lsm3dcomputestablenormalveldt_(
+    LSMLIB_REAL *dt, const LSMLIB_REAL *vel_n, LSMGPU_BOX6(vel_gb),
+    const LSMLIB_REAL *phi_x_plus, const LSMLIB_REAL *phi_y_plus,
+    const LSMLIB_REAL *phi_z_plus, LSMGPU_BOX6(grad_phi_plus_gb),
+    const LSMLIB_REAL *phi_x_minus, const LSMLIB_REAL *phi_y_minus,
+    const LSMLIB_REAL *phi_z_minus, LSMGPU_BOX6(grad_phi_minus_gb),
+    LSMGPU_BOX6(ib), const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+    const LSMLIB_REAL *dz, const LSMLIB_REAL *cfl_number);
+/* replaces LSM3D_COMPUTE_STABLE_CONST_NORMAL_VEL_DT, lsm_utilities3d.h:331 */
+void lsm3dcomputestableconstnormalveldt_(
+    LSMLIB_REAL *dt, const LSMLIB_REAL *vel_n, const LSMLIB_REAL *phi_x_plus,
+    const LSMLIB_REAL *phi_y_plus, const LSMLIB_REAL *phi_z_plus,
+    LSMGPU_BOX6(grad_phi_plus_gb), const LSMLIB_REAL *phi_x_minus,
+    const LSMLIB_REAL *phi_y_minus, const LSMLIB_REAL *phi_z_minus,
+    LSMGPU_BOX6(grad_phi_minus_gb), LSMGPU_BOX6(ib), const LSMLIB_REAL *dx,
+    const LSMLIB_REAL *dy, const LSMLIB_REAL *dz,
+    const LSMLIB_REAL *cfl_number);
+
+/* ---- boundary conditions: src/toolbox/boundary_conditions/
+ *      lsm_boundary_conditions3d.h; bdry_location_idx 0..5 = x-lo, x-hi,
+ *      y-lo, y-hi, z-lo, z-hi -------------------------------------------- */
+
+/* replaces LSM3D_LINEAR_EXTRAPOLATION, lsm_boundary_conditions3d.h:71 */
+void lsm3dlinearextrapolation_(LSMLIB_REAL *phi, LSMGPU_BOX6(gb),
+                               LSMGPU_BOX6(fb), const int *bdry_location_idx);
+/* replaces LSM3D_COPY_EXTRAPOLATION, lsm_boundary_conditions3d.h:135 */
+void lsm3dcopyextrapolation_(LSMLIB_REAL *phi, LSMGPU_BOX6(gb),
+                             LSMGPU_BOX6(fb), const int *bdry_location_idx);
+/* replaces LSM3D_HOMOGENEOUS_NEUMANN_ENO1, lsm_boundary_conditions3d.h:161 */
+void lsm3dhomogeneousneumanneno1_(LSMLIB_REAL *phi, LSMGPU_BOX6(gb),
+                                  LSMGPU_BOX6(fb),
+                                  const int *bdry_location_idx);
+/* replaces LSM3D_HOMOGENEOUS_NEUMANN_ENO2, lsm_boundary_conditions3d.h:186 */
+void lsm3dhomogeneousneumanneno2_(LSMLIB_REAL *phi, LSMGPU_BOX6(gb),
+                                  LSMGPU_BOX6(fb),
+                                  const int *bdry_location_idx);
+/* replaces LSM3D_HOMOGENEOUS_NEUMANN_ENO3, lsm_boundary_conditions3d.h:211 */
+void lsm3dhomogeneousneumanneno3_(LSMLIB_REAL *phi, LSMGPU_BOX6(gb),
+                                  LSMGPU_BOX6(fb),
+                                  const int *bdry_location_idx);
+/* replaces LSM3D_HOMOGENEOUS_NEUMANN_WENO5, lsm_boundary_conditions3d.h:236 */
+void lsm3dhomogeneousneumannweno5_(LSMLIB_REAL *phi, LSMGPU_BOX6(gb),
+                                   LSMGPU_BOX6(fb),
+                                   const int *bdry_location_idx);
+
+/* ======================================================================== */
+/* Part 2 -- extension API                                                   */
+/* ======================================================================== */
+
+/* status codes (lsmgpu_get_last_error) */
+enum {
+  LSMGPU_SUCCESS = 0,
+  LSMGPU_ERR_INVALID_BOX = 1,   /* box arguments would read/write outside */
+  LSMGPU_ERR_NULL_POINTER = 2,
+  LSMGPU_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+  LSMGPU_ERR_ALLOC = 4,         /* device allocation failed */
+  LSMGPU_ERR_INVALID_VALUE = 5, /* a scalar argument is out of range */
+  LSMGPU_ERR_DEVICE = 6         /* a kernel reported a bad state */
+};
+
+/* floating-point modes of the fused kernels (lsmgpu_set_fp_mode) */
+enum {
+  LSMGPU_FP_STRICT = 0, /* reference expression order, no FMA: bit-exact */
+  LSMGPU_FP_FAST = 1    /* FMA and a restructured WENO5 (<= 1e-12 rel.) */
+};
+
+/* returns the calling thread's last error code and clears it */
+int lsmgpu_get_last_error(void);
+/* last error code without clearing it */
+int lsmgpu_peek_last_error(void);
+/* message of the last error ("" when none); valid until the next call */
+const char *lsmgpu_get_last_error_string(void);
+
+/* stream used by the calling thread's subsequent calls (cudaStream_t; NULL =
+ * the legacy default stream) */
+int lsmgpu_set_stream(void *cuda_stream);
+void *lsmgpu_get_stream(void);
+/* 1: every reference-compatible call waits for its work (the reference's
+ * blocking behaviour); 0 (default): calls on device arrays are asynchronous */
+int lsmgpu_set_sync(int on);
+int lsmgpu_set_fp_mode(int mode);
+int lsmgpu_get_fp_mode(void);
+/* waits for the calling thread's stream */
+int lsmgpu_stream_synchronize(void);
+/* number of kernels this library has launched in this process */
+unsigned long long lsmgpu_kernel_launch_count(void);
+
+/* device memory and copies (on the calling thread's stream) */
+void *lsmgpu_malloc(size_t bytes);
+int lsmgpu_free(void *p);
+void *lsmgpu_host_alloc(size_t bytes); /* page-locked host memory */
+int lsmgpu_host_free(void *p);
+int lsmgpu_memcpy_htod(void *dst, const void *src, size_t bytes);
+int lsmgpu_memcpy_dtoh(void *dst, const void *src, size_t bytes);
+int lsmgpu_memcpy_dtod(void *dst, const void *src, size_t bytes);
+
+/* CUDA events on the calling thread's stream, for timing */
+void *lsmgpu_event_create(void);
+int lsmgpu_event_record(void *ev);
+int lsmgpu_event_elapsed_ms(void *start, void *stop, float *ms);
+int lsmgpu_event_destroy(void *ev);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LSMGPU_H */

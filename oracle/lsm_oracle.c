@@ -20,8 +20,9 @@
  * contract; this restatement computes the differences on the fly and leaves
  * the scratch arrays untouched.  The values it uses are the same doubles:
  *   D1(p) = phi(p) - phi(p-s)            (odd order: face p-1/2, sign +1)
- *   D2(p) = -(D1(p) - D1(p+s)) = D1(p+s) - D1(p)   (even order, sign -1;
- *           exact because round-to-nearest is symmetric under negation)
+ *   D2(p) = -(D1(p) - D1(p+s))           (even order, sign -1; the
+ *           negation is kept: it makes an exact zero -0.0, as the reference's
+ *           multiplication by -1.0 does)
  *   D3(p) = D2(p) - D2(p-s)
  * with s the element stride of the direction.
  *
@@ -73,7 +74,7 @@ static inline real D1at(const real *q, long s, long m) {
   return q[m * s] - q[(m - 1) * s];
 }
 static inline real D2at(const real *q, long s, long m) {
-  return D1at(q, s, m + 1) - D1at(q, s, m);
+  return -(D1at(q, s, m) - D1at(q, s, m + 1));
 }
 static inline real D3at(const real *q, long s, long m) {
   return D2at(q, s, m) - D2at(q, s, m - 1);
