@@ -350,6 +350,82 @@ int lsmgpu_event_record(void *ev);
 int lsmgpu_event_elapsed_ms(void *start, void *stop, float *ms);
 int lsmgpu_event_destroy(void *ev);
 
+/* ---- fused TVD Runge-Kutta stages ------------------------------------------
+ * Arrays are device arrays sharing one ghost box gb[6] = {ilo, ihi, jlo, jhi,
+ * klo, khi}; fb[6] is the fill box (cells updated); dx[3] the spacing.
+ * ``precision`` is 8 (double arrays) or 4 (float arrays, FP32 storage; the CFL
+ * reduction and t/dt stay FP64).  All calls are asynchronous on the calling
+ * thread's stream unless lsmgpu_set_sync(1); the arithmetic mode is
+ * lsmgpu_set_fp_mode's.  Return LSMGPU_SUCCESS or an error code. */
+
+/* stage kinds */
+enum {
+  LSMGPU_STAGE_ADVECT = 0, /* aux0..2 = vel_x,y,z: upwind WENO5, -V.grad phi */
+  LSMGPU_STAGE_NORMAL = 1, /* aux0 = F: WENO5 +-, Godunov, -F |grad phi| */
+  LSMGPU_STAGE_REINIT = 2  /* reinitialization RHS; aux0 = phi0 if use_phi0 */
+};
+/* Runge-Kutta combinations (rk_kind): 1 = u + dt L (RK1 / any stage 1),
+ * 22 = TVD-RK2 stage 2, 32 = TVD-RK3 stage 2, 33 = TVD-RK3 stage 3 */
+
+/* One fused stage: out = RK(rk_kind, phi_n, phi_s, dt * L(phi_s)) on fb.
+ * Faces whose bit is set in bc_mask (bit f for face f = x-lo, x-hi, y-lo,
+ * y-hi, z-lo, z-hi) read linear-extrapolation ghost values of phi_s computed
+ * on the fly from the domain box dom[6] (NULL: dom = fb); other faces read the
+ * ghost cells stored in phi_s.  dt_dev (device, double) overrides dt. */
+int lsmgpu_lse_stage(int kind, int precision, void *out, const void *phi_s,
+                     const void *phi_n, const void *aux0, const void *aux1,
+                     const void *aux2, const int gb[6], const int fb[6],
+                     const int dom[6], unsigned bc_mask, const double dx[3],
+                     const double *dt_dev, double dt, int rk_kind,
+                     int use_phi0);
+
+/* Linear-extrapolation ghost fill of all six faces, in the reference's face
+ * order (its serial driver's "all faces" case). */
+int lsmgpu_fill_ghosts_linear(void *phi, int precision, const int gb[6],
+                              const int fb[6]);
+
+/* A workspace owns the stage buffers, device dt/t and CFL scratch of one
+ * grid (ghost box gb) for the multi-step drivers below. */
+typedef struct lsmgpu_workspace lsmgpu_workspace;
+int lsmgpu_workspace_create(lsmgpu_workspace **ws, const int gb[6],
+                            int precision);
+int lsmgpu_workspace_destroy(lsmgpu_workspace *ws);
+/* faces using on-the-fly linear extrapolation (the drivers need 0x3f) */
+int lsmgpu_workspace_set_bc(lsmgpu_workspace *ws, unsigned linear_faces_mask);
+int lsmgpu_workspace_set_time(lsmgpu_workspace *ws, double t);
+/* waits for the stream; t and the dt of the last step */
+int lsmgpu_workspace_get_time(lsmgpu_workspace *ws, double *t,
+                              double *dt_last);
+/* device address of the workspace scalars {dt, t, dt_last} (doubles) */
+const double *lsmgpu_workspace_device_scalars(lsmgpu_workspace *ws);
+
+/* nsteps TVD-RK3 steps of phi (in place) under the velocity arrays vx, vy,
+ * vz; dt = dt_fixed when > 0, else the LSM3D_COMPUTE_STABLE_ADVECTION_DT dt
+ * of every step (clipped so that t does not pass t_end when t_end > 0). */
+int lsmgpu_advect_tvdrk3(lsmgpu_workspace *ws, void *phi, const void *vx,
+                         const void *vy, const void *vz, const int fb[6],
+                         const double dx[3], double cfl, double dt_fixed,
+                         double t_end, int nsteps);
+/* nsteps TVD-RK3 steps under LeVeque's deformation field with period
+ * ``period`` (velocity at t, t+dt, t+dt/2 for the three stages), CFL dt each
+ * step, clipped at t_end; cell centres at x_lo + (i + 1/2) dx. */
+int lsmgpu_deformation_tvdrk3(lsmgpu_workspace *ws, void *phi, const int fb[6],
+                              const double dx[3], const double x_lo[3],
+                              double period, double cfl, double t_end,
+                              int nsteps);
+/* nsteps TVD-RK3 steps of phi_t + F|grad phi| = 0 (F a device array), CFL dt
+ * of LSM3D_COMPUTE_STABLE_NORMAL_VEL_DT each step; after every
+ * reinit_interval-th step (steps counted from step0) reinit_iters TVD-RK3
+ * reinitialization pseudo-steps with dt = cfl * min(dx). */
+int lsmgpu_normal_tvdrk3(lsmgpu_workspace *ws, void *phi, const void *F,
+                         const int fb[6], const double dx[3], double cfl,
+                         int nsteps, int step0, int reinit_interval,
+                         int reinit_iters, int use_phi0_for_sgn);
+/* iters TVD-RK3 reinitialization pseudo-steps of phi (in place) */
+int lsmgpu_reinit_tvdrk3(lsmgpu_workspace *ws, void *phi, const int fb[6],
+                         const double dx[3], double cfl, int iters,
+                         int use_phi0_for_sgn);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -52,7 +52,7 @@ struct Grid3 {
 };
 
 template <typename T>
-__host__ inline Grid3<T> make_grid(T* p, const Box& b) {
+__host__ __device__ inline Grid3<T> make_grid(T* p, const Box& b) {
   Grid3<T> g;
   g.sy = b.sy();
   g.sz = b.sz();

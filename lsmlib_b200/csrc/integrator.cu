@@ -1,0 +1,604 @@
+// integrator.cu -- fused TVD-RK3 time stepping (extension API, Part 2 of
+// include/lsmgpu/lsmgpu.h).
+//
+// A workspace owns the stage buffers of one grid (phi^(1), phi^(2), the stage
+// RHS, phi0 for the reinitialization sign, velocity buffers, device scalars
+// dt and t, and the CFL partial maxima).  The drivers reproduce the call
+// order of the reference's integrators
+//   LevelSetFunctionIntegrator::advanceLevelSetEqnUsingTVDRK3
+//     (LevelSetFunctionIntegrator.cc:1319-1510; dt from computeStableDt,
+//     :345-587; reinitialization every interval steps, :658-697)
+//   ReinitializationAlgorithm::reinitializeLevelSetFunctions
+//     (ReinitializationAlgorithm.cc:177-330; dt = cfl * min dx, :216)
+// with one fused kernel per Runge-Kutta stage.  dt and t live on the device,
+// so a whole run is launched without a host synchronisation.
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "capi_common.h"
+#include "launch.h"
+#include "stage.cuh"
+#include "stage_launch.h"
+
+using namespace lsmgpu;
+
+struct lsmgpu_workspace {
+  Box gb;
+  int prec;
+  size_t bytes;
+  void* phi1 = nullptr;
+  void* phi2 = nullptr;
+  void* rhs = nullptr;
+  void* phi0 = nullptr;
+  void* vel[3] = {nullptr, nullptr, nullptr};
+  double* scal = nullptr;   // [0] dt, [1] t, [2] dt of the last step
+  double* partials = nullptr;
+  int npart = 0;
+  unsigned bc_mask = 0x3fu;
+  unsigned long long steps = 0;
+};
+
+namespace {
+
+enum { kDt = 0, kT = 1, kDtLast = 2, kNumScal = 4 };
+
+__device__ __forceinline__ double gmax(double m, double v) { return v > m ? v : m; }
+
+// dt = cfl / (max + tiny) (lsm_utilities3d.f.in:322, :445), optionally
+// clipped so that t + dt does not pass t_end
+__global__ void k_dt_finish(const double* partials, int np, double cfl,
+                            double tiny, double* scal, double t_end) {
+  __shared__ double red[8];
+  double m = -1.0;
+  for (int t = threadIdx.x; t < np; t += blockDim.x) m = gmax(m, partials[t]);
+  for (int o = 16; o > 0; o >>= 1) m = gmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = gmax(m, red[w]);
+    m = gmax(red[0], m);
+    double dt = cfl / (m + tiny);
+    if (t_end > 0.0 && scal[kT] + dt > t_end) dt = t_end - scal[kT];
+    scal[kDt] = dt;
+  }
+}
+
+__global__ void k_set_dt(double* scal, double dt) { scal[kDt] = dt; }
+__global__ void k_advance_t(double* scal) {
+  scal[kT] = scal[kT] + scal[kDt];
+  scal[kDtLast] = scal[kDt];
+}
+
+// LeVeque's 3D deformation field at time t + c*dt, g(t) = cos(pi t / period):
+// u = 2 sin^2(pi x) sin(2 pi y) sin(2 pi z) g, v = -sin(2 pi x) sin^2(pi y)
+// sin(2 pi z) g, w = -sin(2 pi x) sin(2 pi y) sin^2(pi z) g, cell centres
+// x_i = x_lo + (i + 1/2) dx.
+template <typename T>
+__global__ void k_deformation(T* vx, T* vy, T* vz, Box gb, FillBox fb,
+                              double x0, double y0, double z0, double dx,
+                              double dy, double dz, const double* scal,
+                              double c, double period) {
+  const int i = fb.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = fb.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > fb.hi[0] || j > fb.hi[1]) return;
+  const double t = scal[kT] + c * scal[kDt];
+  const double g = cos(M_PI * t / period);
+  const double x = x0 + (i + 0.5) * dx, y = y0 + (j + 0.5) * dy;
+  const double sx = sin(M_PI * x), s2x = sin(2.0 * M_PI * x);
+  const double sy = sin(M_PI * y), s2y = sin(2.0 * M_PI * y);
+  for (int k = fb.lo[2] + blockIdx.z; k <= fb.hi[2]; k += gridDim.z) {
+    const double z = z0 + (k + 0.5) * dz;
+    const double sz = sin(M_PI * z), s2z = sin(2.0 * M_PI * z);
+    const long o = (long)(i - gb.lo[0]) + gb.sy() * (j - gb.lo[1]) +
+                   gb.sz() * (k - gb.lo[2]);
+    vx[o] = (T)(2.0 * sx * sx * s2y * s2z * g);
+    vy[o] = (T)(-s2x * sy * sy * s2z * g);
+    vz[o] = (T)(-s2x * s2y * sz * sz * g);
+  }
+}
+
+// the CFL reduction of the deformation field at time t (FP64)
+template <typename T>
+__global__ void k_adv_partials(const T* vx, const T* vy, const T* vz, Box gb,
+                               FillBox fb, double ix, double iy, double iz,
+                               double* partials) {
+  double m = -1.0;
+  const long n = fb.count();
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+       t += (long)gridDim.x * blockDim.x) {
+    const int i = fb.lo[0] + (int)(t % fb.n(0));
+    const long r = t / fb.n(0);
+    const int j = fb.lo[1] + (int)(r % fb.n(1));
+    const int k = fb.lo[2] + (int)(r / fb.n(1));
+    const long o = (long)(i - gb.lo[0]) + gb.sy() * (j - gb.lo[1]) +
+                   gb.sz() * (k - gb.lo[2]);
+    const double u = fabs((double)vx[o]) * ix + fabs((double)vy[o]) * iy +
+                     fabs((double)vz[o]) * iz;
+    m = gmax(m, u);
+  }
+  __shared__ double red[8];
+  for (int o = 16; o > 0; o >>= 1) m = gmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = gmax(m, red[w]);
+    partials[blockIdx.x] = gmax(red[0], m);
+  }
+}
+
+constexpr int kAdvRedBlocks = 1184;
+
+bool ws_ok(lsmgpu_workspace* ws, const char* R) {
+  if (!ws) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null workspace");
+    return false;
+  }
+  return true;
+}
+
+bool fb_in(const Box& gb, const FillBox& fb, int w, const char* R) {
+  return covers(gb, fb, w, "phi", R);
+}
+
+void* ws_alloc(size_t bytes, const char* R) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(LSMGPU_ERR_ALLOC, std::string(R) + ": cudaMalloc failed");
+    return nullptr;
+  }
+  return p;
+}
+
+cudaError_t stage(int kind, int prec, const StageArgs& a, cudaStream_t st) {
+  return fp_mode() == LSMGPU_FP_FAST ? launch_stage_fast(kind, prec, a, st)
+                                     : launch_stage_strict(kind, prec, a, st);
+}
+
+StageArgs base_args(lsmgpu_workspace* ws, const FillBox& fb, const double dx[3]) {
+  StageArgs a;
+  memset(&a, 0, sizeof a);
+  a.gb = ws->gb;
+  a.fb = fb;
+  a.dom = fb;
+  a.bc_mask = ws->bc_mask;
+  for (int d = 0; d < 3; d++) a.inv[d] = 1.0 / dx[d];
+  double m = dx[0] > dx[1] ? dx[0] : dx[1];
+  m = m > dx[2] ? m : dx[2];
+  a.dx_sq = m * m;
+  a.dt_dev = ws->scal + kDt;
+  a.fp64_kinks = ws->prec == 4 ? 1 : 0;
+  return a;
+}
+
+// One TVD-RK3 reinitialization pseudo-step of phi (in place) with dt = dtr.
+bool reinit_step(lsmgpu_workspace* ws, void* phi, const FillBox& fb,
+                 const double dx[3], double dtr, int use0, cudaStream_t st,
+                 const char* R) {
+  StageArgs a = base_args(ws, fb, dx);
+  a.dt_dev = nullptr;
+  a.dt = dtr;
+  a.use_phi0 = use0;
+  a.aux[0] = ws->phi0;
+  a.out = ws->phi1; a.phi_s = phi; a.phi_n = phi; a.rk_kind = 1;
+  if (!cuda_ok(stage(kStageReinit, ws->prec, a, st), R)) return false;
+  a.out = ws->phi2; a.phi_s = ws->phi1; a.rk_kind = 32;
+  if (!cuda_ok(stage(kStageReinit, ws->prec, a, st), R)) return false;
+  a.out = phi; a.phi_s = ws->phi2; a.rk_kind = 33;
+  return cuda_ok(stage(kStageReinit, ws->prec, a, st), R);
+}
+
+bool reinit_run(lsmgpu_workspace* ws, void* phi, const FillBox& fb,
+                const double dx[3], double cfl, int iters, int use0,
+                cudaStream_t st, const char* R) {
+  if (iters <= 0) return true;
+  if (use0 == 1) {
+    if (!ws->phi0 && !(ws->phi0 = ws_alloc(ws->bytes, R))) return false;
+    if (!cuda_ok(cudaMemcpyAsync(ws->phi0, phi, ws->bytes,
+                                 cudaMemcpyDeviceToDevice, st),
+                 R))
+      return false;
+  }
+  // ReinitializationAlgorithm.cc:211-216: dt = cfl * min(dx)
+  double mn = dx[0] < dx[1] ? dx[0] : dx[1];
+  mn = mn < dx[2] ? mn : dx[2];
+  const double dtr = cfl * mn;
+  for (int it = 0; it < iters; it++)
+    if (!reinit_step(ws, phi, fb, dx, dtr, use0, st, R)) return false;
+  return true;
+}
+
+FillBox fb6(const int* f) {
+  FillBox b;
+  b.lo[0] = f[0]; b.hi[0] = f[1];
+  b.lo[1] = f[2]; b.hi[1] = f[3];
+  b.lo[2] = f[4]; b.hi[2] = f[5];
+  return b;
+}
+
+bool common_checks(lsmgpu_workspace* ws, const void* phi, const int* fb,
+                   const double* dx, const char* R, FillBox* out) {
+  clear_error();
+  if (!ws_ok(ws, R)) return false;
+  if (!phi || !fb || !dx) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null argument");
+    return false;
+  }
+  *out = fb6(fb);
+  if (out->n(0) < 2 || out->n(1) < 2 || out->n(2) < 2) {
+    set_error(LSMGPU_ERR_INVALID_BOX,
+              std::string(R) + ": the fill box needs two cells per axis");
+    return false;
+  }
+  if (!fb_in(ws->gb, *out, 3, R)) return false;
+  if (!(dx[0] > 0 && dx[1] > 0 && dx[2] > 0)) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": dx must be positive");
+    return false;
+  }
+  if (ws->bc_mask != 0x3fu) {
+    set_error(LSMGPU_ERR_INVALID_VALUE,
+              std::string(R) + ": multi-step drivers need the linear "
+                               "extrapolation on all six faces");
+    return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lsmgpu_workspace_create(lsmgpu_workspace** out, const int gb[6],
+                            int precision) {
+  const char* R = "lsmgpu_workspace_create";
+  clear_error();
+  if (!out || !gb) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null argument");
+    return LSMGPU_ERR_NULL_POINTER;
+  }
+  *out = nullptr;
+  if (precision != 8 && precision != 4) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": precision is 8 or 4");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  lsmgpu_workspace* ws = new lsmgpu_workspace();
+  ws->gb = box_from(&gb[0], &gb[1], &gb[2], &gb[3], &gb[4], &gb[5]);
+  if (!box_valid(ws->gb, "phi", R)) {
+    delete ws;
+    return LSMGPU_ERR_INVALID_BOX;
+  }
+  ws->prec = precision;
+  ws->bytes = (size_t)ws->gb.count() * (size_t)precision;
+  ws->npart = kAdvRedBlocks;
+  FillBox whole;
+  for (int d = 0; d < 3; d++) { whole.lo[d] = ws->gb.lo[d]; whole.hi[d] = ws->gb.hi(d); }
+  if (stage_blocks(whole) > ws->npart) ws->npart = stage_blocks(whole);
+  if (!(ws->phi1 = ws_alloc(ws->bytes, R)) || !(ws->phi2 = ws_alloc(ws->bytes, R)) ||
+      !(ws->rhs = ws_alloc(ws->bytes, R)) ||
+      !(ws->scal = (double*)ws_alloc(sizeof(double) * kNumScal, R)) ||
+      !(ws->partials = (double*)ws_alloc(sizeof(double) * ws->npart, R))) {
+    lsmgpu_workspace_destroy(ws);
+    return LSMGPU_ERR_ALLOC;
+  }
+  cudaMemset(ws->scal, 0, sizeof(double) * kNumScal);
+  // the stage buffers are only ever read inside the fill box, but start them
+  // from zero so that no uninitialised memory is ever read by a caller
+  cudaMemset(ws->phi1, 0, ws->bytes);
+  cudaMemset(ws->phi2, 0, ws->bytes);
+  cudaMemset(ws->rhs, 0, ws->bytes);
+  if (!cuda_ok(cudaDeviceSynchronize(), R)) {
+    lsmgpu_workspace_destroy(ws);
+    return LSMGPU_ERR_CUDA;
+  }
+  *out = ws;
+  return LSMGPU_SUCCESS;
+}
+
+int lsmgpu_workspace_destroy(lsmgpu_workspace* ws) {
+  if (!ws) return LSMGPU_SUCCESS;
+  void* ps[] = {ws->phi1, ws->phi2, ws->rhs, ws->phi0, ws->vel[0], ws->vel[1],
+                ws->vel[2], ws->scal, ws->partials};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  delete ws;
+  return LSMGPU_SUCCESS;
+}
+
+int lsmgpu_workspace_set_bc(lsmgpu_workspace* ws, unsigned linear_faces_mask) {
+  if (!ws_ok(ws, "lsmgpu_workspace_set_bc")) return LSMGPU_ERR_NULL_POINTER;
+  ws->bc_mask = linear_faces_mask & 0x3fu;
+  return LSMGPU_SUCCESS;
+}
+
+int lsmgpu_workspace_set_time(lsmgpu_workspace* ws, double t) {
+  if (!ws_ok(ws, "lsmgpu_workspace_set_time")) return LSMGPU_ERR_NULL_POINTER;
+  double v[2] = {0.0, t};
+  return cuda_ok(cudaMemcpy(ws->scal, v, sizeof v, cudaMemcpyHostToDevice),
+                 "lsmgpu_workspace_set_time")
+             ? LSMGPU_SUCCESS
+             : LSMGPU_ERR_CUDA;
+}
+
+// host copy of t and of the dt of the last step (waits for the stream)
+int lsmgpu_workspace_get_time(lsmgpu_workspace* ws, double* t, double* dt_last) {
+  if (!ws_ok(ws, "lsmgpu_workspace_get_time")) return LSMGPU_ERR_NULL_POINTER;
+  double v[kNumScal];
+  cudaStream_t st = cur_stream();
+  if (!cuda_ok(cudaMemcpyAsync(v, ws->scal, sizeof v, cudaMemcpyDeviceToHost, st),
+               "lsmgpu_workspace_get_time") ||
+      !cuda_ok(cudaStreamSynchronize(st), "lsmgpu_workspace_get_time"))
+    return LSMGPU_ERR_CUDA;
+  if (t) *t = v[kT];
+  if (dt_last) *dt_last = v[kDtLast];
+  return LSMGPU_SUCCESS;
+}
+
+const double* lsmgpu_workspace_device_scalars(lsmgpu_workspace* ws) {
+  return ws ? ws->scal : nullptr;
+}
+
+// One fused stage on caller-owned device arrays (all with ghost box gb).
+int lsmgpu_lse_stage(int kind, int precision, void* out, const void* phi_s,
+                     const void* phi_n, const void* aux0, const void* aux1,
+                     const void* aux2, const int gb[6], const int fb[6],
+                     const int dom[6], unsigned bc_mask, const double dx[3],
+                     const double* dt_dev, double dt, int rk_kind,
+                     int use_phi0) {
+  const char* R = "lsmgpu_lse_stage";
+  clear_error();
+  if (!out || !phi_s || !gb || !fb || !dx || (rk_kind != 1 && !phi_n) ||
+      (kind == kStageAdvect && (!aux0 || !aux1 || !aux2)) ||
+      (kind == kStageNormal && !aux0) ||
+      (kind == kStageReinit && use_phi0 == 1 && !aux0)) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null argument");
+    return LSMGPU_ERR_NULL_POINTER;
+  }
+  if (kind < kStageAdvect || kind > kStageReinit || (precision != 8 && precision != 4) ||
+      (rk_kind != 1 && rk_kind != 22 && rk_kind != 32 && rk_kind != 33)) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": bad kind/precision/rk");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  const Box g = box_from(&gb[0], &gb[1], &gb[2], &gb[3], &gb[4], &gb[5]);
+  const FillBox f = fb6(fb);
+  if (f.n(0) < 1 || f.n(1) < 1 || f.n(2) < 1) return LSMGPU_SUCCESS;
+  if (!box_valid(g, "phi", R) || !covers(g, f, 3, "phi", R))
+    return LSMGPU_ERR_INVALID_BOX;
+  StageArgs a;
+  memset(&a, 0, sizeof a);
+  a.gb = g;
+  a.fb = f;
+  a.bc_mask = bc_mask & 0x3fu;
+  a.dom = dom ? fb6(dom) : f;
+  if (a.bc_mask) {
+    for (int d = 0; d < 3; d++)
+      if (a.dom.lo[d] > f.lo[d] || a.dom.hi[d] < f.hi[d] ||
+          a.dom.hi[d] - a.dom.lo[d] < 1 || a.dom.lo[d] < g.lo[d] ||
+          a.dom.hi[d] > g.hi(d)) {
+        set_error(LSMGPU_ERR_INVALID_BOX,
+                  std::string(R) + ": domain box must contain the fill box, "
+                                   "lie in the ghost box and span 2 cells");
+        return LSMGPU_ERR_INVALID_BOX;
+      }
+  }
+  a.out = out; a.phi_s = phi_s; a.phi_n = phi_n;
+  a.aux[0] = aux0; a.aux[1] = aux1; a.aux[2] = aux2;
+  for (int d = 0; d < 3; d++) a.inv[d] = 1.0 / dx[d];
+  double m = dx[0] > dx[1] ? dx[0] : dx[1];
+  m = m > dx[2] ? m : dx[2];
+  a.dx_sq = m * m;
+  a.dt_dev = dt_dev;
+  a.dt = dt;
+  a.rk_kind = rk_kind;
+  a.use_phi0 = use_phi0;
+  a.fp64_kinks = precision == 4;
+  cudaStream_t st = cur_stream();
+  if (!cuda_ok(stage(kind, precision, a, st), R)) return LSMGPU_ERR_CUDA;
+  if (sync_mode() && !cuda_ok(cudaStreamSynchronize(st), R)) return LSMGPU_ERR_CUDA;
+  return LSMGPU_SUCCESS;
+}
+
+// Linear-extrapolation ghost fill of all six faces in the reference's order
+// (lsm_boundary_conditions.c:227-293, case 9).
+int lsmgpu_fill_ghosts_linear(void* phi, int precision, const int gb[6],
+                              const int fb[6]) {
+  const char* R = "lsmgpu_fill_ghosts_linear";
+  clear_error();
+  if (!phi || !gb || !fb) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null argument");
+    return LSMGPU_ERR_NULL_POINTER;
+  }
+  const Box g = box_from(&gb[0], &gb[1], &gb[2], &gb[3], &gb[4], &gb[5]);
+  const FillBox f = fb6(fb);
+  if (!box_valid(g, "phi", R) || !covers(g, f, 0, "phi", R)) return LSMGPU_ERR_INVALID_BOX;
+  if (f.n(0) < 2 || f.n(1) < 2 || f.n(2) < 2) {
+    set_error(LSMGPU_ERR_INVALID_BOX, std::string(R) + ": fill box too thin");
+    return LSMGPU_ERR_INVALID_BOX;
+  }
+  cudaStream_t st = cur_stream();
+  for (int face = 0; face < 6; face++)
+    if (!cuda_ok(launch_bc(precision, 0, phi, g, f, face, st), R)) return LSMGPU_ERR_CUDA;
+  return LSMGPU_SUCCESS;
+}
+
+// TVD-RK3 steps under an external velocity field (device arrays with the
+// workspace ghost box).  dt_fixed > 0: constant dt; otherwise the CFL dt of
+// LSM3D_COMPUTE_STABLE_ADVECTION_DT every step (clipped at t_end > 0).
+int lsmgpu_advect_tvdrk3(lsmgpu_workspace* ws, void* phi, const void* vx,
+                         const void* vy, const void* vz, const int fb[6],
+                         const double dx[3], double cfl, double dt_fixed,
+                         double t_end, int nsteps) {
+  const char* R = "lsmgpu_advect_tvdrk3";
+  FillBox f;
+  if (!common_checks(ws, phi, fb, dx, R, &f)) return lsmgpu_peek_last_error();
+  if (!vx || !vy || !vz) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null velocity");
+    return LSMGPU_ERR_NULL_POINTER;
+  }
+  cudaStream_t st = cur_stream();
+  const void* vel[3] = {vx, vy, vz};
+  const double tiny = ws->prec == 8 ? Consts<double>::tiny : (double)Consts<float>::tiny;
+  for (int s = 0; s < nsteps; s++) {
+    if (dt_fixed > 0) {
+      k_set_dt<<<1, 1, 0, st>>>(ws->scal, dt_fixed);
+    } else {
+      const double inv[3] = {1.0 / dx[0], 1.0 / dx[1], 1.0 / dx[2]};
+      if (ws->prec == 8)
+        k_adv_partials<double><<<kAdvRedBlocks, 256, 0, st>>>(
+            (const double*)vx, (const double*)vy, (const double*)vz, ws->gb, f,
+            inv[0], inv[1], inv[2], ws->partials);
+      else
+        k_adv_partials<float><<<kAdvRedBlocks, 256, 0, st>>>(
+            (const float*)vx, (const float*)vy, (const float*)vz, ws->gb, f,
+            inv[0], inv[1], inv[2], ws->partials);
+      ++launch_counter();
+      k_dt_finish<<<1, 256, 0, st>>>(ws->partials, kAdvRedBlocks, cfl, tiny,
+                                     ws->scal, t_end);
+    }
+    ++launch_counter();
+    StageArgs a = base_args(ws, f, dx);
+    for (int d = 0; d < 3; d++) a.aux[d] = vel[d];
+    a.out = ws->phi1; a.phi_s = phi; a.phi_n = phi; a.rk_kind = 1;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    a.out = ws->phi2; a.phi_s = ws->phi1; a.rk_kind = 32;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    a.out = phi; a.phi_s = ws->phi2; a.rk_kind = 33;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    k_advance_t<<<1, 1, 0, st>>>(ws->scal);
+    ++launch_counter();
+    ws->steps++;
+  }
+  if (!cuda_ok(cudaGetLastError(), R)) return LSMGPU_ERR_CUDA;
+  if (sync_mode() && !cuda_ok(cudaStreamSynchronize(st), R)) return LSMGPU_ERR_CUDA;
+  return LSMGPU_SUCCESS;
+}
+
+// TVD-RK3 steps under the deformation field of LeVeque (period ``period``),
+// velocity re-evaluated at t, t+dt, t+dt/2 for the three stages
+// (LevelSetFunctionIntegrator.cc:1332, :1404, :1476); CFL dt every step from
+// the velocity at t, clipped at t_end.  x_lo is the lower corner of the
+// domain; cell centres sit at x_lo + (i + 1/2) dx.
+int lsmgpu_deformation_tvdrk3(lsmgpu_workspace* ws, void* phi, const int fb[6],
+                              const double dx[3], const double x_lo[3],
+                              double period, double cfl, double t_end,
+                              int nsteps) {
+  const char* R = "lsmgpu_deformation_tvdrk3";
+  FillBox f;
+  if (!common_checks(ws, phi, fb, dx, R, &f)) return lsmgpu_peek_last_error();
+  if (!x_lo || !(period > 0)) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": bad x_lo/period");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  for (int d = 0; d < 3; d++)
+    if (!ws->vel[d] && !(ws->vel[d] = ws_alloc(ws->bytes, R))) return LSMGPU_ERR_ALLOC;
+  cudaStream_t st = cur_stream();
+  const double tiny = ws->prec == 8 ? Consts<double>::tiny : (double)Consts<float>::tiny;
+  const double inv[3] = {1.0 / dx[0], 1.0 / dx[1], 1.0 / dx[2]};
+  dim3 vb(32, 4, 1), vg((f.n(0) + 31) / 32, (f.n(1) + 3) / 4,
+                        f.n(2) < 65535 ? f.n(2) : 65535);
+  auto velocity = [&](double c) {
+    if (ws->prec == 8)
+      k_deformation<double><<<vg, vb, 0, st>>>(
+          (double*)ws->vel[0], (double*)ws->vel[1], (double*)ws->vel[2], ws->gb,
+          f, x_lo[0], x_lo[1], x_lo[2], dx[0], dx[1], dx[2], ws->scal, c, period);
+    else
+      k_deformation<float><<<vg, vb, 0, st>>>(
+          (float*)ws->vel[0], (float*)ws->vel[1], (float*)ws->vel[2], ws->gb, f,
+          x_lo[0], x_lo[1], x_lo[2], dx[0], dx[1], dx[2], ws->scal, c, period);
+    ++launch_counter();
+  };
+  for (int s = 0; s < nsteps; s++) {
+    // dt from the velocity at t (the stage-1 field)
+    velocity(0.0);
+    if (ws->prec == 8)
+      k_adv_partials<double><<<kAdvRedBlocks, 256, 0, st>>>(
+          (const double*)ws->vel[0], (const double*)ws->vel[1],
+          (const double*)ws->vel[2], ws->gb, f, inv[0], inv[1], inv[2], ws->partials);
+    else
+      k_adv_partials<float><<<kAdvRedBlocks, 256, 0, st>>>(
+          (const float*)ws->vel[0], (const float*)ws->vel[1],
+          (const float*)ws->vel[2], ws->gb, f, inv[0], inv[1], inv[2], ws->partials);
+    k_dt_finish<<<1, 256, 0, st>>>(ws->partials, kAdvRedBlocks, cfl, tiny, ws->scal,
+                                   t_end);
+    launch_counter() += 2;
+    StageArgs a = base_args(ws, f, dx);
+    for (int d = 0; d < 3; d++) a.aux[d] = ws->vel[d];
+    a.out = ws->phi1; a.phi_s = phi; a.phi_n = phi; a.rk_kind = 1;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    velocity(1.0);
+    a.out = ws->phi2; a.phi_s = ws->phi1; a.rk_kind = 32;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    velocity(0.5);
+    a.out = phi; a.phi_s = ws->phi2; a.rk_kind = 33;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    k_advance_t<<<1, 1, 0, st>>>(ws->scal);
+    ++launch_counter();
+    ws->steps++;
+  }
+  if (!cuda_ok(cudaGetLastError(), R)) return LSMGPU_ERR_CUDA;
+  if (sync_mode() && !cuda_ok(cudaStreamSynchronize(st), R)) return LSMGPU_ERR_CUDA;
+  return LSMGPU_SUCCESS;
+}
+
+// TVD-RK3 steps of phi_t + F |grad phi| = 0 with a normal-speed array F and
+// the CFL dt of LSM3D_COMPUTE_STABLE_NORMAL_VEL_DT every step; after every
+// reinit_interval-th step (counted from step0) reinit_iters reinitialization
+// pseudo-steps.
+int lsmgpu_normal_tvdrk3(lsmgpu_workspace* ws, void* phi, const void* F,
+                         const int fb[6], const double dx[3], double cfl,
+                         int nsteps, int step0, int reinit_interval,
+                         int reinit_iters, int use_phi0_for_sgn) {
+  const char* R = "lsmgpu_normal_tvdrk3";
+  FillBox f;
+  if (!common_checks(ws, phi, fb, dx, R, &f)) return lsmgpu_peek_last_error();
+  if (!F) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null speed");
+    return LSMGPU_ERR_NULL_POINTER;
+  }
+  cudaStream_t st = cur_stream();
+  const double tiny = ws->prec == 8 ? Consts<double>::tiny : (double)Consts<float>::tiny;
+  const int nblk = stage_blocks(f);
+  for (int s = 0; s < nsteps; s++) {
+    StageArgs a = base_args(ws, f, dx);
+    a.aux[0] = F;
+    // WENO5 +- of phi^n once: L(phi^n) for stage 1 and the CFL maxima
+    a.rhs_out = ws->rhs; a.partials = ws->partials; a.phi_s = phi;
+    if (!cuda_ok(stage(kStageNormalRhs, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    k_dt_finish<<<1, 256, 0, st>>>(ws->partials, nblk, cfl, tiny, ws->scal, 0.0);
+    ++launch_counter();
+    // stage 1: phi1 = phi + dt L (LSM3D_TVD_RK3_STAGE1)
+    if (!cuda_ok(launch_rk(ws->prec, 1, ws->phi1, ws->gb, nullptr, ws->gb, phi,
+                           ws->gb, ws->rhs, ws->gb, f, 0.0, ws->scal + kDt, st),
+                 R))
+      return LSMGPU_ERR_CUDA;
+    a.out = ws->phi2; a.phi_s = ws->phi1; a.phi_n = phi; a.rk_kind = 32;
+    if (!cuda_ok(stage(kStageNormal, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    a.out = phi; a.phi_s = ws->phi2; a.rk_kind = 33;
+    if (!cuda_ok(stage(kStageNormal, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    k_advance_t<<<1, 1, 0, st>>>(ws->scal);
+    ++launch_counter();
+    ws->steps++;
+    if (reinit_interval > 0 && (step0 + s + 1) % reinit_interval == 0)
+      if (!reinit_run(ws, phi, f, dx, cfl, reinit_iters, use_phi0_for_sgn, st, R))
+        return lsmgpu_peek_last_error();
+  }
+  if (!cuda_ok(cudaGetLastError(), R)) return LSMGPU_ERR_CUDA;
+  if (sync_mode() && !cuda_ok(cudaStreamSynchronize(st), R)) return LSMGPU_ERR_CUDA;
+  return LSMGPU_SUCCESS;
+}
+
+// reinitialization pseudo-steps alone (ReinitializationAlgorithm.cc:177-330)
+int lsmgpu_reinit_tvdrk3(lsmgpu_workspace* ws, void* phi, const int fb[6],
+                         const double dx[3], double cfl, int iters,
+                         int use_phi0_for_sgn) {
+  const char* R = "lsmgpu_reinit_tvdrk3";
+  FillBox f;
+  if (!common_checks(ws, phi, fb, dx, R, &f)) return lsmgpu_peek_last_error();
+  cudaStream_t st = cur_stream();
+  if (!reinit_run(ws, phi, f, dx, cfl, iters, use_phi0_for_sgn, st, R))
+    return lsmgpu_peek_last_error();
+  if (sync_mode() && !cuda_ok(cudaStreamSynchronize(st), R)) return LSMGPU_ERR_CUDA;
+  return LSMGPU_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,45 @@
+// stage_launch.h -- type-erased arguments of the fused stage kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace lsmgpu {
+
+struct StageArgs {
+  void* out;
+  const void* phi_s;
+  const void* phi_n;
+  const void* aux[3];
+  void* rhs_out;
+  double* partials;
+  Box gb;
+  FillBox fb;
+  FillBox dom;
+  unsigned bc_mask;
+  double inv[3];
+  double dx_sq;
+  const double* dt_dev;
+  double dt;
+  int rk_kind;
+  int use_phi0;
+  int fp64_kinks;
+};
+
+// tile of the stage kernels: TX x TY cells per block, TZ planes per block
+constexpr int kStageTX = 32, kStageTY = 8, kStageTZ = 32;
+
+inline int stage_blocks(const FillBox& fb) {
+  const int gx = (fb.n(0) + kStageTX - 1) / kStageTX;
+  const int gy = (fb.n(1) + kStageTY - 1) / kStageTY;
+  const int gz = (fb.n(2) + kStageTZ - 1) / kStageTZ;
+  return gx * gy * gz;
+}
+
+// kind: StageKind; prec: 8 (FP64) or 4 (FP32)
+cudaError_t launch_stage_strict(int kind, int prec, const StageArgs& a,
+                                cudaStream_t st);
+cudaError_t launch_stage_fast(int kind, int prec, const StageArgs& a,
+                              cudaStream_t st);
+
+}  // namespace lsmgpu

@@ -1,0 +1,92 @@
+// weno_fast.cuh -- HJ-WENO5 restructured for the FP64/FP32 ALU of sm_100a.
+//
+// Same reconstruction as the reference (lsm_spatial_derivatives3d.f.in:
+// 1292-1323) with three changes that alter only rounding:
+//  * FMA contraction (the translation unit is built with --fmad=true);
+//  * the nonlinear weights are normalised with a single reciprocal:
+//      a_k = d_k / q_k^2,  q_k = S_k + eps
+//      w_k = d_k * prod_{j!=k} q_j^2 / sum_m (d_m * prod_{j!=m} q_j^2)
+//    after scaling every q_k by the power of two s = 2^-floor(log2 eps), so
+//    that 1 <= q_k*s < 2^27 and the fourth-degree products stay far inside
+//    the FP32 and FP64 ranges (S_k <= 33.4 max v^2 and eps >= 1e-6 max v^2);
+//  * the reciprocal is the hardware seed (rcp.approx.ftz) refined by
+//    Newton-Raphson steps r <- r + r(1 - d r) (Markstein, IBM J. Res. Dev.
+//    34(1), 1990): two steps in FP64, one in FP32.
+// The parity tests bound the difference to the reference at 1e-12 relative
+// (FP64).
+#pragma once
+#include "common.cuh"
+
+namespace lsmgpu {
+
+__device__ __forceinline__ double rcp_nr(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+}
+__device__ __forceinline__ float rcp_nr(float d) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(d));
+  const float e = fmaf(-d, r, 1.0f);
+  return fmaf(r, e, r);
+}
+
+// 2^-(unbiased exponent of x) for a positive normal x
+__device__ __forceinline__ double inv_pow2_of(double x) {
+  const int e = (__double2hiint(x) >> 20) & 0x7ff;
+  return __hiloint2double((2046 - e) << 20, 0);
+}
+__device__ __forceinline__ float inv_pow2_of(float x) {
+  const int e = (__float_as_int(x) >> 23) & 0xff;
+  return __int_as_float((254 - e) << 23);
+}
+
+// Reconstruction from five scaled differences v1..v5 (reference ordering:
+// minus side v = V(i-2..i+2); plus side v = V(i+3..i-1)).
+template <typename T>
+__device__ __forceinline__ T weno5_fast(T v1, T v2, T v3, T v4, T v5) {
+  const T s1 = v1 * v1, s2 = v2 * v2, s3 = v3 * v3, s4 = v4 * v4, s5 = v5 * v5;
+  const T m = fmax(fmax(fmax(s1, s2), fmax(s3, s4)), s5);
+  const T eps = T(1e-6) * m + Consts<T>::tiny;
+  const T p1 = T(1.0 / 3.0) * v1 - T(7.0 / 6.0) * v2 + T(11.0 / 6.0) * v3;
+  const T p2 = -T(1.0 / 6.0) * v2 + T(5.0 / 6.0) * v3 + T(1.0 / 3.0) * v4;
+  const T p3 = T(1.0 / 3.0) * v3 + T(5.0 / 6.0) * v4 - T(1.0 / 6.0) * v5;
+  T t = v1 - T(2) * v2 + v3, u = v1 - T(4) * v2 + T(3) * v3;
+  const T S1 = T(13.0 / 12.0) * (t * t) + T(0.25) * (u * u);
+  t = v2 - T(2) * v3 + v4;
+  u = v2 - v4;
+  const T S2 = T(13.0 / 12.0) * (t * t) + T(0.25) * (u * u);
+  t = v3 - T(2) * v4 + v5;
+  u = T(3) * v3 - T(4) * v4 + v5;
+  const T S3 = T(13.0 / 12.0) * (t * t) + T(0.25) * (u * u);
+  const T sc = inv_pow2_of(eps);
+  const T es = eps * sc;
+  const T q1 = S1 * sc + es, q2 = S2 * sc + es, q3 = S3 * sc + es;
+  const T Q1 = q1 * q1, Q2 = q2 * q2, Q3 = q3 * q3;
+  const T n1 = T(0.1) * (Q2 * Q3), n2 = T(0.6) * (Q1 * Q3), n3 = T(0.3) * (Q1 * Q2);
+  const T r = rcp_nr(n1 + n2 + n3);
+  return (n1 * p1 + n2 * p2 + n3 * p3) * r;
+}
+
+// True when the smoothness indicators of a stencil differ by more than a
+// factor 1e3, i.e. the stencil straddles a kink.  Used by the FP32 form to
+// recompute such values in FP64.
+template <typename T>
+__device__ __forceinline__ bool weno5_is_kink(T v1, T v2, T v3, T v4, T v5) {
+  T t = v1 - T(2) * v2 + v3, u = v1 - T(4) * v2 + T(3) * v3;
+  const T S1 = T(13.0 / 12.0) * (t * t) + T(0.25) * (u * u);
+  t = v2 - T(2) * v3 + v4;
+  u = v2 - v4;
+  const T S2 = T(13.0 / 12.0) * (t * t) + T(0.25) * (u * u);
+  t = v3 - T(2) * v4 + v5;
+  u = T(3) * v3 - T(4) * v4 + v5;
+  const T S3 = T(13.0 / 12.0) * (t * t) + T(0.25) * (u * u);
+  const T mx = fmax(fmax(S1, S2), S3), mn = fmin(fmin(S1, S2), S3);
+  const T scale = fmax(fmax(fmax(v1 * v1, v2 * v2), fmax(v3 * v3, v4 * v4)), v5 * v5);
+  return mx > T(1e3) * mn + T(1e-4) * scale;
+}
+
+}  // namespace lsmgpu

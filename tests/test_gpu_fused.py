@@ -1,0 +1,226 @@
+"""Fused TVD-RK3 stages and drivers against the oracle's reference-order chain.
+
+Strict mode (reference expression order, no FMA) must be bit-identical to the
+chain ghost fill -> zero RHS -> WENO5 -> RHS term -> TVD-RK3 stage of the
+oracle; fast mode must stay within 1e-12 of it (relative max-norm:
+max|gpu - ref| / max|ref|); the FP32 form within 1e-5 of the FP64 oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from oracle.driver import Grid, Stepper, deformation_velocity
+
+pytestmark = pytest.mark.gpu
+
+REL_FAST = 1e-12
+ABS_FP32 = 1e-5
+
+
+def rel_err(got, want):
+    return float(np.max(np.abs(got - want)) / max(np.max(np.abs(want)), 1e-300))
+
+
+def sphere(g, x_lo, c=(0.1, -0.05, 0.0), r=0.25):
+    x, y, z = g.centers(x_lo)
+    return np.sqrt((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) - r
+
+
+def spheres(g, x_lo, seed, count=6):
+    rng = np.random.default_rng(seed)
+    x, y, z = g.centers(x_lo)
+    phi = np.full(g.shape, np.inf)
+    for _ in range(count):
+        c = rng.uniform(-0.6, 0.6, 3)
+        r = rng.uniform(0.1, 0.3)
+        phi = np.minimum(phi, np.sqrt((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) - r)
+    return phi
+
+
+def same_bits(a, b):
+    return np.array_equal(np.ascontiguousarray(a).view(np.uint64),
+                          np.ascontiguousarray(b).view(np.uint64))
+
+
+@pytest.fixture(params=["strict", "fast"])
+def mode(request):
+    from lsmlib_b200 import integrator
+    prev = integrator.get_fp_mode()
+    integrator.set_fp_mode(integrator.FP_STRICT if request.param == "strict"
+                           else integrator.FP_FAST)
+    yield request.param
+    integrator.set_fp_mode(prev)
+
+
+def check(mode, got, want):
+    if mode == "strict":
+        assert same_bits(got, want), "max diff %g" % np.max(np.abs(got - want))
+    else:
+        assert rel_err(got, want) <= REL_FAST
+
+
+GRIDS = [(37, 11, 35), (16, 16, 16), (64, 9, 33)]
+
+
+@pytest.mark.parametrize("n", GRIDS)
+def test_advect_constant_velocity(mode, n):
+    from lsmlib_b200 import gpu, integrator
+    g = Grid(n, dx=(2.0 / n[0], 2.0 / n[1], 2.0 / n[2]))
+    x_lo = (-1.0, -1.0, -1.0)
+    phi0 = sphere(g, x_lo)
+    vel = [g.field(np.full(g.shape, c)) for c in (1.0, 0.5, -0.25)]
+    st = Stepper(oracle.oracle_toolbox(), g)
+    ref = g.field(phi0)
+    dt = st.advect_dt(vel, 0.5)
+    for _ in range(3):
+        st.advect_step(ref, lambda c: vel, dt)
+    ws = integrator.Workspace(g.gb, 8)
+    d = gpu.DeviceArray.from_host(phi0)
+    dv = [gpu.DeviceArray.from_host(v.data) for v in vel]
+    ws.advect(d, dv, g.fb, g.dx, cfl=0.5, nsteps=3)
+    t, dt_last = ws.time()
+    assert dt_last == dt
+    check(mode, g.interior(g.field(d.download())), g.interior(ref))
+
+
+@pytest.mark.parametrize("n", [(24, 20, 18), (33, 17, 40)])
+def test_advect_random_velocity_field(mode, n):
+    """Velocity with sign changes and exact zeros exercises every upwind
+    branch (zero, backward, forward)."""
+    from lsmlib_b200 import gpu, integrator
+    rng = np.random.default_rng(7)
+    g = Grid(n, dx=(0.05, 0.06, 0.07))
+    phi0 = spheres(g, (-0.6, -0.6, -0.6), seed=3)
+    vel = []
+    for _ in range(3):
+        v = rng.standard_normal(g.shape)
+        v[rng.random(g.shape) < 0.1] = 0.0
+        vel.append(g.field(v))
+    st = Stepper(oracle.oracle_toolbox(), g)
+    ref = g.field(phi0)
+    dt = 0.01
+    for _ in range(2):
+        st.advect_step(ref, lambda c: vel, dt)
+    ws = integrator.Workspace(g.gb, 8)
+    d = gpu.DeviceArray.from_host(phi0)
+    dv = [gpu.DeviceArray.from_host(v.data) for v in vel]
+    ws.advect(d, dv, g.fb, g.dx, dt_fixed=dt, nsteps=2)
+    check(mode, g.interior(g.field(d.download())), g.interior(ref))
+
+
+@pytest.mark.parametrize("n", [(32, 24, 20), (19, 33, 17)])
+def test_normal_velocity_with_reinitialization(mode, n):
+    from lsmlib_b200 import gpu, integrator
+    g = Grid(n, dx=(2.0 / n[0],) * 3)
+    x_lo = (-1.0, -1.0, -1.0)
+    phi0 = spheres(g, x_lo, seed=11)
+    x, y, z = g.centers(x_lo)
+    F = 1.0 + 0.2 * np.sin(4 * np.pi * x) * np.sin(4 * np.pi * y) * np.sin(4 * np.pi * z)
+    Ff = g.field(F)
+    st = Stepper(oracle.oracle_toolbox(), g)
+    ref = g.field(phi0)
+    for s in range(4):
+        st.normal_step(ref, Ff, 0.5)
+        if (s + 1) % 2 == 0:
+            st.reinit(ref, 0.5, 3, use0=0)
+    ws = integrator.Workspace(g.gb, 8)
+    d = gpu.DeviceArray.from_host(phi0)
+    dF = gpu.DeviceArray.from_host(F)
+    ws.normal(d, dF, g.fb, g.dx, cfl=0.5, nsteps=4, reinit_interval=2,
+              reinit_iters=3, use_phi0=0)
+    check(mode, g.interior(g.field(d.download())), g.interior(ref))
+
+
+@pytest.mark.parametrize("use0", [0, 1])
+def test_reinitialization(mode, use0):
+    from lsmlib_b200 import gpu, integrator
+    g = Grid((26, 22, 30), dx=(0.05, 0.05, 0.05))
+    phi0 = 3.0 * spheres(g, (-0.6, -0.6, -0.6), seed=5, count=3)   # not a distance
+    st = Stepper(oracle.oracle_toolbox(), g)
+    ref = g.field(phi0)
+    st.reinit(ref, 0.5, 4, use0=use0)
+    ws = integrator.Workspace(g.gb, 8)
+    d = gpu.DeviceArray.from_host(phi0)
+    ws.reinit(d, g.fb, g.dx, cfl=0.5, iters=4, use_phi0=use0)
+    check(mode, g.interior(g.field(d.download())), g.interior(ref))
+
+
+def test_deformation_field_matches_oracle():
+    """LeVeque's field is evaluated on the device (CUDA sin/cos) and on the
+    host (numpy); the two differ by a few ulps, so the comparison is at the
+    fast-mode tolerance."""
+    from lsmlib_b200 import gpu, integrator
+    n = (40, 40, 40)
+    g = Grid(n, dx=(1.0 / 40,) * 3)
+    x_lo = (0.0, 0.0, 0.0)
+    phi0 = sphere(g, x_lo, c=(0.35, 0.35, 0.35), r=0.15)
+    st = Stepper(oracle.oracle_toolbox(), g)
+    ref = g.field(phi0)
+    t = 0.0
+    for _ in range(3):
+        v0 = deformation_velocity(g, x_lo, t)
+        dt = st.advect_dt(v0, 0.5)
+        st.advect_step(ref, lambda c: deformation_velocity(g, x_lo, t + c * dt), dt)
+        t += dt
+    ws = integrator.Workspace(g.gb, 8)
+    d = gpu.DeviceArray.from_host(phi0)
+    ws.deformation(d, g.fb, g.dx, x_lo, period=3.0, cfl=0.5, t_end=3.0, nsteps=3)
+    tg, _ = ws.time()
+    assert abs(tg - t) <= 1e-12 * t
+    assert rel_err(g.interior(g.field(d.download())), g.interior(ref)) <= REL_FAST
+
+
+def test_single_stage_with_caller_ghosts(mode):
+    """bc_mask = 0: the stage reads the ghost cells stored in phi_s (a patch
+    whose halo came from a neighbour), on a fill box with non-zero bounds."""
+    from lsmlib_b200 import gpu, integrator
+    rng = np.random.default_rng(2)
+    g = Grid((21, 14, 12), lo=(-5, 3, 7), dx=(0.1, 0.1, 0.1))
+    phi = g.field(rng.standard_normal(g.shape))
+    vel = [g.field(rng.standard_normal(g.shape)) for _ in range(3)]
+    tb = oracle.oracle_toolbox()
+    st = Stepper(tb, g)
+    st.zero_rhs()
+    f = dict(st.up)
+    f.update({"phi": phi, "vel_x": vel[0], "vel_y": vel[1], "vel_z": vel[2]})
+    tb.call("lsm3dupwindhjweno5_", f, g.fb, **g.dxyz())
+    tb.call("lsm3daddadvectiontermtolserhs_",
+            {"lse_rhs": st.rhs, "phi_x": st.up["phi_x"], "phi_y": st.up["phi_y"],
+             "phi_z": st.up["phi_z"], "vel_x": vel[0], "vel_y": vel[1],
+             "vel_z": vel[2]}, g.fb)
+    out = g.zeros()
+    tb.call("lsm3dtvdrk3stage1_", {"u_stage1": out, "u_cur": phi, "rhs": st.rhs},
+            g.fb, dt=0.013)
+    d_out = gpu.DeviceArray(g.shape)
+    d_phi = gpu.DeviceArray.from_host(phi.data)
+    dv = [gpu.DeviceArray.from_host(v.data) for v in vel]
+    integrator.stage(0, 8, d_out, d_phi, d_phi, dv, g.gb, g.fb, g.dx, 0.013, 1,
+                     bc_mask=0)
+    check(mode, g.interior(g.field(d_out.download())), g.interior(out))
+
+
+def test_fp32_form_error_against_fp64():
+    """FP32 storage and arithmetic (FP64 CFL reduction, dt and t, FP64 WENO5
+    on kink stencils, FP64 smoothed sign) stays within 1e-5 of the FP64
+    oracle over 10 normal-velocity steps with a reinitialization."""
+    from lsmlib_b200 import gpu, integrator
+    n = (48, 48, 48)
+    g = Grid(n, dx=(2.0 / 48,) * 3)
+    x_lo = (-1.0, -1.0, -1.0)
+    phi0 = spheres(g, x_lo, seed=11)
+    x, y, z = g.centers(x_lo)
+    F = 1.0 + 0.2 * np.sin(4 * np.pi * x) * np.sin(4 * np.pi * y) * np.sin(4 * np.pi * z)
+    st = Stepper(oracle.oracle_toolbox(), g)
+    ref = g.field(phi0)
+    Ff = g.field(F)
+    for s in range(10):
+        st.normal_step(ref, Ff, 0.5)
+        if (s + 1) % 5 == 0:
+            st.reinit(ref, 0.5, 4)
+    ws = integrator.Workspace(g.gb, 4)
+    d = gpu.DeviceArray.from_host(phi0.astype(np.float32))
+    dF = gpu.DeviceArray.from_host(F.astype(np.float32))
+    ws.normal(d, dF, g.fb, g.dx, cfl=0.5, nsteps=10, reinit_interval=5,
+              reinit_iters=4)
+    got = g.interior(g.field(d.download().astype(np.float64)))
+    err = np.abs(got - g.interior(ref))
+    assert err.max() <= ABS_FP32, err.max()
