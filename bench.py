@@ -1,0 +1,446 @@
+#!/usr/bin/env python3
+"""Benchmark of the level-set toolbox hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one GPU): 256^3 interior cells on [-1,1]^3 (3 ghost cells), union
+of 6 seeded spheres, normal-velocity motion F = 1 + 0.2 sin(4 pi x) sin(4 pi y)
+sin(4 pi z), HJ-WENO5 + Godunov + TVD-RK3 at CFL 0.5 with the CFL dt of every
+step, reinitialization (20 TVD-RK3 pseudo-steps, dt = 0.5 dx) after every 10th
+step.  One benchmark step = one physical time step (CFL dt + 3 stages), the
+reinitialization cost included at its cadence.  Metric: cell-updates/s (one
+interior cell advanced one full step), FP64.
+
+Our arm prints one JSON line with value (device-resident fused drivers, FP64
+fast arithmetic), the FP32 form beside it (with its error against the FP64
+run), e2e (the same steps through the C ABI with the level set and speed on
+pinned host memory, copied in and out every step), the roofline of the
+dominant kernel, the CFL-dt kernel count and the reference's CPU toolbox timed
+on this host.  Under torchrun every rank runs a replica on its own GPU
+(weak scaling, no data-path collective).
+
+``--impl reference`` times the reference's own toolbox routines (translated
+from its Fortran sources, oracle/_ref) on all host cores, patch-decomposed as
+the reference's parallel package does, on a bounded z-slab of the same
+workload; rank 0 alone runs it.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("cell-updates/s, plain FP64 vs FP32/batched at ≤1e-5 err; "
+          "% HBM; adjoint/fwd")
+UNIT = "cell-updates/s"
+N_CELLS = 256
+WORKLOAD = ("256^3 normal-velocity level set (6 spheres, F = 1 + 0.2 sin sin sin), "
+            "HJ-WENO5 + Godunov + TVD-RK3, CFL 0.5, reinit every 10 steps x 20")
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--id=%d" % self.index, "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for nm, v in zip(names, r[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(self.rows), "reasons": sorted(reasons)}
+
+
+def dist_setup(n_gpus):
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, v):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, world, rank, local, pg):
+    from lsmlib_b200 import gpu, integrator, workloads
+    from lsmlib_b200.ext_abi import dbls, ints
+
+    lib = gpu.load()
+    gpu.check_rc(lib.lsmgpu_set_device(local), "set_device")
+    cfg = workloads.config2(N_CELLS)
+    n = cfg["n"]
+    gb, fb = workloads.boxes(n)
+    dx = cfg["dx"]
+    cells = n[0] * n[1] * n[2]
+    K, W = args.steps, args.warmup
+    interval, iters = cfg["reinit_interval"], cfg["reinit_iters"]
+
+    def run_steps(ws, d_phi, d_F, nsteps, step0):
+        ws.normal(d_phi, d_F, fb, dx, cfl=cfg["cfl"], nsteps=nsteps, step0=step0,
+                  reinit_interval=interval, reinit_iters=iters, use_phi0=cfg["use_phi0"])
+
+    integrator.set_fp_mode(integrator.FP_FAST)
+    timer = gpu.Timer()
+
+    # ---- FP64, device resident -------------------------------------------
+    ws = integrator.Workspace(gb, 8)
+    d_phi = gpu.DeviceArray.from_host(cfg["phi"])
+    d_F = gpu.DeviceArray.from_host(cfg["F"])
+    run_steps(ws, d_phi, d_F, W, 0)
+    gpu.check_rc(lib.lsmgpu_stream_synchronize(), "sync")
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(pg)
+    gpu.check_rc(lib.lsmgpu_stream_synchronize(), "sync")
+    launches0 = lib.lsmgpu_kernel_launch_count()
+    timer.start()
+    run_steps(ws, d_phi, d_F, K, W)
+    timer.stop()
+    ms = timer.ms()
+    gpu.check_rc(lib.lsmgpu_stream_synchronize(), "sync")
+    launches = lib.lsmgpu_kernel_launch_count() - launches0
+    barrier(pg)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(pg, ms)
+    value = world * cells * K / (ms_max / 1e3)
+    phi64 = d_phi.download()
+
+    fp32 = None
+    if not args.no_fp32:
+        # ---- FP32 form beside it -----------------------------------------
+        ws32 = integrator.Workspace(gb, 4)
+        d32 = gpu.DeviceArray.from_host(cfg["phi"].astype(np.float32))
+        dF32 = gpu.DeviceArray.from_host(cfg["F"].astype(np.float32))
+        run_steps(ws32, d32, dF32, W, 0)
+        barrier(pg)
+        gpu.check_rc(lib.lsmgpu_stream_synchronize(), "sync")
+        timer.start()
+        run_steps(ws32, d32, dF32, K, W)
+        timer.stop()
+        ms32 = max_over_ranks(pg, timer.ms())
+        value32 = world * cells * K / (ms32 / 1e3)
+        phi32 = d32.download().astype(np.float64)
+        g = 3
+        inner = (slice(g, g + n[0]), slice(g, g + n[1]), slice(g, g + n[2]))
+        diff = np.abs(phi32[inner] - phi64[inner])
+        band = np.abs(phi64[inner]) < 5 * dx[0]
+        err32 = {"max_abs": float(diff.max()), "l1_mean": float(diff.mean()),
+                 "max_abs_band_5dx": float(diff[band].max()) if band.any() else None,
+                 "steps_compared": W + K}
+        del d32, dF32, ws32
+        fp32 = {"value": value32, "unit": UNIT, "ms_per_step": ms32 / K,
+                "speedup_vs_fp64": value32 / value, "error_vs_fp64": err32}
+
+    # ---- dominant kernels, timed alone on the same stream -----------------
+    peak, peak_kind = load_peaks()
+    kern = {}
+    for name, kind, rk, nbytes in (("stage_reinit_rk32", 2, 32, 3),
+                                   ("stage_normal_rk32", 1, 32, 4)):
+        a = gpu.DeviceArray(d_phi.shape)
+        b = gpu.DeviceArray.from_host(phi64)
+        for _ in range(3):
+            integrator.stage(kind, 8, a, b, b, [d_F], gb, fb, dx, 1e-3, rk)
+        reps = 20
+        timer.start()
+        for _ in range(reps):
+            integrator.stage(kind, 8, a, b, b, [d_F], gb, fb, dx, 1e-3, rk)
+        timer.stop()
+        t = timer.ms() / reps
+        kern[name] = {"ms": t, "bytes": nbytes * 8 * cells}
+        del a, b
+    # launches per step at the reinit cadence: reinit 3*iters/interval,
+    # normal 2 (+ the fused L/CFL pass)
+    share_re = 3 * iters / interval * kern["stage_reinit_rk32"]["ms"]
+    share_no = 3 * kern["stage_normal_rk32"]["ms"]
+    dom = "stage_reinit_rk32" if share_re >= share_no else "stage_normal_rk32"
+    achieved = kern[dom]["bytes"] / (kern[dom]["ms"] / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get(dom)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                "kernel": dom, "kernel_ms": round(kern[dom]["ms"], 4),
+                "algorithmic_bytes_per_launch": kern[dom]["bytes"],
+                "peak_source": peak_kind,
+                "other_kernels": {k: round(v["ms"], 4) for k, v in kern.items() if k != dom}}
+
+    e2e = None
+    if not args.no_e2e:
+        # ---- e2e: host-resident level set through the C ABI ----------------
+        h_phi = lib.lsmgpu_host_alloc(cfg["phi"].nbytes)
+        h_F = lib.lsmgpu_host_alloc(cfg["F"].nbytes)
+        count = cfg["phi"].size
+        hp = np.ctypeslib.as_array((ctypes.c_double * count).from_address(h_phi))
+        hf = np.ctypeslib.as_array((ctypes.c_double * count).from_address(h_F))
+        hp[:] = cfg["phi"].ravel(order="F")
+        hf[:] = cfg["F"].ravel(order="F")
+        ws_e = integrator.Workspace(gb, 8)
+        e_phi = gpu.DeviceArray(cfg["phi"].shape)
+        e_F = gpu.DeviceArray(cfg["F"].shape)
+        nb = cfg["phi"].nbytes
+
+        def e2e_step(s):
+            gpu.check_rc(lib.lsmgpu_memcpy_htod(e_phi.ptr, h_phi, nb), "htod")
+            gpu.check_rc(lib.lsmgpu_memcpy_htod(e_F.ptr, h_F, nb), "htod")
+            run_steps(ws_e, e_phi, e_F, 1, s)
+            gpu.check_rc(lib.lsmgpu_memcpy_dtoh(h_phi, e_phi.ptr, nb), "dtoh")
+
+        for s in range(W):
+            e2e_step(s)
+        barrier(pg)
+        t0 = time.perf_counter()
+        for s in range(W, W + K):
+            e2e_step(s)
+        t_e2e = max_over_ranks(pg, time.perf_counter() - t0)
+        e2e = {"value": world * cells * K / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": 2 * nb, "d2h_bytes_per_step": nb,
+               "ms_per_step": 1e3 * t_e2e / K,
+               "path": "lsmgpu_normal_tvdrk3 with phi and F copied from pinned host "
+                       "memory and phi copied back every step"}
+        lib.lsmgpu_host_free(h_phi)
+        lib.lsmgpu_host_free(h_F)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample(cfg)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": ms_max / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": list(n), "ghost": 3,
+                   "cfl": cfg["cfl"], "reinit_interval": interval,
+                   "reinit_iters": iters, "seed": cfg["seed"],
+                   "fp_mode": "fast (FMA, single-reciprocal WENO5 weights; <=1e-12 rel. vs reference)",
+                   "l2": "inputs larger than L2 (144 MB per field, 6 fields live)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "fp32": fp32, "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    return line
+
+
+# ---------------------------------------------------------------------------
+# CPU reference
+# ---------------------------------------------------------------------------
+def slab_case(cfg, nz):
+    """A z-slab of the config-2 grid: rows through the middle of the domain,
+    linear-extrapolation boundaries on all faces of the slab."""
+    from oracle.driver import Grid
+    n = cfg["n"]
+    k0 = (n[2] - nz) // 2
+    g = Grid((n[0], n[1], nz), dx=cfg["dx"])
+    ks = slice(k0, k0 + nz + 6)
+    phi = g.field(cfg["phi"][:, :, ks])
+    F = g.field(cfg["F"][:, :, ks])
+    return g, phi, F
+
+
+def reference_toolbox():
+    import oracle
+    if oracle.reference_available():
+        return oracle.reference_toolbox(), "reference"
+    return oracle.oracle_toolbox(), "port"
+
+
+def cpu_baseline_sample(cfg, nz=64):
+    """Single-thread reference routines on a 256x256xnz slab: one normal step
+    and two reinitialization pseudo-steps (the per-step share of 20
+    pseudo-steps every 10 steps)."""
+    from oracle.driver import Stepper
+    tb, kind = reference_toolbox()
+    g, phi, F = slab_case(cfg, nz)
+    st = Stepper(tb, g)
+    t0 = time.perf_counter()
+    st.normal_step(phi, F, cfg["cfl"])
+    t1 = time.perf_counter()
+    st.reinit(phi, cfg["cfl"], 2)
+    t2 = time.perf_counter()
+    per_step = (t1 - t0) + (t2 - t1) * (cfg["reinit_iters"] / cfg["reinit_interval"]) / 2
+    cells = g.n[0] * g.n[1] * g.n[2]
+    return {"value": cells / per_step, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": "256x256x%d slab of the workload: 1 step + 2 reinit pseudo-steps "
+                      "(= the reinit share of one step), %.1f s" % (nz, t2 - t0)}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    from oracle.driver import PatchedNormalStepper
+    from lsmlib_b200 import workloads
+    cfg = workloads.config2(N_CELLS)
+    threads = os.cpu_count() or 1
+    nz = max(8, 4 * threads)
+    tb, kind = reference_toolbox()
+    g, phi, F = slab_case(cfg, nz)
+    ps = PatchedNormalStepper(tb, g, threads)
+    parts, Fs = ps.scatter(phi), ps.scatter(F)
+    iters_per_step = cfg["reinit_iters"] // cfg["reinit_interval"]
+
+    def step():
+        ps.normal_step(parts, Fs, cfg["cfl"])
+        ps.reinit(parts, cfg["cfl"], iters_per_step)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    cells = g.n[0] * g.n[1] * g.n[2]
+    value = cells * args.steps / dt
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "grid": list(cfg["n"]), "ghost": 3,
+                   "cfl": cfg["cfl"], "sample": "256x256x%d z-slab" % nz},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(ps.patches),
+                         "kind": kind,
+                         "sample": "256x256x%d slab, %d patches on %d threads; a step = "
+                                   "1 time step + %d reinit pseudo-steps"
+                                   % (nz, len(ps.patches), threads, iters_per_step)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def profile_kernels():
+    """Two launches each of the FP64 normal-velocity and reinitialization
+    stage kernels (TVD-RK3 stage 2) on the workload's grid."""
+    from lsmlib_b200 import gpu, integrator, workloads
+    cfg = workloads.config2(N_CELLS)
+    gb, fb = workloads.boxes(cfg["n"])
+    integrator.set_fp_mode(integrator.FP_FAST)
+    a = gpu.DeviceArray(cfg["phi"].shape)
+    b = gpu.DeviceArray.from_host(cfg["phi"])
+    f = gpu.DeviceArray.from_host(cfg["F"])
+    for kind in (1, 2):
+        for _ in range(2):
+            integrator.stage(kind, 8, a, b, b, [f], gb, fb, cfg["dx"], 1e-3, 32)
+    gpu.check_rc(gpu.load().lsmgpu_stream_synchronize(), "sync")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true",
+                    help="skip the CPU baseline sample of our arm")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 form")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg")
+    ap.add_argument("--size", type=int, default=256, help="interior cells per axis")
+    ap.add_argument("--profile", action="store_true",
+                    help="only launch the two fused stage kernels twice each "
+                         "(for ncu captures) and exit")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    global N_CELLS
+    N_CELLS = args.size
+    world, rank, local, pg = dist_setup(args.gpus)
+    if args.profile:
+        profile_kernels()
+        return
+    if args.impl == "reference":
+        line = run_reference(args, world, rank)
+    else:
+        line = run_ours(args, world, rank, local, pg)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

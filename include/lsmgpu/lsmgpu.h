@@ -321,6 +321,8 @@ int lsmgpu_peek_last_error(void);
 /* message of the last error ("" when none); valid until the next call */
 const char *lsmgpu_get_last_error_string(void);
 
+/* CUDA device used by the calling thread (cudaSetDevice) */
+int lsmgpu_set_device(int device);
 /* stream used by the calling thread's subsequent calls (cudaStream_t; NULL =
  * the legacy default stream) */
 int lsmgpu_set_stream(void *cuda_stream);

@@ -867,6 +867,10 @@ const char* lsmgpu_get_last_error_string(void) {
   t_msg_out = t_msg;
   return t_msg_out.c_str();
 }
+int lsmgpu_set_device(int device) {
+  return cuda_ok(cudaSetDevice(device), "cudaSetDevice") ? LSMGPU_SUCCESS
+                                                         : LSMGPU_ERR_CUDA;
+}
 int lsmgpu_set_stream(void* s) {
   t_stream = (cudaStream_t)s;
   return LSMGPU_SUCCESS;

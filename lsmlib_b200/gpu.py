@@ -32,6 +32,7 @@ _EXT = {
     "lsmgpu_get_last_error": (ctypes.c_int, []),
     "lsmgpu_peek_last_error": (ctypes.c_int, []),
     "lsmgpu_get_last_error_string": (ctypes.c_char_p, []),
+    "lsmgpu_set_device": (ctypes.c_int, [ctypes.c_int]),
     "lsmgpu_set_stream": (ctypes.c_int, [ctypes.c_void_p]),
     "lsmgpu_get_stream": (ctypes.c_void_p, []),
     "lsmgpu_set_sync": (ctypes.c_int, [ctypes.c_int]),

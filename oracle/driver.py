@@ -181,6 +181,131 @@ class Stepper:
             self.rk(3, phi, self.stage2, phi, dtr)
 
 
+class PatchedNormalStepper:
+    """Normal-velocity steps with reinitialization over z-slab patches run by
+    a thread pool -- the reference's own parallel strategy (patch loops over
+    the toolbox routines, a 3-cell ghost exchange before every stage and a
+    global minimum of dt; LevelSetFunctionIntegrator.cc:382, :567, :1377).
+    ctypes releases the GIL during each routine, so patches run in parallel.
+    Interior results equal the single-grid Stepper's bit for bit."""
+
+    def __init__(self, tb, grid, nthreads):
+        import concurrent.futures
+        self.g = grid
+        self.nthreads = max(1, int(nthreads))
+        nz = grid.n[2]
+        npatch = max(1, min(self.nthreads, nz // 4))
+        cuts = [grid.fb_lo[2] + (nz * p) // npatch for p in range(npatch + 1)]
+        self.patches = []
+        for p in range(npatch):
+            klo, khi = cuts[p], cuts[p + 1] - 1
+            pg = Grid((grid.n[0], grid.n[1], khi - klo + 1), ghost=grid.ghost,
+                      lo=(grid.fb_lo[0], grid.fb_lo[1], klo), dx=grid.dx)
+            self.patches.append((pg, Stepper(tb, pg)))
+        self.pool = concurrent.futures.ThreadPoolExecutor(self.nthreads)
+
+    def scatter(self, full):
+        """Per-patch copies of a global Field (interior plus halo)."""
+        out = []
+        for pg, _ in self.patches:
+            f = pg.zeros()
+            f.data[...] = full.view(pg.gb_lo, pg.gb_hi)
+            out.append(f)
+        return out
+
+    def gather(self, parts, full):
+        for (pg, _), f in zip(self.patches, parts):
+            full.view(pg.fb_lo, pg.fb_hi)[...] = pg.interior(f)
+
+    def exchange(self, parts):
+        """z-halo planes from the neighbouring patches' interiors; the global
+        z faces get the linear extrapolation."""
+        for p, ((pg, st), f) in enumerate(zip(self.patches, parts)):
+            if p > 0:
+                qg, _ = self.patches[p - 1]
+                lo = (pg.gb_lo[0], pg.gb_lo[1], pg.gb_lo[2])
+                hi = (pg.gb_hi[0], pg.gb_hi[1], pg.fb_lo[2] - 1)
+                f.view(lo, hi)[...] = parts[p - 1].view(lo, hi)
+            if p + 1 < len(parts):
+                lo = (pg.gb_lo[0], pg.gb_lo[1], pg.fb_hi[2] + 1)
+                hi = (pg.gb_hi[0], pg.gb_hi[1], pg.gb_hi[2])
+                f.view(lo, hi)[...] = parts[p + 1].view(lo, hi)
+
+    def _fill(self, p, f):
+        pg, st = self.patches[p]
+        faces = [0, 1, 2, 3]
+        if p == 0:
+            faces.append(4)
+        if p == len(self.patches) - 1:
+            faces.append(5)
+        for face in faces:
+            st.tb.call("lsm3dlinearextrapolation_", {"phi": f}, pg.fb,
+                       bdry_location_idx=face)
+
+    def _map(self, fn):
+        return list(self.pool.map(fn, range(len(self.patches))))
+
+    def _stage_rhs(self, parts, rhs_kind, aux, phi0s=None, use0=0):
+        self.exchange(parts)
+
+        def work(p):
+            pg, st = self.patches[p]
+            f = parts[p]
+            self._fill(p, f)
+            if rhs_kind == "normal":
+                st.zero_rhs()
+                st.weno_pm(f)
+                d = dict(st.grads)
+                d.update({"lse_rhs": st.rhs, "vel_n": aux[p]})
+                st.tb.call("lsm3daddnormalveltermtolserhs_", d, pg.fb)
+            else:
+                st.weno_pm(f)
+                d = dict(st.grads)
+                d.update({"reinit_rhs": st.rhs, "phi": f, "phi0": phi0s[p]})
+                st.tb.call("lsm3dcomputereinitializationeqnrhs_", d, pg.fb,
+                           use_phi0_for_sgn=use0, **pg.dxyz())
+        self._map(work)
+
+    def _rk(self, s, outs, uss, ucs, dt):
+        self._map(lambda p: self.patches[p][1].rk(s, outs[p], uss[p] if uss else None,
+                                                  ucs[p], dt))
+
+    def normal_step(self, parts, Fs, cfl):
+        self.exchange(parts)
+
+        def dtp(p):
+            pg, st = self.patches[p]
+            self._fill(p, parts[p])
+            st.weno_pm(parts[p])
+            d = dict(st.grads)
+            d["vel_n"] = Fs[p]
+            return st.tb.call("lsm3dcomputestablenormalveldt_", d, pg.fb,
+                              cfl_number=cfl, **pg.dxyz())["dt"]
+        dt = min(self._map(dtp))         # minReduction of the patch dts
+        s1 = [st.stage1 for _, st in self.patches]
+        s2 = [st.stage2 for _, st in self.patches]
+        self._stage_rhs(parts, "normal", Fs)
+        self._rk(1, s1, None, parts, dt)
+        self._stage_rhs(s1, "normal", Fs)
+        self._rk(2, s2, s1, parts, dt)
+        self._stage_rhs(s2, "normal", Fs)
+        self._rk(3, parts, s2, parts, dt)
+        return dt
+
+    def reinit(self, parts, cfl, iters, use0=0):
+        dtr = cfl * min(self.g.dx)
+        phi0s = [f.copy() for f in parts]
+        s1 = [st.stage1 for _, st in self.patches]
+        s2 = [st.stage2 for _, st in self.patches]
+        for _ in range(iters):
+            self._stage_rhs(parts, "reinit", None, phi0s, use0)
+            self._rk(1, s1, None, parts, dtr)
+            self._stage_rhs(s1, "reinit", None, phi0s, use0)
+            self._rk(2, s2, s1, parts, dtr)
+            self._stage_rhs(s2, "reinit", None, phi0s, use0)
+            self._rk(3, parts, s2, parts, dtr)
+
+
 def deformation_velocity(grid, x_lo, t, period=3.0):
     """LeVeque's 3D deformation field at time t on the ghost box."""
     x, y, z = grid.centers(x_lo)
