@@ -428,6 +428,32 @@ int lsmgpu_reinit_tvdrk3(lsmgpu_workspace *ws, void *phi, const int fb[6],
                          const double dx[3], double cfl, int iters,
                          int use_phi0_for_sgn);
 
+/* ---- an entry point that allocates no memory --------------------------------
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory when they call in: code running under a fixed, pre-reserved memory
+ * pool, a real-time loop that cannot absorb cudaMalloc's device-wide
+ * synchronisation, or a host framework that owns all device memory.
+ *
+ * Computes, over the fill box fb, rhs = -F |grad phi| (HJ-WENO5 derivatives,
+ * Godunov selection; the value LSM3D_HJ_WENO5 followed by
+ * LSM3D_ADD_NORMAL_VEL_TERM_TO_LSE_RHS writes into a zeroed RHS) and the CFL
+ * dt of LSM3D_COMPUTE_STABLE_NORMAL_VEL_DT over fb.  phi, F and rhs are
+ * double device arrays sharing the ghost box gb, which must cover fb by 3
+ * cells; the ghost cells of phi are read as stored.  dt is a host or device
+ * double; a host dt makes the call wait for the result.
+ *
+ * Scratch: one partial maximum per tile of 32x8x32 cells lives in a static
+ * device array of 4096 + 1 doubles (32 KB) that every GPU loading the library
+ * holds until exit; a fill box needing more than 4096 tiles is rejected with
+ * LSMGPU_ERR_INVALID_BOX.  The first call on a device looks up that array's
+ * device address, so make it before any stream capture.  Every call reuses
+ * the same array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. */
+int lsmgpu_normal_rhs_dt_noalloc(double *rhs, double *dt, const double *phi,
+                                 const double *F, const int gb[6],
+                                 const int fb[6], const double dx[3],
+                                 double cfl_number);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -34,6 +34,7 @@ SOURCES = {
     "integrator.cu": ["--fmad=false"],
     "batched.cu": ["--fmad=true"],
     "adjoint.cu": ["--fmad=true"],
+    "noalloc.cu": ["--fmad=false"],
 }
 
 
