@@ -428,6 +428,38 @@ int lsmgpu_reinit_tvdrk3(lsmgpu_workspace *ws, void *phi, const int fb[6],
                          const double dx[3], double cfl, int iters,
                          int use_phi0_for_sgn);
 
+/* ---- batched grids -------------------------------------------------------------
+ * Many independent grids of uneven sizes advanced together under their own
+ * constant velocities and CFL dts.  The grids are packed in one device buffer
+ * (grid g's ghost box, interior 0..n-1 per axis with 3 ghost cells, starts at
+ * the element offset lsmgpu_batch_grid returns).  Every TVD-RK3 stage is one
+ * persistent launch that takes tiles from a work-list; a step is captured in
+ * a CUDA graph.  The tile shape is chosen by lsmgpu_batch_autotune. */
+typedef struct lsmgpu_batch lsmgpu_batch;
+/* n[3*g..3*g+2]: interior cells of grid g; dx[3*g..3*g+2]: its spacing */
+int lsmgpu_batch_create(lsmgpu_batch **b, int ngrids, const int *n,
+                        const double *dx, int precision);
+int lsmgpu_batch_destroy(lsmgpu_batch *b);
+int lsmgpu_batch_grid(lsmgpu_batch *b, int g, long long *offset, int gb[6]);
+long long lsmgpu_batch_total_elements(lsmgpu_batch *b);
+long long lsmgpu_batch_cells(lsmgpu_batch *b);
+int lsmgpu_batch_upload(lsmgpu_batch *b, const void *host);
+int lsmgpu_batch_download(lsmgpu_batch *b, void *host);
+/* vel[3*g..3*g+2]: constant velocity of grid g; sets every grid's CFL dt */
+int lsmgpu_batch_set_velocity(lsmgpu_batch *b, const double *vel, double cfl);
+int lsmgpu_batch_get_dt(lsmgpu_batch *b, double *dt);
+int lsmgpu_batch_set_tile(lsmgpu_batch *b, int shape);
+int lsmgpu_batch_get_tile(lsmgpu_batch *b, int *shape, int tile[3]);
+int lsmgpu_batch_set_fp64_kinks(lsmgpu_batch *b, int on);
+/* times each tile shape on the batch (state preserved), keeps the fastest;
+ * ms_out (optional) receives one time per shape */
+int lsmgpu_batch_autotune(lsmgpu_batch *b, float *ms_out);
+/* mode 0: graph replay of persistent work-list launches; 1: the same without
+ * a graph; 2: one launch per grid per stage */
+int lsmgpu_batch_advect_tvdrk3(lsmgpu_batch *b, int nsteps, int mode,
+                               int sync);
+void *lsmgpu_batch_stream(lsmgpu_batch *b);
+
 /* ---- an entry point that allocates no memory --------------------------------
  * No counterpart in the reference.  For callers that must not allocate device
  * memory when they call in: code running under a fixed, pre-reserved memory

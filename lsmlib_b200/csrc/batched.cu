@@ -1,0 +1,536 @@
+// batched.cu -- many level-set grids of uneven sizes advanced together.
+//
+// The grids of a batch live in one packed device buffer (each grid's ghost
+// box contiguous, 256-byte aligned).  A work-list holds one entry per tile
+// (grid, tile x, tile y, tile z) of every grid.  Each TVD-RK3 stage is ONE
+// persistent launch: every block takes the next tile from an atomic counter
+// and runs the fused stage of stage.cuh on it, until the list is exhausted;
+// blocks never wait for one another.  A whole step (three stages and the
+// counter resets) is captured once in a CUDA graph and replayed.
+//
+// Each grid has its own constant velocity and its own CFL dt
+//   dt = cfl / (|u|/dx + |v|/dy + |w|/dz + tiny)
+// -- the value LSM3D_COMPUTE_STABLE_ADVECTION_DT returns for a constant field
+// (lsm_utilities3d.f.in:299-322), kept in FP64.
+//
+// The tile shape (TX x TY cells, TZ planes) is chosen per batch by timing the
+// candidates on the batch itself (lsmgpu_batch_autotune); the choice is
+// cached per (precision, size class).
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "capi_common.h"
+#include "launch.h"
+#include "stage.cuh"
+
+using namespace lsmgpu;
+
+namespace {
+
+struct GridMeta {
+  long offset;     // element offset of the grid's ghost box
+  Box gb;
+  FillBox fb;
+  double inv[3];
+  double dx_sq;
+  double dt;
+  double vel[3];
+};
+
+// tile shapes the autotuner chooses from
+struct TileShape { int tx, ty, tz; };
+constexpr TileShape kShapes[] = {{32, 8, 16}, {32, 8, 32}, {32, 8, 64}, {16, 8, 16},
+                                 {16, 8, 32}};
+constexpr int kNumShapes = 5;
+
+template <typename T, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TX * TY, 2)
+k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ items,
+                int nitems, unsigned* counter, T* out, const T* phi_s,
+                const T* phi_n, int rk_kind, int fp64_kinks) {
+  __shared__ T tile[2][TY + 6][TX + 6];
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) s_item = (int)atomicAdd(counter, 1u);
+    __syncthreads();
+    const int t = s_item;
+    // every thread has read s_item and finished the previous tile
+    __syncthreads();
+    if (t >= nitems) break;
+    const int4 it = items[t];
+    const GridMeta& g = grids[it.x];
+    StageParams<T> p;
+    p.out = out + g.offset;
+    p.phi_s = phi_s + g.offset;
+    p.phi_n = phi_n + g.offset;
+    p.aux0 = p.aux1 = p.aux2 = nullptr;
+    p.rhs_out = nullptr;
+    p.partials = nullptr;
+    p.gb = g.gb;
+    p.fb = g.fb;
+    p.dom = g.fb;
+    p.bc_mask = 0x3fu;
+    for (int d = 0; d < 3; d++) {
+      p.inv[d] = (T)g.inv[d];
+      p.vel_const[d] = (T)g.vel[d];
+    }
+    p.dx_sq = (T)g.dx_sq;
+    p.dt_dev = nullptr;
+    p.dt = g.dt;
+    p.rk_kind = rk_kind;
+    p.use_phi0 = 0;
+    p.fp64_kinks = fp64_kinks;
+    stage_tile<T, kStageAdvectConst, true, TX, TY, TZ>(p, it.y, it.z, it.w, tile);
+  }
+}
+
+// the plain alternative: one launch per grid per stage
+template <typename T, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TX * TY, 2)
+k_grid_stage(const GridMeta* __restrict__ grids, int gi, T* out, const T* phi_s,
+             const T* phi_n, int rk_kind, int fp64_kinks) {
+  __shared__ T tile[2][TY + 6][TX + 6];
+  const GridMeta& g = grids[gi];
+  StageParams<T> p;
+  p.out = out + g.offset;
+  p.phi_s = phi_s + g.offset;
+  p.phi_n = phi_n + g.offset;
+  p.aux0 = p.aux1 = p.aux2 = nullptr;
+  p.rhs_out = nullptr;
+  p.partials = nullptr;
+  p.gb = g.gb;
+  p.fb = g.fb;
+  p.dom = g.fb;
+  p.bc_mask = 0x3fu;
+  for (int d = 0; d < 3; d++) {
+    p.inv[d] = (T)g.inv[d];
+    p.vel_const[d] = (T)g.vel[d];
+  }
+  p.dx_sq = (T)g.dx_sq;
+  p.dt_dev = nullptr;
+  p.dt = g.dt;
+  p.rk_kind = rk_kind;
+  p.use_phi0 = 0;
+  p.fp64_kinks = fp64_kinks;
+  stage_tile<T, kStageAdvectConst, true, TX, TY, TZ>(p, (int)blockIdx.x, (int)blockIdx.y,
+                                                     (int)blockIdx.z, tile);
+}
+
+std::mutex g_tune_mutex;
+std::map<std::pair<int, int>, int> g_tune_cache;   // (precision, size class) -> shape
+
+}  // namespace
+
+struct lsmgpu_batch {
+  int ngrids = 0;
+  int prec = 8;
+  std::vector<GridMeta> meta;       // host copy
+  GridMeta* d_meta = nullptr;
+  long total = 0;                   // elements in each packed buffer
+  long cells = 0;                   // interior cells of all grids
+  void* phi = nullptr;
+  void* phi1 = nullptr;
+  void* phi2 = nullptr;
+  int4* d_items[kNumShapes] = {nullptr};
+  int nitems[kNumShapes] = {0};
+  unsigned* d_counter = nullptr;    // three counters, one per stage
+  int shape = 1;
+  int fp64_kinks = 0;
+  int blocks_per_sm = 2;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graph_shape = -1;
+};
+
+namespace {
+
+int size_class(const lsmgpu_batch* b) {
+  // mean interior edge length bucketed by powers of two
+  const double mean = b->ngrids ? (double)b->cells / b->ngrids : 0.0;
+  int c = 0;
+  for (double e = std::cbrt(mean); e >= 2.0; e /= 2.0) c++;
+  return c;
+}
+
+template <typename T>
+cudaError_t launch_shape(lsmgpu_batch* b, int shape, bool batched, int rk_kind,
+                         T* out, const T* in, const T* base, unsigned* counter,
+                         cudaStream_t st) {
+  const int grid = b->num_sms * b->blocks_per_sm;
+#define BATCH_CASE(I, TX, TY, TZ)                                                  \
+  case I:                                                                          \
+    if (batched) {                                                                 \
+      k_batched_stage<T, TX, TY, TZ><<<grid, dim3(TX, TY), 0, st>>>(               \
+          b->d_meta, b->d_items[I], b->nitems[I], counter, out, in, base, rk_kind, \
+          b->fp64_kinks);                                                          \
+    } else {                                                                       \
+      for (int gi = 0; gi < b->ngrids; gi++) {                                     \
+        const FillBox& f = b->meta[gi].fb;                                         \
+        dim3 g((f.n(0) + TX - 1) / TX, (f.n(1) + TY - 1) / TY, (f.n(2) + TZ - 1) / TZ); \
+        k_grid_stage<T, TX, TY, TZ><<<g, dim3(TX, TY), 0, st>>>(                   \
+            b->d_meta, gi, out, in, base, rk_kind, b->fp64_kinks);                 \
+      }                                                                            \
+    }                                                                              \
+    break;
+  switch (shape) {
+    BATCH_CASE(0, 32, 8, 16)
+    BATCH_CASE(1, 32, 8, 32)
+    BATCH_CASE(2, 32, 8, 64)
+    BATCH_CASE(3, 16, 8, 16)
+    BATCH_CASE(4, 16, 8, 32)
+    default: return cudaErrorInvalidValue;
+  }
+#undef BATCH_CASE
+  launch_counter() += batched ? 1 : b->ngrids;
+  return cudaGetLastError();
+}
+
+// one TVD-RK3 step of every grid (phi in place)
+cudaError_t step(lsmgpu_batch* b, int shape, bool batched, cudaStream_t st) {
+  cudaError_t e;
+  for (int s = 0; s < 3; s++)
+    if ((e = cudaMemsetAsync(b->d_counter + s, 0, sizeof(unsigned), st)) != cudaSuccess)
+      return e;
+  if (b->prec == 8) {
+    double *phi = (double*)b->phi, *p1 = (double*)b->phi1, *p2 = (double*)b->phi2;
+    if ((e = launch_shape<double>(b, shape, batched, 1, p1, phi, phi, b->d_counter, st))) return e;
+    if ((e = launch_shape<double>(b, shape, batched, 32, p2, p1, phi, b->d_counter + 1, st))) return e;
+    return launch_shape<double>(b, shape, batched, 33, phi, p2, phi, b->d_counter + 2, st);
+  }
+  float *phi = (float*)b->phi, *p1 = (float*)b->phi1, *p2 = (float*)b->phi2;
+  if ((e = launch_shape<float>(b, shape, batched, 1, p1, phi, phi, b->d_counter, st))) return e;
+  if ((e = launch_shape<float>(b, shape, batched, 32, p2, p1, phi, b->d_counter + 1, st))) return e;
+  return launch_shape<float>(b, shape, batched, 33, phi, p2, phi, b->d_counter + 2, st);
+}
+
+bool batch_ok(lsmgpu_batch* b, const char* R) {
+  if (!b) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null batch");
+    return false;
+  }
+  return true;
+}
+
+void drop_graph(lsmgpu_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->graph_shape = -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ngrids grids with interior sizes n[3*g..3*g+2] (cells 0..n-1 per axis, 3
+// ghost cells per side) and spacings dx[3*g..3*g+2].
+int lsmgpu_batch_create(lsmgpu_batch** out, int ngrids, const int* n,
+                        const double* dx, int precision) {
+  const char* R = "lsmgpu_batch_create";
+  clear_error();
+  if (!out || !n || !dx) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null argument");
+    return LSMGPU_ERR_NULL_POINTER;
+  }
+  *out = nullptr;
+  if (ngrids < 1 || (precision != 8 && precision != 4)) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": bad count/precision");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  lsmgpu_batch* b = new lsmgpu_batch();
+  b->ngrids = ngrids;
+  b->prec = precision;
+  b->fp64_kinks = 0;
+  long off = 0;
+  const long align = 256 / precision;
+  for (int g = 0; g < ngrids; g++) {
+    GridMeta m;
+    memset(&m, 0, sizeof m);
+    for (int d = 0; d < 3; d++) {
+      if (n[3 * g + d] < 2 || !(dx[3 * g + d] > 0)) {
+        set_error(LSMGPU_ERR_INVALID_BOX, std::string(R) + ": grid needs >= 2 cells "
+                                                         "per axis and dx > 0");
+        delete b;
+        return LSMGPU_ERR_INVALID_BOX;
+      }
+      m.gb.lo[d] = -3;
+      m.gb.n[d] = n[3 * g + d] + 6;
+      m.fb.lo[d] = 0;
+      m.fb.hi[d] = n[3 * g + d] - 1;
+      m.inv[d] = 1.0 / dx[3 * g + d];
+    }
+    double mx = dx[3 * g] > dx[3 * g + 1] ? dx[3 * g] : dx[3 * g + 1];
+    mx = mx > dx[3 * g + 2] ? mx : dx[3 * g + 2];
+    m.dx_sq = mx * mx;
+    m.offset = off;
+    off += (m.gb.count() + align - 1) / align * align;
+    b->cells += m.fb.count();
+    b->meta.push_back(m);
+  }
+  b->total = off;
+  const size_t bytes = (size_t)off * precision;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  bool ok = cudaMalloc(&b->phi, bytes) == cudaSuccess &&
+            cudaMalloc(&b->phi1, bytes) == cudaSuccess &&
+            cudaMalloc(&b->phi2, bytes) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_meta, sizeof(GridMeta) * ngrids) == cudaSuccess &&
+            cudaMalloc((void**)&b->d_counter, sizeof(unsigned) * 4) == cudaSuccess;
+  // work-lists for every candidate tile shape, largest tiles first
+  for (int s = 0; ok && s < kNumShapes; s++) {
+    std::vector<int4> items;
+    std::vector<long> cost;
+    for (int g = 0; g < ngrids; g++) {
+      const FillBox& f = b->meta[g].fb;
+      const int gx = (f.n(0) + kShapes[s].tx - 1) / kShapes[s].tx;
+      const int gy = (f.n(1) + kShapes[s].ty - 1) / kShapes[s].ty;
+      const int gz = (f.n(2) + kShapes[s].tz - 1) / kShapes[s].tz;
+      for (int z = 0; z < gz; z++)
+        for (int y = 0; y < gy; y++)
+          for (int x = 0; x < gx; x++) {
+            items.push_back(make_int4(g, x, y, z));
+            const long cx = std::min(kShapes[s].tx, f.n(0) - x * kShapes[s].tx);
+            const long cy = std::min(kShapes[s].ty, f.n(1) - y * kShapes[s].ty);
+            const long cz = std::min(kShapes[s].tz, f.n(2) - z * kShapes[s].tz);
+            cost.push_back(cx * cy * cz);
+          }
+    }
+    std::vector<int> order(items.size());
+    for (size_t q = 0; q < order.size(); q++) order[q] = (int)q;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int c) { return cost[a] > cost[c]; });
+    std::vector<int4> sorted(items.size());
+    for (size_t q = 0; q < order.size(); q++) sorted[q] = items[order[q]];
+    b->nitems[s] = (int)sorted.size();
+    ok = cudaMalloc((void**)&b->d_items[s], sizeof(int4) * sorted.size()) == cudaSuccess &&
+         cudaMemcpy(b->d_items[s], sorted.data(), sizeof(int4) * sorted.size(),
+                    cudaMemcpyHostToDevice) == cudaSuccess;
+  }
+  ok = ok && cudaMemset(b->phi, 0, bytes) == cudaSuccess &&
+       cudaMemset(b->phi1, 0, bytes) == cudaSuccess &&
+       cudaMemset(b->phi2, 0, bytes) == cudaSuccess &&
+       cudaMemcpy(b->d_meta, b->meta.data(), sizeof(GridMeta) * ngrids,
+                  cudaMemcpyHostToDevice) == cudaSuccess &&
+       cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    set_error(LSMGPU_ERR_ALLOC, std::string(R) + ": device allocation failed");
+    lsmgpu_batch_destroy(b);
+    return LSMGPU_ERR_ALLOC;
+  }
+  *out = b;
+  return LSMGPU_SUCCESS;
+}
+
+int lsmgpu_batch_destroy(lsmgpu_batch* b) {
+  if (!b) return LSMGPU_SUCCESS;
+  drop_graph(b);
+  void* ps[] = {b->phi, b->phi1, b->phi2, b->d_meta, b->d_counter};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  for (int s = 0; s < kNumShapes; s++)
+    if (b->d_items[s]) cudaFree(b->d_items[s]);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return LSMGPU_SUCCESS;
+}
+
+// element offset of grid g in the packed buffer and its ghost box
+int lsmgpu_batch_grid(lsmgpu_batch* b, int g, long long* offset, int gb[6]) {
+  if (!batch_ok(b, "lsmgpu_batch_grid")) return LSMGPU_ERR_NULL_POINTER;
+  if (g < 0 || g >= b->ngrids) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, "lsmgpu_batch_grid: grid index out of range");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  const GridMeta& m = b->meta[g];
+  if (offset) *offset = m.offset;
+  if (gb)
+    for (int d = 0; d < 3; d++) {
+      gb[2 * d] = m.gb.lo[d];
+      gb[2 * d + 1] = m.gb.hi(d);
+    }
+  return LSMGPU_SUCCESS;
+}
+
+// copy the whole packed phi buffer from/to the host (grid g at its offset)
+int lsmgpu_batch_upload(lsmgpu_batch* b, const void* host) {
+  if (!batch_ok(b, "lsmgpu_batch_upload")) return LSMGPU_ERR_NULL_POINTER;
+  return cuda_ok(cudaMemcpy(b->phi, host, (size_t)b->total * b->prec,
+                            cudaMemcpyHostToDevice),
+                 "lsmgpu_batch_upload")
+             ? LSMGPU_SUCCESS
+             : LSMGPU_ERR_CUDA;
+}
+int lsmgpu_batch_download(lsmgpu_batch* b, void* host) {
+  if (!batch_ok(b, "lsmgpu_batch_download")) return LSMGPU_ERR_NULL_POINTER;
+  if (!cuda_ok(cudaStreamSynchronize(b->stream), "lsmgpu_batch_download"))
+    return LSMGPU_ERR_CUDA;
+  return cuda_ok(cudaMemcpy(host, b->phi, (size_t)b->total * b->prec,
+                            cudaMemcpyDeviceToHost),
+                 "lsmgpu_batch_download")
+             ? LSMGPU_SUCCESS
+             : LSMGPU_ERR_CUDA;
+}
+long long lsmgpu_batch_total_elements(lsmgpu_batch* b) { return b ? b->total : 0; }
+long long lsmgpu_batch_cells(lsmgpu_batch* b) { return b ? b->cells : 0; }
+
+// constant velocity of every grid (3 per grid) and the CFL number: sets each
+// grid's dt = cfl / (|u|/dx + |v|/dy + |w|/dz + tiny)
+int lsmgpu_batch_set_velocity(lsmgpu_batch* b, const double* vel, double cfl) {
+  const char* R = "lsmgpu_batch_set_velocity";
+  if (!batch_ok(b, R)) return LSMGPU_ERR_NULL_POINTER;
+  if (!vel) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null velocity");
+    return LSMGPU_ERR_NULL_POINTER;
+  }
+  const double tiny = b->prec == 8 ? Consts<double>::tiny : (double)Consts<float>::tiny;
+  for (int g = 0; g < b->ngrids; g++) {
+    GridMeta& m = b->meta[g];
+    for (int d = 0; d < 3; d++) m.vel[d] = vel[3 * g + d];
+    const double u = fabs(m.vel[0]) * m.inv[0] + fabs(m.vel[1]) * m.inv[1] +
+                     fabs(m.vel[2]) * m.inv[2];
+    m.dt = cfl / (u + tiny);
+  }
+  drop_graph(b);
+  return cuda_ok(cudaMemcpy(b->d_meta, b->meta.data(), sizeof(GridMeta) * b->ngrids,
+                            cudaMemcpyHostToDevice),
+                 R)
+             ? LSMGPU_SUCCESS
+             : LSMGPU_ERR_CUDA;
+}
+
+int lsmgpu_batch_get_dt(lsmgpu_batch* b, double* dt) {
+  if (!batch_ok(b, "lsmgpu_batch_get_dt") || !dt) return LSMGPU_ERR_NULL_POINTER;
+  for (int g = 0; g < b->ngrids; g++) dt[g] = b->meta[g].dt;
+  return LSMGPU_SUCCESS;
+}
+
+int lsmgpu_batch_set_tile(lsmgpu_batch* b, int shape) {
+  if (!batch_ok(b, "lsmgpu_batch_set_tile")) return LSMGPU_ERR_NULL_POINTER;
+  if (shape < 0 || shape >= kNumShapes) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, "lsmgpu_batch_set_tile: unknown shape");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  if (shape != b->shape) drop_graph(b);
+  b->shape = shape;
+  return LSMGPU_SUCCESS;
+}
+int lsmgpu_batch_get_tile(lsmgpu_batch* b, int* shape, int tile[3]) {
+  if (!batch_ok(b, "lsmgpu_batch_get_tile")) return LSMGPU_ERR_NULL_POINTER;
+  if (shape) *shape = b->shape;
+  if (tile) {
+    tile[0] = kShapes[b->shape].tx;
+    tile[1] = kShapes[b->shape].ty;
+    tile[2] = kShapes[b->shape].tz;
+  }
+  return LSMGPU_SUCCESS;
+}
+// FP32 batches: recompute kink stencils in FP64 (0 off, 1 on)
+int lsmgpu_batch_set_fp64_kinks(lsmgpu_batch* b, int on) {
+  if (!batch_ok(b, "lsmgpu_batch_set_fp64_kinks")) return LSMGPU_ERR_NULL_POINTER;
+  b->fp64_kinks = on ? 1 : 0;
+  drop_graph(b);
+  return LSMGPU_SUCCESS;
+}
+
+// Time one step per tile shape (on a scratch copy of phi, so the batch state
+// is unchanged) and keep the fastest; the choice is cached per (precision,
+// size class).  ms_out[kNumShapes] receives the timings when non-null.
+int lsmgpu_batch_autotune(lsmgpu_batch* b, float* ms_out) {
+  const char* R = "lsmgpu_batch_autotune";
+  if (!batch_ok(b, R)) return LSMGPU_ERR_NULL_POINTER;
+  const std::pair<int, int> key(b->prec, size_class(b));
+  if (!ms_out) {
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) return lsmgpu_batch_set_tile(b, it->second);
+  }
+  const size_t bytes = (size_t)b->total * b->prec;
+  void* save = nullptr;
+  if (!cuda_ok(cudaMalloc(&save, bytes), R)) return LSMGPU_ERR_ALLOC;
+  cudaMemcpyAsync(save, b->phi, bytes, cudaMemcpyDeviceToDevice, b->stream);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int best = b->shape;
+  float best_ms = 1e30f;
+  for (int s = 0; s < kNumShapes; s++) {
+    float ms = 0.f;
+    bool ok = step(b, s, true, b->stream) == cudaSuccess;  // warm-up
+    ok = ok && cudaEventRecord(e0, b->stream) == cudaSuccess;
+    for (int r = 0; ok && r < 3; r++) ok = step(b, s, true, b->stream) == cudaSuccess;
+    ok = ok && cudaEventRecord(e1, b->stream) == cudaSuccess &&
+         cudaEventSynchronize(e1) == cudaSuccess &&
+         cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+    if (!ok) {
+      cuda_ok(cudaGetLastError(), R);
+      break;
+    }
+    if (ms_out) ms_out[s] = ms / 3;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = s;
+    }
+  }
+  cudaMemcpyAsync(b->phi, save, bytes, cudaMemcpyDeviceToDevice, b->stream);
+  cudaStreamSynchronize(b->stream);
+  cudaFree(save);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    g_tune_cache[key] = best;
+  }
+  return lsmgpu_batch_set_tile(b, best);
+}
+
+// nsteps TVD-RK3 steps of every grid.  mode 0: persistent work-list launches
+// replayed from a CUDA graph; 1: the same launches without a graph; 2: one
+// launch per grid per stage (the plain path, for comparison).  Runs on the
+// batch's own stream; waits for completion when ``sync``.
+int lsmgpu_batch_advect_tvdrk3(lsmgpu_batch* b, int nsteps, int mode, int sync) {
+  const char* R = "lsmgpu_batch_advect_tvdrk3";
+  clear_error();
+  if (!batch_ok(b, R)) return LSMGPU_ERR_NULL_POINTER;
+  if (mode == 0) {
+    if (!b->exec || b->graph_shape != b->shape) {
+      drop_graph(b);
+      if (!cuda_ok(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), R))
+        return LSMGPU_ERR_CUDA;
+      const cudaError_t e = step(b, b->shape, true, b->stream);
+      cudaGraph_t g = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+      if (!cuda_ok(e, R) || !cuda_ok(e2, R)) {
+        if (g) cudaGraphDestroy(g);
+        return LSMGPU_ERR_CUDA;
+      }
+      b->graph = g;
+      if (!cuda_ok(cudaGraphInstantiate(&b->exec, b->graph, 0), R)) {
+        drop_graph(b);
+        return LSMGPU_ERR_CUDA;
+      }
+      b->graph_shape = b->shape;
+    }
+    for (int s = 0; s < nsteps; s++) {
+      if (!cuda_ok(cudaGraphLaunch(b->exec, b->stream), R)) return LSMGPU_ERR_CUDA;
+      launch_counter() += 3;
+    }
+  } else {
+    for (int s = 0; s < nsteps; s++)
+      if (!cuda_ok(step(b, b->shape, mode == 1, b->stream), R)) return LSMGPU_ERR_CUDA;
+  }
+  if (sync && !cuda_ok(cudaStreamSynchronize(b->stream), R)) return LSMGPU_ERR_CUDA;
+  return LSMGPU_SUCCESS;
+}
+
+void* lsmgpu_batch_stream(lsmgpu_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+}  // extern "C"

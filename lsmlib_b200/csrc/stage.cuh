@@ -31,7 +31,8 @@ enum StageKind {
   kStageAdvect = 0,    // external velocity arrays: upwind WENO5, -V.grad(phi)
   kStageNormal = 1,    // normal speed array: WENO5 +-, Godunov, -F|grad phi|
   kStageReinit = 2,    // reinitialization RHS, sign from phi_s (or phi0)
-  kStageNormalRhs = 3  // normal speed, writes L(phi) and CFL maxima only
+  kStageNormalRhs = 3, // normal speed, writes L(phi) and CFL maxima only
+  kStageAdvectConst = 4  // constant velocity vel_const: upwind WENO5, -V.grad
 };
 
 template <typename T>
@@ -55,6 +56,7 @@ struct StageParams {
   int rk_kind;         // 1, 22, 32, 33 (see rk_update)
   int use_phi0;
   int fp64_kinks;      // FP32 form: recompute kink stencils in FP64
+  T vel_const[3];      // kStageAdvectConst: the grid's constant velocity
 };
 
 template <typename T>
@@ -72,27 +74,27 @@ template <typename T>
 __device__ __forceinline__ T fetch_bc(const Grid3<const T>& g,
                                       const StageParams<T>& p, int i, int j,
                                       int k) {
-  int c[3] = {i, j, k};
-#pragma unroll
-  for (int d = 0; d < 3; d++) {
-    if (c[d] < p.dom.lo[d] && (p.bc_mask & (1u << (2 * d)))) {
-      const int dist = p.dom.lo[d] - c[d];
-      c[d] = p.dom.lo[d];
-      const T* e = g.ptr(c[0], c[1], c[2]);
-      const T e0 = __ldg(e), e1 = __ldg(e + g.stride(d));
-      const T slope = e0 - e1;
-      return e0 + slope * (T)dist;
-    }
-    if (c[d] > p.dom.hi[d] && (p.bc_mask & (2u << (2 * d)))) {
-      const int dist = c[d] - p.dom.hi[d];
-      c[d] = p.dom.hi[d];
-      const T* e = g.ptr(c[0], c[1], c[2]);
-      const T e0 = __ldg(e), e1 = __ldg(e - g.stride(d));
-      const T slope = e0 - e1;
-      return e0 + slope * (T)dist;
-    }
+  const T* e;
+  long inward;
+  int dist;
+  if (i < p.dom.lo[0] && (p.bc_mask & 1u)) {
+    e = g.ptr(p.dom.lo[0], j, k); inward = 1; dist = p.dom.lo[0] - i;
+  } else if (i > p.dom.hi[0] && (p.bc_mask & 2u)) {
+    e = g.ptr(p.dom.hi[0], j, k); inward = -1; dist = i - p.dom.hi[0];
+  } else if (j < p.dom.lo[1] && (p.bc_mask & 4u)) {
+    e = g.ptr(i, p.dom.lo[1], k); inward = g.sy; dist = p.dom.lo[1] - j;
+  } else if (j > p.dom.hi[1] && (p.bc_mask & 8u)) {
+    e = g.ptr(i, p.dom.hi[1], k); inward = -g.sy; dist = j - p.dom.hi[1];
+  } else if (k < p.dom.lo[2] && (p.bc_mask & 16u)) {
+    e = g.ptr(i, j, p.dom.lo[2]); inward = g.sz; dist = p.dom.lo[2] - k;
+  } else if (k > p.dom.hi[2] && (p.bc_mask & 32u)) {
+    e = g.ptr(i, j, p.dom.hi[2]); inward = -g.sz; dist = k - p.dom.hi[2];
+  } else {
+    return __ldg(g.ptr(i, j, k));
   }
-  return __ldg(g.ptr(i, j, k));
+  const T e0 = __ldg(e), e1 = __ldg(e + inward);
+  const T slope = e0 - e1;
+  return e0 + slope * (T)dist;
 }
 
 // One-sided WENO5 from seven consecutive phi values w[0..6] = phi(c-3..c+3).
@@ -170,7 +172,8 @@ __device__ __forceinline__ T reinit_cell(T pc, T xp, T yp, T zp, T xm, T ym,
     }
     gs[d] = fmax2(gp[d], gm[d]);
   }
-  if (!(fabsT(pc) >= Consts<T>::zero_tol)) return z;
+  // FP64 build's zero_tol for both precisions (see stage_zero_tol)
+  if (!(fabsT(pc) >= T(1.0e-11))) return z;
   const T nsq = gs[0] * gs[0] + gs[1] * gs[1] + gs[2] * gs[2];
   if (sizeof(T) == 4) {
     const double pd = pc, nd = nsq, dd = dx_sq;
@@ -182,14 +185,49 @@ __device__ __forceinline__ T reinit_cell(T pc, T xp, T yp, T zp, T xm, T ym,
   return sgn * (T(1) - sqrtT(nsq));
 }
 
+// Zero tolerance of the fused stages.  The FP32 form keeps the FP64 build's
+// value (configure.ac:268) so that its decisions track the FP64 reference;
+// the reference's single-precision build uses 1e-5 (configure.ac:265), which
+// would switch the reinitialization RHS off at |phi| < 1e-5 where the FP64
+// build keeps it (a difference of a whole pseudo-step dt at such cells).
+template <typename T>
+__device__ __forceinline__ T stage_zero_tol() { return T(1.0e-11); }
+
+// plus and minus WENO5 of one axis from w[0..6] = phi(c-3..c+3)
+template <typename T, bool FAST>
+__device__ __forceinline__ void weno_axis(const T* w, T inv, bool kink64, T& vp,
+                                          T& vm) {
+  if (FAST || sizeof(T) == 4) {
+    if (sizeof(T) == 4 && kink64) weno5_pm_fast<T, true>(w, inv, vp, vm);
+    else weno5_pm_fast<T, false>(w, inv, vp, vm);
+  } else {
+    vp = weno_plus7<T, false>(w, inv);
+    vm = weno_minus7<T, false>(w, inv);
+  }
+}
+
+// one side only (upwind derivative)
+template <typename T, bool FAST>
+__device__ __forceinline__ T weno_upwind_side(const T* w, T inv, bool plus,
+                                              bool kink64) {
+  if (FAST || sizeof(T) == 4) return weno_side<T, true>(w, inv, plus, kink64);
+  return plus ? weno_plus7<T, false>(w, inv) : weno_minus7<T, false>(w, inv);
+}
+
+// One tile of a fused stage: TX x TY cells (tile bx, by) marched over planes
+// [bz*TZ, bz*TZ + TZ) of the fill box.  ``tile`` holds two shared planes:
+// plane k is written into buffer (k-kb)&1 while the other buffer may still be
+// read by slower threads of the previous plane.  Returns the tile's largest
+// CFL speed for kStageNormalRhs (-1 otherwise).  The caller synchronises the
+// block before reusing ``tile``.
 template <typename T, int KIND, bool FAST, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX * TY)
-k_stage(StageParams<T> p) {
-  __shared__ T tile[TY + 6][TX + 6];
+__device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
+                                             int by, int bz,
+                                             T (*tile)[TY + 6][TX + 6]) {
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int i = p.fb.lo[0] + (int)blockIdx.x * TX + tx;
-  const int j = p.fb.lo[1] + (int)blockIdx.y * TY + ty;
-  const int kb = p.fb.lo[2] + (int)blockIdx.z * TZ;
+  const int i = p.fb.lo[0] + bx * TX + tx;
+  const int j = p.fb.lo[1] + by * TY + ty;
+  const int kb = p.fb.lo[2] + bz * TZ;
   const int ke = min(kb + TZ - 1, p.fb.hi[2]);
   const bool act = (i <= p.fb.hi[0]) && (j <= p.fb.hi[1]);
   const Grid3<const T> phi = make_grid(p.phi_s, p.gb);
@@ -197,6 +235,7 @@ k_stage(StageParams<T> p) {
   const long base0 = -((long)p.gb.lo[0] + sy * p.gb.lo[1] + sz * p.gb.lo[2]);
   const T dt = p.dt_dev ? (T)(*p.dt_dev) : (T)p.dt;
   const bool need_bc = p.bc_mask != 0u;
+  const bool kink64 = p.fp64_kinks != 0;
   double hmax = -1.0;
 
   // Tile roles.  Active threads put their own phi(i,j,k) in the tile.  In a
@@ -210,70 +249,87 @@ k_stage(StageParams<T> p) {
   const bool has_hx = (j <= hi1) && ((tx < 3) || (tx >= TX - 3 && i <= hi0));
   const int hj = (ty < 3) ? (j - 3) : (j + 3);
   const bool has_hy = (i <= hi0) && ((ty < 3) || (ty >= TY - 3 && j <= hi1));
+  const int tcol = (tx < 3) ? tx : tx + 6;
+  const int trow = (ty < 3) ? ty : ty + 6;
+
+  auto ld = [&](int a, int b, int c) -> T {
+    return need_bc ? fetch_bc(phi, p, a, b, c) : __ldg(phi.ptr(a, b, c));
+  };
+
+  // registers of the plane to be written next: the new top of the z window
+  // (active threads) or the own cell (halo threads), and the strip cells
+  T nx_c = T(0), nx_hx = T(0), nx_hy = T(0);
+  auto prefetch = [&](int k) {
+    if (act) nx_c = ld(i, j, k + 3);
+    else if (ctr_halo) nx_c = ld(i, j, k);
+    if (has_hx) nx_hx = ld(hx, j, k);
+    if (has_hy) nx_hy = ld(i, hj, k);
+  };
 
   T w[7];
   if (act) {
 #pragma unroll
-    for (int m = 0; m < 6; m++)
-      w[m + 1] = need_bc ? fetch_bc(phi, p, i, j, kb - 3 + m)
-                         : __ldg(phi.ptr(i, j, kb - 3 + m));
+    for (int m = 0; m < 6; m++) w[m + 1] = ld(i, j, kb - 3 + m);
   }
+  prefetch(kb);
   for (int k = kb; k <= ke; ++k) {
+    const int buf = (k - kb) & 1;
     if (act) {
 #pragma unroll
       for (int m = 0; m < 6; m++) w[m] = w[m + 1];
-      w[6] = need_bc ? fetch_bc(phi, p, i, j, k + 3) : __ldg(phi.ptr(i, j, k + 3));
-      tile[ty + 3][tx + 3] = w[3];
+      w[6] = nx_c;
+      tile[buf][ty + 3][tx + 3] = w[3];
     } else if (ctr_halo) {
-      tile[ty + 3][tx + 3] = need_bc ? fetch_bc(phi, p, i, j, k)
-                                     : __ldg(phi.ptr(i, j, k));
+      tile[buf][ty + 3][tx + 3] = nx_c;
     }
-    if (has_hx) {
-      const int tcol = (tx < 3) ? tx : tx + 6;
-      tile[ty + 3][tcol] = need_bc ? fetch_bc(phi, p, hx, j, k)
-                                   : __ldg(phi.ptr(hx, j, k));
-    }
-    if (has_hy) {
-      const int trow = (ty < 3) ? ty : ty + 6;
-      tile[trow][tx + 3] = need_bc ? fetch_bc(phi, p, i, hj, k)
-                                   : __ldg(phi.ptr(i, hj, k));
-    }
+    if (has_hx) tile[buf][ty + 3][tcol] = nx_hx;
+    if (has_hy) tile[buf][trow][tx + 3] = nx_hy;
     __syncthreads();
+    if (k < ke) prefetch(k + 1);
     if (act) {
+      const long o = base0 + (long)i + sy * j + sz * k;
+      // point loads of this cell, issued before the stencil arithmetic
+      T a0 = T(0), a1 = T(0), a2 = T(0), uc = T(0);
+      if (KIND == kStageAdvect) {
+        a0 = __ldg(p.aux0 + o); a1 = __ldg(p.aux1 + o); a2 = __ldg(p.aux2 + o);
+      } else if (KIND == kStageAdvectConst) {
+        a0 = p.vel_const[0]; a1 = p.vel_const[1]; a2 = p.vel_const[2];
+      } else if (KIND == kStageNormal || KIND == kStageNormalRhs ||
+                 (KIND == kStageReinit && p.use_phi0 == 1)) {
+        a0 = __ldg(p.aux0 + o);
+      }
+      if (KIND != kStageNormalRhs && p.rk_kind != 1) uc = __ldg(p.phi_n + o);
       T wx[7], wy[7];
 #pragma unroll
       for (int m = 0; m < 7; m++) {
-        wx[m] = tile[ty + 3][tx + m];
-        wy[m] = tile[ty + m][tx + 3];
+        wx[m] = tile[buf][ty + 3][tx + m];
+        wy[m] = tile[buf][ty + m][tx + 3];
       }
-      const long o = base0 + (long)i + sy * j + sz * k;
+      const T ztol = stage_zero_tol<T>();
       T L;
-      if (KIND == kStageAdvect) {
+      if (KIND == kStageAdvect || KIND == kStageAdvectConst) {
         // LSM3D_UPWIND_HJ_WENO5 + LSM3D_ADD_ADVECTION_TERM_TO_LSE_RHS
-        const T u = __ldg(p.aux0 + o), v = __ldg(p.aux1 + o), ww = __ldg(p.aux2 + o);
         T gx = T(0), gy = T(0), gz = T(0);
-        if (!(fabsT(u) < Consts<T>::zero_tol))
-          gx = weno_side<T, FAST>(wx, p.inv[0], !(u > T(0)), p.fp64_kinks);
-        if (!(fabsT(v) < Consts<T>::zero_tol))
-          gy = weno_side<T, FAST>(wy, p.inv[1], !(v > T(0)), p.fp64_kinks);
-        if (!(fabsT(ww) < Consts<T>::zero_tol))
-          gz = weno_side<T, FAST>(w, p.inv[2], !(ww > T(0)), p.fp64_kinks);
-        L = T(0) - (u * gx + v * gy + ww * gz);
+        if (!(fabsT(a0) < ztol))
+          gx = weno_upwind_side<T, FAST>(wx, p.inv[0], !(a0 > T(0)), kink64);
+        if (!(fabsT(a1) < ztol))
+          gy = weno_upwind_side<T, FAST>(wy, p.inv[1], !(a1 > T(0)), kink64);
+        if (!(fabsT(a2) < ztol))
+          gz = weno_upwind_side<T, FAST>(w, p.inv[2], !(a2 > T(0)), kink64);
+        L = T(0) - (a0 * gx + a1 * gy + a2 * gz);
       } else {
-        const T xp = weno_side<T, FAST>(wx, p.inv[0], true, p.fp64_kinks);
-        const T xm = weno_side<T, FAST>(wx, p.inv[0], false, p.fp64_kinks);
-        const T yp = weno_side<T, FAST>(wy, p.inv[1], true, p.fp64_kinks);
-        const T ym = weno_side<T, FAST>(wy, p.inv[1], false, p.fp64_kinks);
-        const T zp = weno_side<T, FAST>(w, p.inv[2], true, p.fp64_kinks);
-        const T zm = weno_side<T, FAST>(w, p.inv[2], false, p.fp64_kinks);
+        T xp, xm, yp, ym, zp, zm;
+        weno_axis<T, FAST>(wx, p.inv[0], kink64, xp, xm);
+        weno_axis<T, FAST>(wy, p.inv[1], kink64, yp, ym);
+        weno_axis<T, FAST>(w, p.inv[2], kink64, zp, zm);
         if (KIND == kStageReinit) {
-          const T pc = p.use_phi0 == 1 ? __ldg(p.aux0 + o) : w[3];
+          const T pc = p.use_phi0 == 1 ? a0 : w[3];
           L = reinit_cell(pc, xp, yp, zp, xm, ym, zm, p.dx_sq, p.use_phi0 == 1);
         } else {
           // LSM3D_ADD_NORMAL_VEL_TERM_TO_LSE_RHS (:209-231)
-          const T f = __ldg(p.aux0 + o);
+          const T f = a0;
           L = T(0);
-          if (fabsT(f) >= Consts<T>::zero_tol)
+          if (fabsT(f) >= ztol)
             L = T(0) - f * sqrtT(godunov_sq2(f, xp, yp, zp, xm, ym, zm));
           if (KIND == kStageNormalRhs) {
             // LSM3D_COMPUTE_STABLE_NORMAL_VEL_DT per-cell speed (FP64)
@@ -291,12 +347,20 @@ k_stage(StageParams<T> p) {
       if (KIND == kStageNormalRhs) {
         p.rhs_out[o] = L;
       } else {
-        const T uc = (p.rk_kind == 1) ? T(0) : __ldg(p.phi_n + o);
         p.out[o] = rk_combine(p.rk_kind, uc, w[3], L, dt);
       }
     }
-    __syncthreads();
   }
+  return hmax;
+}
+
+template <typename T, int KIND, bool FAST, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TX * TY, 2)
+k_stage(StageParams<T> p) {
+  __shared__ T tile[2][TY + 6][TX + 6];
+  const double hmax = stage_tile<T, KIND, FAST, TX, TY, TZ>(
+      p, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, tile);
+  const int tx = threadIdx.x, ty = threadIdx.y;
   if (KIND == kStageNormalRhs) {
     // block maximum with the reference's "if (h > m) m = h" comparison
     __shared__ double red[TX * TY / 32];

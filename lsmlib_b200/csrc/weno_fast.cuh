@@ -71,6 +71,86 @@ __device__ __forceinline__ T weno5_fast(T v1, T v2, T v3, T v4, T v5) {
   return (n1 * p1 + n2 * p2 + n3 * p3) * r;
 }
 
+// Weights and combination of one side from its smoothness indicators,
+// candidates and eps (see the header comment for the scaled single-reciprocal
+// normalisation).
+template <typename T>
+__device__ __forceinline__ T weno5_weigh(T S1, T S2, T S3, T p1, T p2, T p3,
+                                         T eps) {
+  const T sc = inv_pow2_of(eps);
+  const T es = eps * sc;
+  const T q1 = S1 * sc + es, q2 = S2 * sc + es, q3 = S3 * sc + es;
+  const T Q1 = q1 * q1, Q2 = q2 * q2, Q3 = q3 * q3;
+  const T n1 = T(0.1) * (Q2 * Q3), n2 = T(0.6) * (Q1 * Q3), n3 = T(0.3) * (Q1 * Q2);
+  const T r = rcp_nr(n1 + n2 + n3);
+  return (n1 * p1 + n2 * p2 + n3 * p3) * r;
+}
+
+// Plus and minus HJ-WENO5 derivatives of one axis from seven consecutive
+// values w[0..6] = phi(c-3..c+3), computed together: the six scaled
+// differences V_m = (w[m+1]-w[m])/dx, their squares, the common part of the
+// two eps maxima and two of the three curvature terms (a-2b+c)^2 of each
+// side are shared.  minus uses v1..v5 = V0..V4, plus uses v1..v5 = V5..V1
+// (lsm_spatial_derivatives3d.f.in:1286-1290, :1330-1334).  When KINK64 is
+// set (FP32 form), a side whose smoothness indicators differ by more than a
+// factor 1e3 is recomputed in FP64 from the phi values.
+template <typename T, bool KINK64>
+__device__ __forceinline__ void weno5_pm_fast(const T* w, T inv, T& vp, T& vm) {
+  T V[6], s[6];
+#pragma unroll
+  for (int m = 0; m < 6; m++) {
+    V[m] = (w[m + 1] - w[m]) * inv;
+    s[m] = V[m] * V[m];
+  }
+  const T mid = fmax(fmax(s[1], s[2]), fmax(s[3], s[4]));
+  const T eps_m = T(1e-6) * fmax(mid, s[0]) + Consts<T>::tiny;
+  const T eps_p = T(1e-6) * fmax(mid, s[5]) + Consts<T>::tiny;
+  const T c13_12 = T(13.0 / 12.0), c14 = T(0.25);
+  T t;
+  t = V[0] - T(2) * V[1] + V[2]; const T cA = t * t;
+  t = V[1] - T(2) * V[2] + V[3]; const T cB = t * t;
+  t = V[2] - T(2) * V[3] + V[4]; const T cC = t * t;
+  t = V[3] - T(2) * V[4] + V[5]; const T cD = t * t;
+  // minus side
+  t = V[0] - T(4) * V[1] + T(3) * V[2];
+  const T mS1 = c13_12 * cA + c14 * (t * t);
+  t = V[1] - V[3];
+  const T mS2 = c13_12 * cB + c14 * (t * t);
+  t = T(3) * V[2] - T(4) * V[3] + V[4];
+  const T mS3 = c13_12 * cC + c14 * (t * t);
+  // plus side
+  t = V[5] - T(4) * V[4] + T(3) * V[3];
+  const T pS1 = c13_12 * cD + c14 * (t * t);
+  t = V[4] - V[2];
+  const T pS2 = c13_12 * cC + c14 * (t * t);
+  t = T(3) * V[3] - T(4) * V[2] + V[1];
+  const T pS3 = c13_12 * cB + c14 * (t * t);
+  const T a = T(1.0 / 3.0), b = T(7.0 / 6.0), c = T(11.0 / 6.0), d = T(1.0 / 6.0),
+          e = T(5.0 / 6.0);
+  const T mp1 = a * V[0] - b * V[1] + c * V[2];
+  const T mp2 = -d * V[1] + e * V[2] + a * V[3];
+  const T mp3 = a * V[2] + e * V[3] - d * V[4];
+  const T pp1 = a * V[5] - b * V[4] + c * V[3];
+  const T pp2 = -d * V[4] + e * V[3] + a * V[2];
+  const T pp3 = a * V[3] + e * V[2] - d * V[1];
+  vm = weno5_weigh(mS1, mS2, mS3, mp1, mp2, mp3, eps_m);
+  vp = weno5_weigh(pS1, pS2, pS3, pp1, pp2, pp3, eps_p);
+  if (KINK64) {
+    const T scale = fmax(mid, fmax(s[0], s[5]));
+    const bool km = fmax(fmax(mS1, mS2), mS3) > T(1e3) * fmin(fmin(mS1, mS2), mS3) + T(1e-4) * scale;
+    const bool kp = fmax(fmax(pS1, pS2), pS3) > T(1e3) * fmin(fmin(pS1, pS2), pS3) + T(1e-4) * scale;
+    if (km || kp) {
+      double wd[7];
+#pragma unroll
+      for (int m = 0; m < 7; m++) wd[m] = (double)w[m];
+      double dp, dm;
+      weno5_pm_fast<double, false>(wd, (double)inv, dp, dm);
+      if (km) vm = (T)dm;
+      if (kp) vp = (T)dp;
+    }
+  }
+}
+
 // True when the smoothness indicators of a stencil differ by more than a
 // factor 1e3, i.e. the stencil straddles a kink.  Used by the FP32 form to
 // recompute such values in FP64.

@@ -23,6 +23,21 @@ SIGNATURES = {
     "lsmgpu_normal_tvdrk3": (I, [P, P, P, IA, DA, D, I, I, I, I, I]),
     "lsmgpu_reinit_tvdrk3": (I, [P, P, IA, DA, D, I, I]),
     "lsmgpu_normal_rhs_dt_noalloc": (I, [P, P, P, P, IA, IA, DA, D]),
+    "lsmgpu_batch_create": (I, [ctypes.POINTER(P), I, IA, DA, I]),
+    "lsmgpu_batch_destroy": (I, [P]),
+    "lsmgpu_batch_grid": (I, [P, I, ctypes.POINTER(ctypes.c_longlong), IA]),
+    "lsmgpu_batch_total_elements": (ctypes.c_longlong, [P]),
+    "lsmgpu_batch_cells": (ctypes.c_longlong, [P]),
+    "lsmgpu_batch_upload": (I, [P, P]),
+    "lsmgpu_batch_download": (I, [P, P]),
+    "lsmgpu_batch_set_velocity": (I, [P, DA, D]),
+    "lsmgpu_batch_get_dt": (I, [P, DA]),
+    "lsmgpu_batch_set_tile": (I, [P, I]),
+    "lsmgpu_batch_get_tile": (I, [P, IA, IA]),
+    "lsmgpu_batch_set_fp64_kinks": (I, [P, I]),
+    "lsmgpu_batch_autotune": (I, [P, ctypes.POINTER(ctypes.c_float)]),
+    "lsmgpu_batch_advect_tvdrk3": (I, [P, I, I, I]),
+    "lsmgpu_batch_stream": (P, [P]),
 }
 
 

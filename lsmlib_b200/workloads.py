@@ -76,3 +76,27 @@ def boxes(n, ghost=3):
     gb = (-ghost, n[0] - 1 + ghost, -ghost, n[1] - 1 + ghost, -ghost, n[2] - 1 + ghost)
     fb = (0, n[0] - 1, 0, n[1] - 1, 0, n[2] - 1)
     return gb, fb
+
+
+def config4(ngrids=256, seed=SEED + 4, lo_n=32, hi_n=128):
+    """256 grids, per-axis sizes U{32..128}, each on [-1,1]^3 (dx = 2/n per
+    axis), a union of 1-8 spheres (centres U(-0.6,0.6)^3, radii U(0.1,0.3)),
+    a constant velocity U(-1,1)^3, CFL 0.5, 50 steps."""
+    rng = np.random.default_rng(seed)
+    sizes, dxs, vels, grids = [], [], [], []
+    for _ in range(ngrids):
+        n = tuple(int(v) for v in rng.integers(lo_n, hi_n + 1, size=3))
+        ax, dx = axes(n, (-1, -1, -1), (1, 1, 1))
+        k = int(rng.integers(1, 9))
+        centres = rng.uniform(-0.6, 0.6, size=(k, 3))
+        radii = rng.uniform(0.1, 0.3, size=k)
+        sizes.append(n)
+        dxs.append(tuple(dx))
+        vels.append(tuple(rng.uniform(-1, 1, size=3)))
+        grids.append((ax, centres, radii))
+    return {"sizes": sizes, "dx": dxs, "vel": vels, "grids": grids, "cfl": 0.5,
+            "steps": 50, "seed": seed}
+
+
+def config4_phi(cfg, dtype=np.float64):
+    return [union_of_spheres(ax, c, r, dtype) for ax, c, r in cfg["grids"]]
