@@ -286,6 +286,10 @@ def run_ours(args, world, rank, local, pg):
         lib.lsmgpu_host_free(h_phi)
         lib.lsmgpu_host_free(h_F)
 
+    batched_res = None
+    if not args.no_batched:
+        batched_res = run_batched(lib, pg, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(cfg)
@@ -301,12 +305,69 @@ def run_ours(args, world, rank, local, pg):
                    "fp_mode": "fast (FMA, single-reciprocal WENO5 weights; <=1e-12 rel. vs reference)",
                    "l2": "inputs larger than L2 (144 MB per field, 6 fields live)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "fp32": fp32, "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
+        "fp32": fp32, "batched": batched_res,
+        "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk,
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
     return line
+
+
+def run_batched(lib, pg, world, steps=50, warmup=3):
+    """Config 4: 256 grids of U{32..128}^3 cells, constant velocities, own CFL
+    dt, 50 TVD-RK3 steps; FP64 and FP32 through one persistent work-list
+    launch per stage replayed from a CUDA graph (autotuned tile), and FP64
+    through one launch per grid per stage for comparison."""
+    from lsmlib_b200 import batched, gpu, workloads
+    cfg = workloads.config4()
+    res = {"workload": "256 grids, per-axis U{32..128}, 1-8 spheres, constant "
+                       "velocity U(-1,1)^3, WENO5 + TVD-RK3, CFL 0.5, 50 steps",
+           "grids": len(cfg["sizes"]), "steps": steps}
+    timer = gpu.Timer()
+    finals = {}
+    for prec, key in ((8, "fp64"), (4, "fp32")):
+        dtype = np.float64 if prec == 8 else np.float32
+        b = batched.Batch(cfg["sizes"], cfg["dx"], prec)
+        b.upload(workloads.config4_phi(cfg, dtype))
+        b.set_velocity(cfg["vel"], cfg["cfl"])
+        res["cells"] = int(b.cells)
+        tune = b.autotune(report=True)
+        shape, tile = b.tile()
+        gpu.check_rc(lib.lsmgpu_set_stream(b.stream()), "set_stream")
+        b.advect(warmup, batched.MODE_GRAPH)
+        barrier(pg)
+        timer.start()
+        b.advect(steps, batched.MODE_GRAPH, sync=False)
+        timer.stop()
+        ms = max_over_ranks(pg, timer.ms())
+        finals[key] = np.concatenate([a[3:-3, 3:-3, 3:-3].ravel().astype(np.float64)
+                                      for a in b.download()])
+        entry = {"value": world * b.cells * steps / (ms / 1e3), "unit": UNIT,
+                 "ms_per_step": ms / steps, "tile": list(tile),
+                 "autotune_ms_per_step": [round(t, 4) for t in tune]}
+        if prec == 8:
+            # the plain path: one launch per grid per stage, same kernels
+            b2 = batched.Batch(cfg["sizes"], cfg["dx"], prec)
+            b2.upload(workloads.config4_phi(cfg, dtype))
+            b2.set_velocity(cfg["vel"], cfg["cfl"])
+            b2.set_tile(shape)
+            gpu.check_rc(lib.lsmgpu_set_stream(b2.stream()), "set_stream")
+            b2.advect(warmup, batched.MODE_PER_GRID)
+            timer.start()
+            b2.advect(steps, batched.MODE_PER_GRID, sync=False)
+            timer.stop()
+            ms2 = max_over_ranks(pg, timer.ms())
+            entry["per_grid_launches_value"] = world * b2.cells * steps / (ms2 / 1e3)
+            entry["speedup_vs_per_grid_launches"] = ms2 / ms
+            b2.close()
+        res[key] = entry
+        gpu.check_rc(lib.lsmgpu_set_stream(None), "set_stream")
+        b.close()
+    d = np.abs(finals["fp32"] - finals["fp64"])
+    res["fp32"]["error_vs_fp64"] = {"max_abs": float(d.max()), "l1_mean": float(d.mean()),
+                                    "steps_compared": warmup + steps}
+    return res
 
 
 # ---------------------------------------------------------------------------
@@ -396,21 +457,23 @@ def run_reference(args, world, rank):
 
 
 def profile_kernels():
-    """Two launches each of the FP64 normal-velocity and reinitialization
-    stage kernels (TVD-RK3 stage 2, distinct phi_s and phi^n) on the
-    workload's grid."""
+    """Two launches each of the normal-velocity and reinitialization stage
+    kernels (TVD-RK3 stage 2, distinct phi_s and phi^n) on the workload's
+    grid, in FP64 and then in FP32."""
     from lsmlib_b200 import gpu, integrator, workloads
     cfg = workloads.config2(N_CELLS)
     gb, fb = workloads.boxes(cfg["n"])
     integrator.set_fp_mode(integrator.FP_FAST)
-    a = gpu.DeviceArray(cfg["phi"].shape)
-    b = gpu.DeviceArray.from_host(cfg["phi"])
-    c = gpu.DeviceArray.from_host(cfg["phi"])
-    f = gpu.DeviceArray.from_host(cfg["F"])
-    for kind in (1, 2):
-        for _ in range(2):
-            integrator.stage(kind, 8, a, b, c, [f], gb, fb, cfg["dx"], 1e-3, 32)
-    gpu.check_rc(gpu.load().lsmgpu_stream_synchronize(), "sync")
+    for prec, dtype in ((8, np.float64), (4, np.float32)):
+        a = gpu.DeviceArray(cfg["phi"].shape, dtype)
+        b = gpu.DeviceArray.from_host(cfg["phi"].astype(dtype))
+        c = gpu.DeviceArray.from_host(cfg["phi"].astype(dtype))
+        f = gpu.DeviceArray.from_host(cfg["F"].astype(dtype))
+        for kind in (1, 2):
+            for _ in range(2):
+                integrator.stage(kind, prec, a, b, c, [f], gb, fb, cfg["dx"], 1e-3, 32)
+        gpu.check_rc(gpu.load().lsmgpu_stream_synchronize(), "sync")
+        del a, b, c, f
 
 
 def main():
@@ -423,6 +486,8 @@ def main():
                     help="skip the CPU baseline sample of our arm")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 form")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched uneven-grid leg (config 4)")
     ap.add_argument("--size", type=int, default=256, help="interior cells per axis")
     ap.add_argument("--profile", action="store_true",
                     help="only launch the two fused stage kernels twice each "
