@@ -290,6 +290,10 @@ def run_ours(args, world, rank, local, pg):
     if not args.no_batched:
         batched_res = run_batched(lib, pg, world)
 
+    adjoint_res = None
+    if not args.no_adjoint:
+        adjoint_res = run_adjoint()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(cfg)
@@ -305,13 +309,67 @@ def run_ours(args, world, rank, local, pg):
                    "fp_mode": "fast (FMA, single-reciprocal WENO5 weights; <=1e-12 rel. vs reference)",
                    "l2": "inputs larger than L2 (144 MB per field, 6 fields live)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "fp32": fp32, "batched": batched_res,
+        "fp32": fp32, "batched": batched_res, "adjoint": adjoint_res,
         "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk,
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
     return line
+
+
+def run_adjoint(n_fd=20, h=1e-6):
+    """Config 5: 128^3, B-spline velocity (8^3 x 3 coefficients), 200 steps,
+    checkpoints every 15 steps.  Times the forward run (with its
+    checkpoints) and the reverse sweep (segment recomputation included), and
+    checks dJ/dtheta against central finite differences of the GPU forward
+    model on n_fd seeded coefficients."""
+    from lsmlib_b200 import adjoint, workloads
+    cfg = workloads.config5()
+    p = adjoint.AdvectionAdjoint(cfg["n"], cfg["dx"], cfg["x_lo"], cfg["lattice"],
+                                 cfg["steps"], 15)
+    p.set_theta(cfg["theta"])
+    dt = p.cfl_dt(cfg["cfl"])
+    p.set_dt(dt)
+    p.set_fields(cfg["phi0"], cfg["target"], cfg["eps"])
+    p.forward()
+    p.backward()                        # warm-up
+    fwd, rev = [], []
+    for _ in range(3):
+        loss = p.forward()
+        f, _ = p.timing()
+        gt, gp = p.backward()
+        _, a = p.timing()
+        fwd.append(f)
+        rev.append(a)
+    f, a = min(fwd), min(rev)
+    rng = np.random.default_rng(cfg["seed"])
+    picks = rng.choice(gt.size, n_fd, replace=False)
+    theta = cfg["theta"]
+    worst = 0.0
+    scale = float(np.max(np.abs(gt)))
+    for q in picks:
+        idx = np.unravel_index(q, gt.shape)
+        t = theta.copy()
+        t[idx] += h
+        p.set_theta(t)
+        lp = p.forward()
+        t[idx] -= 2 * h
+        p.set_theta(t)
+        lm = p.forward()
+        fd = (lp - lm) / (2 * h)
+        worst = max(worst, abs(fd - gt[idx]) / max(abs(fd), 1e-3 * scale))
+    p.close()
+    cells = cfg["n"][0] * cfg["n"][1] * cfg["n"][2]
+    return {"workload": "128^3, trilinear B-spline velocity on 8^3 x 3 coefficients, "
+                        "sphere to ellipsoid, WENO5 + TVD-RK3, 200 steps, frozen dt, "
+                        "checkpoints every 15 steps",
+            "loss": loss, "dt": dt, "forward_ms": f, "reverse_ms": a,
+            "reverse_over_forward": a / f, "gradient_over_forward": (f + a) / f,
+            "forward_cell_updates_per_s": cells * cfg["steps"] / (f / 1e3),
+            "fd_check": {"coefficients": n_fd, "h": h,
+                         "max_rel_err": worst,
+                         "rel_err_floor": "1e-3 * max|dJ/dtheta|"}}
 
 
 def run_batched(lib, pg, world, steps=50, warmup=3):
@@ -322,7 +380,8 @@ def run_batched(lib, pg, world, steps=50, warmup=3):
     from lsmlib_b200 import batched, gpu, workloads
     cfg = workloads.config4()
     res = {"workload": "256 grids, per-axis U{32..128}, 1-8 spheres, constant "
-                       "velocity U(-1,1)^3, WENO5 + TVD-RK3, CFL 0.5, 50 steps",
+                       "velocity U(-1,1)^3, WENO5 + TVD-RK3, CFL 0.5, 50 steps, "
+                       "periodic boundaries",
            "grids": len(cfg["sizes"]), "steps": steps}
     timer = gpu.Timer()
     finals = {}
@@ -331,6 +390,7 @@ def run_batched(lib, pg, world, steps=50, warmup=3):
         b = batched.Batch(cfg["sizes"], cfg["dx"], prec)
         b.upload(workloads.config4_phi(cfg, dtype))
         b.set_velocity(cfg["vel"], cfg["cfl"])
+        b.set_bc(batched.BC_PERIODIC)
         res["cells"] = int(b.cells)
         tune = b.autotune(report=True)
         shape, tile = b.tile()
@@ -351,6 +411,7 @@ def run_batched(lib, pg, world, steps=50, warmup=3):
             b2 = batched.Batch(cfg["sizes"], cfg["dx"], prec)
             b2.upload(workloads.config4_phi(cfg, dtype))
             b2.set_velocity(cfg["vel"], cfg["cfl"])
+            b2.set_bc(batched.BC_PERIODIC)
             b2.set_tile(shape)
             gpu.check_rc(lib.lsmgpu_set_stream(b2.stream()), "set_stream")
             b2.advect(warmup, batched.MODE_PER_GRID)
@@ -486,6 +547,8 @@ def main():
                     help="skip the CPU baseline sample of our arm")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 form")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint leg (config 5)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched uneven-grid leg (config 4)")
     ap.add_argument("--size", type=int, default=256, help="interior cells per axis")

@@ -370,10 +370,11 @@ enum {
  * 22 = TVD-RK2 stage 2, 32 = TVD-RK3 stage 2, 33 = TVD-RK3 stage 3 */
 
 /* One fused stage: out = RK(rk_kind, phi_n, phi_s, dt * L(phi_s)) on fb.
- * Faces whose bit is set in bc_mask (bit f for face f = x-lo, x-hi, y-lo,
- * y-hi, z-lo, z-hi) read linear-extrapolation ghost values of phi_s computed
- * on the fly from the domain box dom[6] (NULL: dom = fb); other faces read the
- * ghost cells stored in phi_s.  dt_dev (device, double) overrides dt. */
+ * Faces with a bit set in bc_mask (bit f for face f = x-lo, x-hi, y-lo,
+ * y-hi, z-lo, z-hi: linear extrapolation; bit 8+f: copy extrapolation; bit
+ * 16+f: periodic) read ghost values of phi_s generated on the fly from the
+ * domain box dom[6] (NULL: dom = fb); other faces read the ghost cells
+ * stored in phi_s.  dt_dev (device, double) overrides dt. */
 int lsmgpu_lse_stage(int kind, int precision, void *out, const void *phi_s,
                      const void *phi_n, const void *aux0, const void *aux1,
                      const void *aux2, const int gb[6], const int fb[6],
@@ -392,7 +393,10 @@ typedef struct lsmgpu_workspace lsmgpu_workspace;
 int lsmgpu_workspace_create(lsmgpu_workspace **ws, const int gb[6],
                             int precision);
 int lsmgpu_workspace_destroy(lsmgpu_workspace *ws);
-/* faces using on-the-fly linear extrapolation (the drivers need 0x3f) */
+/* boundary kinds generated on the fly, per face f (0..5 = x-lo, x-hi, y-lo,
+ * y-hi, z-lo, z-hi): bit f linear extrapolation (default 0x3f), bit 8+f copy
+ * extrapolation, bit 16+f periodic (in lo/hi pairs).  The drivers need one
+ * kind on every face. */
 int lsmgpu_workspace_set_bc(lsmgpu_workspace *ws, unsigned linear_faces_mask);
 int lsmgpu_workspace_set_time(lsmgpu_workspace *ws, double t);
 /* waits for the stream; t and the dt of the last step */
@@ -451,6 +455,9 @@ int lsmgpu_batch_get_dt(lsmgpu_batch *b, double *dt);
 int lsmgpu_batch_set_tile(lsmgpu_batch *b, int shape);
 int lsmgpu_batch_get_tile(lsmgpu_batch *b, int *shape, int tile[3]);
 int lsmgpu_batch_set_fp64_kinks(lsmgpu_batch *b, int on);
+/* boundary of every grid: 0 linear extrapolation (default), 1 copy
+ * (homogeneous Neumann), 2 periodic */
+int lsmgpu_batch_set_bc(lsmgpu_batch *b, int kind);
 /* times each tile shape on the batch (state preserved), keeps the fastest;
  * ms_out (optional) receives one time per shape */
 int lsmgpu_batch_autotune(lsmgpu_batch *b, float *ms_out);
@@ -459,6 +466,40 @@ int lsmgpu_batch_autotune(lsmgpu_batch *b, float *ms_out);
 int lsmgpu_batch_advect_tvdrk3(lsmgpu_batch *b, int nsteps, int mode,
                                int sync);
 void *lsmgpu_batch_stream(lsmgpu_batch *b);
+
+/* ---- discrete adjoint --------------------------------------------------------
+ * phi_t + V(x; theta).grad phi = 0 on an n[0] x n[1] x n[2] grid (3 ghost
+ * cells, linear-extrapolation boundaries) over [x_lo, x_lo + n dx], V a
+ * trilinear B-spline on an m^3 lattice spanning the domain, upwind HJ-WENO5 +
+ * TVD-RK3 with a frozen dt, loss J = sum (H(phi_T) - H(target))^2 dx dy dz
+ * with H the smoothed Heaviside LSM_HEAVISIDE of width eps.  The gradient is
+ * the exact transpose of the discrete forward map (upwind side, zero-velocity
+ * cut and the WENO eps argmax frozen as the forward pass chose them), with
+ * the forward states recomputed from checkpoints every ``checkpoint_every``
+ * steps.  FP64.  Arrays passed here are host arrays; theta is [3][m][m][m]
+ * with x fastest. */
+typedef struct lsmgpu_adjoint lsmgpu_adjoint;
+int lsmgpu_adjoint_create(lsmgpu_adjoint **h, const int n[3], const double dx[3],
+                          const double x_lo[3], int lattice, int nsteps,
+                          int checkpoint_every);
+int lsmgpu_adjoint_destroy(lsmgpu_adjoint *h);
+int lsmgpu_adjoint_set_theta(lsmgpu_adjoint *h, const double *theta);
+/* CFL dt of the current velocity (LSM3D_COMPUTE_STABLE_ADVECTION_DT) */
+int lsmgpu_adjoint_cfl_dt(lsmgpu_adjoint *h, double cfl, double *dt);
+int lsmgpu_adjoint_set_dt(lsmgpu_adjoint *h, double dt);
+/* phi0 and target over the ghost box, Heaviside width eps */
+int lsmgpu_adjoint_set_fields(lsmgpu_adjoint *h, const double *phi0,
+                              const double *target, double eps);
+/* forward run from phi0 (keeps the checkpoints and phi_T) and the loss */
+int lsmgpu_adjoint_forward(lsmgpu_adjoint *h, double *loss);
+/* reverse sweep after lsmgpu_adjoint_forward: seed * dJ/dtheta, seed * dJ/dphi0 */
+int lsmgpu_adjoint_backward(lsmgpu_adjoint *h, double seed, double *grad_theta,
+                            double *grad_phi0);
+/* grad_theta: 3*m^3 values; grad_phi0: ghost-box array (interior cells) */
+int lsmgpu_adjoint_gradient(lsmgpu_adjoint *h, double *loss,
+                            double *grad_theta, double *grad_phi0);
+int lsmgpu_adjoint_timing(lsmgpu_adjoint *h, float *fwd_ms, float *adj_ms);
+int lsmgpu_adjoint_phi_final(lsmgpu_adjoint *h, double *host);
 
 /* ---- an entry point that allocates no memory --------------------------------
  * No counterpart in the reference.  For callers that must not allocate device

@@ -13,6 +13,7 @@ from . import gpu
 from .ext_abi import dbls, ints
 
 MODE_GRAPH, MODE_PERSISTENT, MODE_PER_GRID = 0, 1, 2
+BC_LINEAR, BC_COPY, BC_PERIODIC = 0, 1, 2
 
 
 class Batch:
@@ -97,6 +98,9 @@ class Batch:
         gpu.check_rc(gpu.load().lsmgpu_batch_get_tile(self.h, ctypes.byref(s), t),
                      "batch_get_tile")
         return s.value, tuple(t)
+
+    def set_bc(self, kind):
+        gpu.check_rc(gpu.load().lsmgpu_batch_set_bc(self.h, int(kind)), "batch_set_bc")
 
     def set_fp64_kinks(self, on):
         gpu.check_rc(gpu.load().lsmgpu_batch_set_fp64_kinks(self.h, int(on)),

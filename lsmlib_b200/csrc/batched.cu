@@ -51,7 +51,7 @@ template <typename T, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(TX * TY, 2)
 k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ items,
                 int nitems, unsigned* counter, T* out, const T* phi_s,
-                const T* phi_n, int rk_kind, int fp64_kinks) {
+                const T* phi_n, int rk_kind, int fp64_kinks, unsigned bc_mask) {
   __shared__ T tile[2][TY + 6][TX + 6];
   __shared__ int s_item;
   for (;;) {
@@ -73,7 +73,7 @@ k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ ite
     p.gb = g.gb;
     p.fb = g.fb;
     p.dom = g.fb;
-    p.bc_mask = 0x3fu;
+    p.bc_mask = bc_mask;
     for (int d = 0; d < 3; d++) {
       p.inv[d] = (T)g.inv[d];
       p.vel_const[d] = (T)g.vel[d];
@@ -92,7 +92,7 @@ k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ ite
 template <typename T, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(TX * TY, 2)
 k_grid_stage(const GridMeta* __restrict__ grids, int gi, T* out, const T* phi_s,
-             const T* phi_n, int rk_kind, int fp64_kinks) {
+             const T* phi_n, int rk_kind, int fp64_kinks, unsigned bc_mask) {
   __shared__ T tile[2][TY + 6][TX + 6];
   const GridMeta& g = grids[gi];
   StageParams<T> p;
@@ -105,7 +105,7 @@ k_grid_stage(const GridMeta* __restrict__ grids, int gi, T* out, const T* phi_s,
   p.gb = g.gb;
   p.fb = g.fb;
   p.dom = g.fb;
-  p.bc_mask = 0x3fu;
+  p.bc_mask = bc_mask;
   for (int d = 0; d < 3; d++) {
     p.inv[d] = (T)g.inv[d];
     p.vel_const[d] = (T)g.vel[d];
@@ -140,6 +140,7 @@ struct lsmgpu_batch {
   unsigned* d_counter = nullptr;    // three counters, one per stage
   int shape = 1;
   int fp64_kinks = 0;
+  unsigned bc_mask = kBcLinear;
   int blocks_per_sm = 2;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
@@ -168,13 +169,13 @@ cudaError_t launch_shape(lsmgpu_batch* b, int shape, bool batched, int rk_kind,
     if (batched) {                                                                 \
       k_batched_stage<T, TX, TY, TZ><<<grid, dim3(TX, TY), 0, st>>>(               \
           b->d_meta, b->d_items[I], b->nitems[I], counter, out, in, base, rk_kind, \
-          b->fp64_kinks);                                                          \
+          b->fp64_kinks, b->bc_mask);                                              \
     } else {                                                                       \
       for (int gi = 0; gi < b->ngrids; gi++) {                                     \
         const FillBox& f = b->meta[gi].fb;                                         \
         dim3 g((f.n(0) + TX - 1) / TX, (f.n(1) + TY - 1) / TY, (f.n(2) + TZ - 1) / TZ); \
         k_grid_stage<T, TX, TY, TZ><<<g, dim3(TX, TY), 0, st>>>(                   \
-            b->d_meta, gi, out, in, base, rk_kind, b->fp64_kinks);                 \
+            b->d_meta, gi, out, in, base, rk_kind, b->fp64_kinks, b->bc_mask);     \
       }                                                                            \
     }                                                                              \
     break;
@@ -433,6 +434,19 @@ int lsmgpu_batch_get_tile(lsmgpu_batch* b, int* shape, int tile[3]) {
   }
   return LSMGPU_SUCCESS;
 }
+// boundary kind of every grid: 0 linear extrapolation, 1 copy (homogeneous
+// Neumann), 2 periodic
+int lsmgpu_batch_set_bc(lsmgpu_batch* b, int kind) {
+  if (!batch_ok(b, "lsmgpu_batch_set_bc")) return LSMGPU_ERR_NULL_POINTER;
+  if (kind < 0 || kind > 2) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, "lsmgpu_batch_set_bc: kind is 0, 1 or 2");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  b->bc_mask = kind == 0 ? kBcLinear : (kind == 1 ? kBcCopy : kBcPeriodic);
+  drop_graph(b);
+  return LSMGPU_SUCCESS;
+}
+
 // FP32 batches: recompute kink stencils in FP64 (0 off, 1 on)
 int lsmgpu_batch_set_fp64_kinks(lsmgpu_batch* b, int on) {
   if (!batch_ok(b, "lsmgpu_batch_set_fp64_kinks")) return LSMGPU_ERR_NULL_POINTER;

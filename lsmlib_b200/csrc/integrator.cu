@@ -129,6 +129,19 @@ __global__ void k_adv_partials(const T* vx, const T* vy, const T* vz, Box gb,
 
 constexpr int kAdvRedBlocks = 1184;
 
+// A boundary mask (stage.cuh: bit f linear, 8+f copy, 16+f periodic) is
+// usable by the multi-step drivers when every face has exactly one kind and
+// periodic faces come in lo/hi pairs.
+bool bc_mask_complete(unsigned m) {
+  for (int f = 0; f < 6; f++) {
+    const int kinds = ((m >> f) & 1u) + ((m >> (8 + f)) & 1u) + ((m >> (16 + f)) & 1u);
+    if (kinds != 1) return false;
+  }
+  for (int d = 0; d < 3; d++)
+    if (((m >> (16 + 2 * d)) & 1u) != ((m >> (17 + 2 * d)) & 1u)) return false;
+  return true;
+}
+
 bool ws_ok(lsmgpu_workspace* ws, const char* R) {
   if (!ws) {
     set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null workspace");
@@ -236,10 +249,10 @@ bool common_checks(lsmgpu_workspace* ws, const void* phi, const int* fb,
     set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": dx must be positive");
     return false;
   }
-  if (ws->bc_mask != 0x3fu) {
+  if (!bc_mask_complete(ws->bc_mask)) {
     set_error(LSMGPU_ERR_INVALID_VALUE,
-              std::string(R) + ": multi-step drivers need the linear "
-                               "extrapolation on all six faces");
+              std::string(R) + ": multi-step drivers need one generated "
+                               "boundary kind on every face (periodic in pairs)");
     return false;
   }
   return true;
@@ -306,8 +319,9 @@ int lsmgpu_workspace_destroy(lsmgpu_workspace* ws) {
 }
 
 int lsmgpu_workspace_set_bc(lsmgpu_workspace* ws, unsigned linear_faces_mask) {
+  // bits 0-5 linear, 8-13 copy, 16-21 periodic (face f = x-lo .. z-hi)
   if (!ws_ok(ws, "lsmgpu_workspace_set_bc")) return LSMGPU_ERR_NULL_POINTER;
-  ws->bc_mask = linear_faces_mask & 0x3fu;
+  ws->bc_mask = linear_faces_mask & (kBcLinear | kBcCopy | kBcPeriodic);
   return LSMGPU_SUCCESS;
 }
 
@@ -368,7 +382,13 @@ int lsmgpu_lse_stage(int kind, int precision, void* out, const void* phi_s,
   memset(&a, 0, sizeof a);
   a.gb = g;
   a.fb = f;
-  a.bc_mask = bc_mask & 0x3fu;
+  a.bc_mask = bc_mask & (kBcLinear | kBcCopy | kBcPeriodic);
+  for (int d = 0; d < 3; d++)
+    if (((a.bc_mask >> (16 + 2 * d)) & 1u) != ((a.bc_mask >> (17 + 2 * d)) & 1u)) {
+      set_error(LSMGPU_ERR_INVALID_VALUE,
+                std::string(R) + ": periodic faces come in lo/hi pairs");
+      return LSMGPU_ERR_INVALID_VALUE;
+    }
   a.dom = dom ? fb6(dom) : f;
   if (a.bc_mask) {
     for (int d = 0; d < 3; d++)

@@ -69,11 +69,37 @@ __device__ __forceinline__ T rk_combine(int kind, T uc, T us, T r, T dt) {
   }
 }
 
+// Boundary kinds per face f (0..5 = x-lo, x-hi, y-lo, y-hi, z-lo, z-hi) in
+// StageParams::bc_mask: bit f = linear extrapolation
+// (lsm_boundary_conditions3d.f:46-170), bit 8+f = copy extrapolation
+// (homogeneous Neumann, :352-463), bit 16+f = periodic; no bit = the ghost
+// cells stored in the array.
+constexpr unsigned kBcLinear = 0x3fu, kBcCopy = 0x3fu << 8, kBcPeriodic = 0x3fu << 16;
+
 // phi at (i,j,k) where at most one coordinate may lie outside the domain box
 template <typename T>
 __device__ __forceinline__ T fetch_bc(const Grid3<const T>& g,
                                       const StageParams<T>& p, int i, int j,
                                       int k) {
+  const unsigned m = p.bc_mask;
+  if (m & kBcPeriodic) {
+    const int nx = p.dom.hi[0] - p.dom.lo[0] + 1, ny = p.dom.hi[1] - p.dom.lo[1] + 1,
+              nz = p.dom.hi[2] - p.dom.lo[2] + 1;
+    if (i < p.dom.lo[0] && (m & (1u << 16))) return __ldg(g.ptr(i + nx, j, k));
+    if (i > p.dom.hi[0] && (m & (2u << 16))) return __ldg(g.ptr(i - nx, j, k));
+    if (j < p.dom.lo[1] && (m & (4u << 16))) return __ldg(g.ptr(i, j + ny, k));
+    if (j > p.dom.hi[1] && (m & (8u << 16))) return __ldg(g.ptr(i, j - ny, k));
+    if (k < p.dom.lo[2] && (m & (16u << 16))) return __ldg(g.ptr(i, j, k + nz));
+    if (k > p.dom.hi[2] && (m & (32u << 16))) return __ldg(g.ptr(i, j, k - nz));
+  }
+  if (m & kBcCopy) {
+    if (i < p.dom.lo[0] && (m & (1u << 8))) return __ldg(g.ptr(p.dom.lo[0], j, k));
+    if (i > p.dom.hi[0] && (m & (2u << 8))) return __ldg(g.ptr(p.dom.hi[0], j, k));
+    if (j < p.dom.lo[1] && (m & (4u << 8))) return __ldg(g.ptr(i, p.dom.lo[1], k));
+    if (j > p.dom.hi[1] && (m & (8u << 8))) return __ldg(g.ptr(i, p.dom.hi[1], k));
+    if (k < p.dom.lo[2] && (m & (16u << 8))) return __ldg(g.ptr(i, j, p.dom.lo[2]));
+    if (k > p.dom.hi[2] && (m & (32u << 8))) return __ldg(g.ptr(i, j, p.dom.hi[2]));
+  }
   const T* e;
   long inward;
   int dist;
@@ -234,7 +260,14 @@ __device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
   const long sy = p.gb.sy(), sz = p.gb.sz();
   const long base0 = -((long)p.gb.lo[0] + sy * p.gb.lo[1] + sz * p.gb.lo[2]);
   const T dt = p.dt_dev ? (T)(*p.dt_dev) : (T)p.dt;
-  const bool need_bc = p.bc_mask != 0u;
+  // Boundary values are generated only by tiles whose stencil reaches past
+  // the domain box; every other tile loads directly (block-uniform test).
+  const int xlo = p.fb.lo[0] + bx * TX - 3, xhi = min(p.fb.lo[0] + bx * TX + TX - 1, p.fb.hi[0]) + 3;
+  const int ylo = p.fb.lo[1] + by * TY - 3, yhi = min(p.fb.lo[1] + by * TY + TY - 1, p.fb.hi[1]) + 3;
+  const bool inside = xlo >= p.dom.lo[0] && xhi <= p.dom.hi[0] && ylo >= p.dom.lo[1] &&
+                      yhi <= p.dom.hi[1] && kb - 3 >= p.dom.lo[2] &&
+                      ke + 3 <= p.dom.hi[2];
+  const bool need_bc = p.bc_mask != 0u && !inside;
   const bool kink64 = p.fp64_kinks != 0;
   double hmax = -1.0;
 

@@ -35,6 +35,7 @@ SIGNATURES = {
     "lsmgpu_batch_set_tile": (I, [P, I]),
     "lsmgpu_batch_get_tile": (I, [P, IA, IA]),
     "lsmgpu_batch_set_fp64_kinks": (I, [P, I]),
+    "lsmgpu_batch_set_bc": (I, [P, I]),
     "lsmgpu_batch_autotune": (I, [P, ctypes.POINTER(ctypes.c_float)]),
     "lsmgpu_batch_advect_tvdrk3": (I, [P, I, I, I]),
     "lsmgpu_batch_stream": (P, [P]),
@@ -47,3 +48,19 @@ def ints(v):
 
 def dbls(v):
     return (ctypes.c_double * len(v))(*[float(x) for x in v])
+
+DP = ctypes.POINTER(ctypes.c_double)
+FP = ctypes.POINTER(ctypes.c_float)
+SIGNATURES.update({
+    "lsmgpu_adjoint_create": (I, [ctypes.POINTER(P), IA, DA, DA, I, I, I]),
+    "lsmgpu_adjoint_destroy": (I, [P]),
+    "lsmgpu_adjoint_set_theta": (I, [P, P]),
+    "lsmgpu_adjoint_cfl_dt": (I, [P, D, DP]),
+    "lsmgpu_adjoint_set_dt": (I, [P, D]),
+    "lsmgpu_adjoint_set_fields": (I, [P, P, P, D]),
+    "lsmgpu_adjoint_forward": (I, [P, DP]),
+    "lsmgpu_adjoint_backward": (I, [P, D, P, P]),
+    "lsmgpu_adjoint_gradient": (I, [P, DP, P, P]),
+    "lsmgpu_adjoint_timing": (I, [P, FP, FP]),
+    "lsmgpu_adjoint_phi_final": (I, [P, P]),
+})

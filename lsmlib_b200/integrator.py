@@ -20,6 +20,8 @@ from . import gpu
 from .ext_abi import dbls, ints
 
 FP_STRICT, FP_FAST = 0, 1
+# boundary masks (per face f = x-lo .. z-hi): linear, copy, periodic
+BC_LINEAR, BC_COPY, BC_PERIODIC = 0x3F, 0x3F << 8, 0x3F << 16
 
 
 def set_fp_mode(mode):
@@ -50,6 +52,9 @@ class Workspace:
             self.close()
         except Exception:
             pass
+
+    def set_bc(self, mask):
+        gpu.check_rc(gpu.load().lsmgpu_workspace_set_bc(self.h, int(mask)), "set_bc")
 
     def set_time(self, t):
         gpu.check_rc(gpu.load().lsmgpu_workspace_set_time(self.h, float(t)), "set_time")

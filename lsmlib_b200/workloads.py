@@ -81,7 +81,8 @@ def boxes(n, ghost=3):
 def config4(ngrids=256, seed=SEED + 4, lo_n=32, hi_n=128):
     """256 grids, per-axis sizes U{32..128}, each on [-1,1]^3 (dx = 2/n per
     axis), a union of 1-8 spheres (centres U(-0.6,0.6)^3, radii U(0.1,0.3)),
-    a constant velocity U(-1,1)^3, CFL 0.5, 50 steps."""
+    a constant velocity U(-1,1)^3, CFL 0.5, 50 steps, periodic boundaries
+    (the boundary condition of the reference's 3D advection example)."""
     rng = np.random.default_rng(seed)
     sizes, dxs, vels, grids = [], [], [], []
     for _ in range(ngrids):
@@ -95,8 +96,28 @@ def config4(ngrids=256, seed=SEED + 4, lo_n=32, hi_n=128):
         vels.append(tuple(rng.uniform(-1, 1, size=3)))
         grids.append((ax, centres, radii))
     return {"sizes": sizes, "dx": dxs, "vel": vels, "grids": grids, "cfl": 0.5,
-            "steps": 50, "seed": seed}
+            "steps": 50, "seed": seed, "bc": "periodic"}
 
 
 def config4_phi(cfg, dtype=np.float64):
     return [union_of_spheres(ax, c, r, dtype) for ax, c, r in cfg["grids"]]
+
+
+def config5(n=128, lattice=8, seed=SEED + 5):
+    """128^3 on [-1,1]^3; velocity a trilinear B-spline on a lattice^3
+    lattice spanning the domain, coefficients N(0, 0.5^2); phi0 a sphere of
+    radius 0.3 at the origin; target an ellipsoid with semi-axes
+    (0.4, 0.3, 0.25), implicit function scaled by the smallest semi-axis;
+    200 steps, dt frozen at the CFL 0.5 value of t = 0; Heaviside width
+    1.5 dx."""
+    rng = np.random.default_rng(seed)
+    ax, dx = axes((n, n, n), (-1, -1, -1), (1, 1, 1))
+    theta = rng.normal(0.0, 0.5, size=(3, lattice, lattice, lattice))
+    phi0 = union_of_spheres(ax, [(0.0, 0.0, 0.0)], [0.3])
+    x = ax[0][:, None, None]
+    y = ax[1][None, :, None]
+    z = ax[2][None, None, :]
+    target = (np.sqrt((x / 0.4) ** 2 + (y / 0.3) ** 2 + (z / 0.25) ** 2) - 1.0) * 0.25
+    return {"n": (n, n, n), "dx": dx, "x_lo": (-1.0, -1.0, -1.0), "lattice": lattice,
+            "theta": theta, "phi0": phi0, "target": np.asfortranarray(target),
+            "steps": 200, "cfl": 0.5, "eps": 1.5 * dx[0], "seed": seed}

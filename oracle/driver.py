@@ -74,8 +74,8 @@ class Grid:
 class Stepper:
     """Reference-order TVD-RK3 loops over one toolbox and one grid."""
 
-    def __init__(self, tb, grid):
-        self.tb, self.g = tb, grid
+    def __init__(self, tb, grid, bc="linear"):
+        self.tb, self.g, self.bc = tb, grid, bc
         self.rhs = grid.zeros()
         self.grads = {k: grid.zeros() for k in GRADS_PM}
         self.up = {k: grid.zeros() for k in ("phi_x", "phi_y", "phi_z")}
@@ -84,9 +84,27 @@ class Stepper:
 
     # -- building blocks ----------------------------------------------------
     def ghost_fill(self, phi):
+        """Ghost cells of all six faces in the reference's face order: linear
+        extrapolation (LSM3D_LINEAR_EXTRAPOLATION), copy extrapolation
+        (LSM3D_COPY_EXTRAPOLATION) or periodic images (the periodic domains
+        of the reference's SAMRAI examples, e.g.
+        examples/parallel/3d/advection/advection_3d.input:48)."""
+        if self.bc == "periodic":
+            g = self.g.ghost
+            a = phi.data
+            for ax in range(3):
+                n = self.g.n[ax]
+                sl = [slice(None)] * 3
+                src = [slice(None)] * 3
+                sl[ax], src[ax] = slice(0, g), slice(n, n + g)
+                a[tuple(sl)] = a[tuple(src)]
+                sl[ax], src[ax] = slice(n + g, n + 2 * g), slice(g, 2 * g)
+                a[tuple(sl)] = a[tuple(src)]
+            return
+        sym = ("lsm3dcopyextrapolation_" if self.bc == "copy"
+               else "lsm3dlinearextrapolation_")
         for face in range(6):
-            self.tb.call("lsm3dlinearextrapolation_", {"phi": phi}, self.g.fb,
-                         bdry_location_idx=face)
+            self.tb.call(sym, {"phi": phi}, self.g.fb, bdry_location_idx=face)
 
     def weno_pm(self, phi):
         f = dict(self.grads)

@@ -104,3 +104,27 @@ def test_fp32_batch_error_against_fp64():
         res[prec] = np.concatenate([a[3:-3, 3:-3, 3:-3].ravel().astype(np.float64)
                                     for a in b.download()])
     assert np.max(np.abs(res[4] - res[8])) <= 1e-5
+
+
+@pytest.mark.parametrize("bc", [1, 2])
+def test_batched_copy_and_periodic_boundaries(bc):
+    from lsmlib_b200 import batched, workloads
+    cfg = small_batch(seed=17, ngrids=4)
+    phis = workloads.config4_phi(cfg)
+    b = batched.Batch(cfg["sizes"], cfg["dx"], 8)
+    b.upload(phis)
+    b.set_velocity(cfg["vel"], 0.5)
+    b.set_bc(bc)
+    dts = b.dt()
+    b.advect(2, batched.MODE_GRAPH)
+    got = b.download()
+    for g, (n, dx, v) in enumerate(zip(cfg["sizes"], cfg["dx"], cfg["vel"])):
+        grid = Grid(n, dx=dx)
+        phi = grid.field(phis[g])
+        vel = [grid.field(np.full(grid.shape, c)) for c in v]
+        st = Stepper(oracle.oracle_toolbox(), grid, bc="copy" if bc == 1 else "periodic")
+        for _ in range(2):
+            st.advect_step(phi, lambda c: vel, dts[g])
+        want = grid.interior(phi)
+        have = grid.interior(grid.field(got[g]))
+        assert np.max(np.abs(have - want)) <= 1e-12 * np.max(np.abs(want)), g

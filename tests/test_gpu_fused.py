@@ -224,3 +224,52 @@ def test_fp32_form_error_against_fp64():
     got = g.interior(g.field(d.download().astype(np.float64)))
     err = np.abs(got - g.interior(ref))
     assert err.max() <= ABS_FP32, err.max()
+
+
+@pytest.mark.parametrize("bc", ["copy", "periodic"])
+def test_generated_boundary_kinds(mode, bc):
+    """Copy extrapolation (homogeneous Neumann) and periodic ghost values are
+    generated on the fly like the linear ones."""
+    from lsmlib_b200 import gpu, integrator
+    rng = np.random.default_rng(21)
+    g = Grid((30, 19, 26), dx=(0.07, 0.06, 0.08))
+    phi0 = spheres(g, (-1.0, -0.6, -1.0), seed=9, count=4)
+    vel = [g.field(np.full(g.shape, c)) for c in rng.uniform(-1, 1, 3)]
+    st = Stepper(oracle.oracle_toolbox(), g, bc=bc)
+    ref = g.field(phi0)
+    dt = st.advect_dt(vel, 0.5)
+    for _ in range(3):
+        st.advect_step(ref, lambda c: vel, dt)
+    ws = integrator.Workspace(g.gb, 8)
+    ws.set_bc(integrator.BC_COPY if bc == "copy" else integrator.BC_PERIODIC)
+    d = gpu.DeviceArray.from_host(phi0)
+    dv = [gpu.DeviceArray.from_host(v.data) for v in vel]
+    ws.advect(d, dv, g.fb, g.dx, cfl=0.5, nsteps=3)
+    check(mode, g.interior(g.field(d.download())), g.interior(ref))
+
+
+def test_config1_full_run_strict_matches_oracle():
+    """The reference's CPU-runnable case end to end: 64^3 on [-1,1]^3, sphere
+    r = 0.25 at (0.1,-0.05,0), velocity (1, 0.5, 0.25) stored as arrays, CFL
+    0.5, 100 TVD-RK3 steps with linear-extrapolation ghosts -- strict GPU
+    arithmetic equals the oracle's reference-order chain bit for bit."""
+    from lsmlib_b200 import gpu, integrator, workloads
+    cfg = workloads.config1()
+    g = Grid(cfg["n"], dx=cfg["dx"])
+    vel = [g.field(v) for v in cfg["vel"]]
+    st = Stepper(oracle.oracle_toolbox(), g)
+    ref = g.field(cfg["phi"].copy(order="F"))  # the oracle steps in place
+    dt = st.advect_dt(vel, cfg["cfl"])
+    for _ in range(cfg["steps"]):
+        st.advect_step(ref, lambda c: vel, dt)
+    prev = integrator.get_fp_mode()
+    integrator.set_fp_mode(integrator.FP_STRICT)
+    try:
+        ws = integrator.Workspace(g.gb, 8)
+        d = gpu.DeviceArray.from_host(cfg["phi"])
+        dv = [gpu.DeviceArray.from_host(v) for v in cfg["vel"]]
+        ws.advect(d, dv, g.fb, g.dx, cfl=cfg["cfl"], nsteps=cfg["steps"])
+        got = g.interior(g.field(d.download()))
+    finally:
+        integrator.set_fp_mode(prev)
+    assert same_bits(got, g.interior(ref))
