@@ -398,6 +398,15 @@ int lsmgpu_workspace_destroy(lsmgpu_workspace *ws);
  * extrapolation, bit 16+f periodic (in lo/hi pairs).  The drivers need one
  * kind on every face. */
 int lsmgpu_workspace_set_bc(lsmgpu_workspace *ws, unsigned linear_faces_mask);
+/* FP64 parts of an FP32 workspace (no effect on FP64): bit 0 recomputes in
+ * FP64 the WENO5 stencils whose smoothness indicators differ by more than a
+ * factor 1e3 (kinks), bit 1 evaluates the smoothed sign of the
+ * reinitialization RHS in FP64, bit 2 forms each Runge-Kutta combination in
+ * FP64 and rounds it to FP32 stochastically (unbiased; seeded per launch
+ * from a per-workspace counter, so a run is reproducible).  Default 6.  No
+ * reference counterpart: the reference's single-precision build is FP32
+ * throughout. */
+int lsmgpu_workspace_set_fp64_policy(lsmgpu_workspace *ws, int policy);
 int lsmgpu_workspace_set_time(lsmgpu_workspace *ws, double t);
 /* waits for the stream; t and the dt of the last step */
 int lsmgpu_workspace_get_time(lsmgpu_workspace *ws, double *t,
@@ -455,6 +464,10 @@ int lsmgpu_batch_get_dt(lsmgpu_batch *b, double *dt);
 int lsmgpu_batch_set_tile(lsmgpu_batch *b, int shape);
 int lsmgpu_batch_get_tile(lsmgpu_batch *b, int *shape, int tile[3]);
 int lsmgpu_batch_set_fp64_kinks(lsmgpu_batch *b, int on);
+/* FP32 batches: bit 0 as lsmgpu_batch_set_fp64_kinks, bit 2 stochastic
+ * rounding of the stage outputs (see lsmgpu_workspace_set_fp64_policy).
+ * Default 4.  Drops the captured graph. */
+int lsmgpu_batch_set_fp64_policy(lsmgpu_batch *b, int policy);
 /* boundary of every grid: 0 linear extrapolation (default), 1 copy
  * (homogeneous Neumann), 2 periodic */
 int lsmgpu_batch_set_bc(lsmgpu_batch *b, int kind);

@@ -102,6 +102,11 @@ class Batch:
     def set_bc(self, kind):
         gpu.check_rc(gpu.load().lsmgpu_batch_set_bc(self.h, int(kind)), "batch_set_bc")
 
+    def set_fp64_policy(self, policy):
+        """FP32 batches: integrator.FP64_KINKS | integrator.STOCH_ROUND."""
+        gpu.check_rc(gpu.load().lsmgpu_batch_set_fp64_policy(self.h, int(policy)),
+                     "batch_set_fp64_policy")
+
     def set_fp64_kinks(self, on):
         gpu.check_rc(gpu.load().lsmgpu_batch_set_fp64_kinks(self.h, int(on)),
                      "batch_set_fp64_kinks")

@@ -47,11 +47,24 @@ constexpr TileShape kShapes[] = {{32, 8, 16}, {32, 8, 32}, {32, 8, 64}, {16, 8, 
                                  {16, 8, 32}};
 constexpr int kNumShapes = 5;
 
+// seed of the stochastic rounding of one stage: the step number kept on the
+// device (bumped at the end of every step, so that graph replays differ)
+// and the stage
+template <typename T>
+__device__ __forceinline__ unsigned batch_sr_seed(int policy, const unsigned* sr_step,
+                                                  int rk_kind) {
+  if (sizeof(T) != 4 || !(policy & kStochRound) || !sr_step) return 0u;
+  return sr_hash(*sr_step * 64u + (unsigned)rk_kind) | 1u;
+}
+
+__global__ void k_bump(unsigned* c) { *c += 1u; }
+
 template <typename T, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(TX * TY, 2)
 k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ items,
                 int nitems, unsigned* counter, T* out, const T* phi_s,
-                const T* phi_n, int rk_kind, int fp64_kinks, unsigned bc_mask) {
+                const T* phi_n, int rk_kind, int policy, const unsigned* sr_step,
+                unsigned bc_mask) {
   __shared__ T tile[2][TY + 6][TX + 6];
   __shared__ int s_item;
   for (;;) {
@@ -83,7 +96,8 @@ k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ ite
     p.dt = g.dt;
     p.rk_kind = rk_kind;
     p.use_phi0 = 0;
-    p.fp64_kinks = fp64_kinks;
+    p.fp64_policy = policy & kFp64Kinks;
+    p.sr_seed = batch_sr_seed<T>(policy, sr_step, rk_kind);
     stage_tile<T, kStageAdvectConst, true, TX, TY, TZ>(p, it.y, it.z, it.w, tile);
   }
 }
@@ -92,7 +106,8 @@ k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ ite
 template <typename T, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(TX * TY, 2)
 k_grid_stage(const GridMeta* __restrict__ grids, int gi, T* out, const T* phi_s,
-             const T* phi_n, int rk_kind, int fp64_kinks, unsigned bc_mask) {
+             const T* phi_n, int rk_kind, int policy, const unsigned* sr_step,
+             unsigned bc_mask) {
   __shared__ T tile[2][TY + 6][TX + 6];
   const GridMeta& g = grids[gi];
   StageParams<T> p;
@@ -115,7 +130,8 @@ k_grid_stage(const GridMeta* __restrict__ grids, int gi, T* out, const T* phi_s,
   p.dt = g.dt;
   p.rk_kind = rk_kind;
   p.use_phi0 = 0;
-  p.fp64_kinks = fp64_kinks;
+  p.fp64_policy = policy & kFp64Kinks;
+  p.sr_seed = batch_sr_seed<T>(policy, sr_step, rk_kind);
   stage_tile<T, kStageAdvectConst, true, TX, TY, TZ>(p, (int)blockIdx.x, (int)blockIdx.y,
                                                      (int)blockIdx.z, tile);
 }
@@ -137,9 +153,9 @@ struct lsmgpu_batch {
   void* phi2 = nullptr;
   int4* d_items[kNumShapes] = {nullptr};
   int nitems[kNumShapes] = {0};
-  unsigned* d_counter = nullptr;    // three counters, one per stage
+  unsigned* d_counter = nullptr;    // three tile counters (one per stage), step
   int shape = 1;
-  int fp64_kinks = 0;
+  int policy = kStochRound;         // FP32: kFp64Kinks | kStochRound
   unsigned bc_mask = kBcLinear;
   int blocks_per_sm = 2;
   int num_sms = 148;
@@ -169,13 +185,14 @@ cudaError_t launch_shape(lsmgpu_batch* b, int shape, bool batched, int rk_kind,
     if (batched) {                                                                 \
       k_batched_stage<T, TX, TY, TZ><<<grid, dim3(TX, TY), 0, st>>>(               \
           b->d_meta, b->d_items[I], b->nitems[I], counter, out, in, base, rk_kind, \
-          b->fp64_kinks, b->bc_mask);                                              \
+          b->policy, b->d_counter + 3, b->bc_mask);                                \
     } else {                                                                       \
       for (int gi = 0; gi < b->ngrids; gi++) {                                     \
         const FillBox& f = b->meta[gi].fb;                                         \
         dim3 g((f.n(0) + TX - 1) / TX, (f.n(1) + TY - 1) / TY, (f.n(2) + TZ - 1) / TZ); \
         k_grid_stage<T, TX, TY, TZ><<<g, dim3(TX, TY), 0, st>>>(                   \
-            b->d_meta, gi, out, in, base, rk_kind, b->fp64_kinks, b->bc_mask);     \
+            b->d_meta, gi, out, in, base, rk_kind, b->policy, b->d_counter + 3,    \
+            b->bc_mask);                                                           \
       }                                                                            \
     }                                                                              \
     break;
@@ -207,7 +224,13 @@ cudaError_t step(lsmgpu_batch* b, int shape, bool batched, cudaStream_t st) {
   float *phi = (float*)b->phi, *p1 = (float*)b->phi1, *p2 = (float*)b->phi2;
   if ((e = launch_shape<float>(b, shape, batched, 1, p1, phi, phi, b->d_counter, st))) return e;
   if ((e = launch_shape<float>(b, shape, batched, 32, p2, p1, phi, b->d_counter + 1, st))) return e;
-  return launch_shape<float>(b, shape, batched, 33, phi, p2, phi, b->d_counter + 2, st);
+  if ((e = launch_shape<float>(b, shape, batched, 33, phi, p2, phi, b->d_counter + 2, st))) return e;
+  if (b->policy & kStochRound) {
+    k_bump<<<1, 1, 0, st>>>(b->d_counter + 3);
+    ++launch_counter();
+    return cudaGetLastError();
+  }
+  return cudaSuccess;
 }
 
 bool batch_ok(lsmgpu_batch* b, const char* R) {
@@ -248,7 +271,7 @@ int lsmgpu_batch_create(lsmgpu_batch** out, int ngrids, const int* n,
   lsmgpu_batch* b = new lsmgpu_batch();
   b->ngrids = ngrids;
   b->prec = precision;
-  b->fp64_kinks = 0;
+  b->policy = kStochRound;
   long off = 0;
   const long align = 256 / precision;
   for (int g = 0; g < ngrids; g++) {
@@ -284,7 +307,8 @@ int lsmgpu_batch_create(lsmgpu_batch** out, int ngrids, const int* n,
             cudaMalloc(&b->phi1, bytes) == cudaSuccess &&
             cudaMalloc(&b->phi2, bytes) == cudaSuccess &&
             cudaMalloc((void**)&b->d_meta, sizeof(GridMeta) * ngrids) == cudaSuccess &&
-            cudaMalloc((void**)&b->d_counter, sizeof(unsigned) * 4) == cudaSuccess;
+            cudaMalloc((void**)&b->d_counter, sizeof(unsigned) * 4) == cudaSuccess &&
+            cudaMemset(b->d_counter, 0, sizeof(unsigned) * 4) == cudaSuccess;
   // work-lists for every candidate tile shape, largest tiles first
   for (int s = 0; ok && s < kNumShapes; s++) {
     std::vector<int4> items;
@@ -450,7 +474,20 @@ int lsmgpu_batch_set_bc(lsmgpu_batch* b, int kind) {
 // FP32 batches: recompute kink stencils in FP64 (0 off, 1 on)
 int lsmgpu_batch_set_fp64_kinks(lsmgpu_batch* b, int on) {
   if (!batch_ok(b, "lsmgpu_batch_set_fp64_kinks")) return LSMGPU_ERR_NULL_POINTER;
-  b->fp64_kinks = on ? 1 : 0;
+  b->policy = (b->policy & ~kFp64Kinks) | (on ? kFp64Kinks : 0);
+  drop_graph(b);
+  return LSMGPU_SUCCESS;
+}
+
+// FP32 batches: bit 0 kink stencils in FP64, bit 2 stochastic rounding of the
+// stage outputs (bit 1, the reinitialization sign, has no stage here)
+int lsmgpu_batch_set_fp64_policy(lsmgpu_batch* b, int policy) {
+  if (!batch_ok(b, "lsmgpu_batch_set_fp64_policy")) return LSMGPU_ERR_NULL_POINTER;
+  if (policy & ~(kFp64Kinks | kFp64Sign | kStochRound)) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, "lsmgpu_batch_set_fp64_policy: unknown bits");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  b->policy = policy;
   drop_graph(b);
   return LSMGPU_SUCCESS;
 }

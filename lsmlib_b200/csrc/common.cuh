@@ -82,6 +82,39 @@ __device__ __forceinline__ float fabsT(float x) { return fabsf(x); }
 __device__ __forceinline__ double sqrtT(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqrtT(float x) { return sqrtf(x); }
 
+// Stochastic rounding of FP32 state updates.  Round-to-nearest drops every
+// update smaller than half an ulp of phi in the same direction, so over the
+// thousands of stage updates of a run (reinitialization near its steady
+// state in particular) the FP32 state drifts from the FP64 one.  Rounding
+// up with probability (x - down(x)) / ulp makes the stored value unbiased,
+// E[round(x)] = x, and the drift a random walk (Connolly, Higham & Mary,
+// SIAM J. Sci. Comput., 2021; Paxton et al., Mon. Weather Rev., 2022).
+// The random integer comes from a counter-based hash of the cell offset and
+// a per-launch seed, so a run is reproducible.
+
+// 32-bit integer finaliser ("lowbias32", C. Wellons, hash-prospector)
+__host__ __device__ __forceinline__ unsigned sr_hash(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+// x rounded to FP32 stochastically with the low 29 bits of r: adding a
+// uniform integer below 2^29 to the magnitude bits of the FP64 value and
+// truncating those 29 bits (the FP64 significand carries 29 bits more than
+// the FP32 one) rounds up with exactly the probability above; the truncated
+// value converts to FP32 without further rounding (normal FP32 range).
+__device__ __forceinline__ float sr_float(double x, unsigned r) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  const unsigned long long sign = b & 0x8000000000000000ull;
+  unsigned long long mag = (b ^ sign) + (unsigned long long)(r & 0x1fffffffu);
+  mag &= ~0x1fffffffull;
+  return (float)__longlong_as_double((long long)(mag | sign));
+}
+
 // Status word that kernels may raise (never trap): bit 0 = bad argument seen
 // on the device, bit 1 = a bounded wait gave up.
 enum DeviceStatus : unsigned { kDevOk = 0u, kDevBadArg = 1u, kDevTimeout = 2u };

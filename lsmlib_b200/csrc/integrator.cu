@@ -36,6 +36,8 @@ struct lsmgpu_workspace {
   double* partials = nullptr;
   int npart = 0;
   unsigned bc_mask = 0x3fu;
+  int fp64_policy = kFp64Sign | kStochRound;  // FP32 workspaces only
+  unsigned sr_launches = 0;  // stochastic-rounding seeds drawn so far
   unsigned long long steps = 0;
 };
 
@@ -164,7 +166,16 @@ void* ws_alloc(size_t bytes, const char* R) {
   return p;
 }
 
-cudaError_t stage(int kind, int prec, const StageArgs& a, cudaStream_t st) {
+// seed of the next stochastically rounded launch of an FP32 workspace (0 when
+// its policy rounds to nearest)
+unsigned next_sr_seed(lsmgpu_workspace* ws) {
+  if (!ws || ws->prec != 4 || !(ws->fp64_policy & kStochRound)) return 0u;
+  return sr_hash(++ws->sr_launches * 0x9e3779b9u) | 1u;
+}
+
+cudaError_t stage(int kind, int prec, StageArgs a, cudaStream_t st,
+                  lsmgpu_workspace* ws = nullptr) {
+  a.sr_seed = next_sr_seed(ws);
   return fp_mode() == LSMGPU_FP_FAST ? launch_stage_fast(kind, prec, a, st)
                                      : launch_stage_strict(kind, prec, a, st);
 }
@@ -181,7 +192,7 @@ StageArgs base_args(lsmgpu_workspace* ws, const FillBox& fb, const double dx[3])
   m = m > dx[2] ? m : dx[2];
   a.dx_sq = m * m;
   a.dt_dev = ws->scal + kDt;
-  a.fp64_kinks = ws->prec == 4 ? 1 : 0;
+  a.fp64_policy = ws->prec == 4 ? ws->fp64_policy : 0;
   return a;
 }
 
@@ -195,11 +206,11 @@ bool reinit_step(lsmgpu_workspace* ws, void* phi, const FillBox& fb,
   a.use_phi0 = use0;
   a.aux[0] = ws->phi0;
   a.out = ws->phi1; a.phi_s = phi; a.phi_n = phi; a.rk_kind = 1;
-  if (!cuda_ok(stage(kStageReinit, ws->prec, a, st), R)) return false;
+  if (!cuda_ok(stage(kStageReinit, ws->prec, a, st, ws), R)) return false;
   a.out = ws->phi2; a.phi_s = ws->phi1; a.rk_kind = 32;
-  if (!cuda_ok(stage(kStageReinit, ws->prec, a, st), R)) return false;
+  if (!cuda_ok(stage(kStageReinit, ws->prec, a, st, ws), R)) return false;
   a.out = phi; a.phi_s = ws->phi2; a.rk_kind = 33;
-  return cuda_ok(stage(kStageReinit, ws->prec, a, st), R);
+  return cuda_ok(stage(kStageReinit, ws->prec, a, st, ws), R);
 }
 
 bool reinit_run(lsmgpu_workspace* ws, void* phi, const FillBox& fb,
@@ -325,6 +336,18 @@ int lsmgpu_workspace_set_bc(lsmgpu_workspace* ws, unsigned linear_faces_mask) {
   return LSMGPU_SUCCESS;
 }
 
+int lsmgpu_workspace_set_fp64_policy(lsmgpu_workspace* ws, int policy) {
+  // bit 0: WENO5 kink stencils in FP64; bit 1: reinitialization sign in FP64;
+  // bit 2: stochastic rounding of the FP32 stage outputs
+  if (!ws_ok(ws, "lsmgpu_workspace_set_fp64_policy")) return LSMGPU_ERR_NULL_POINTER;
+  if (policy & ~(kFp64Kinks | kFp64Sign | kStochRound)) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, "lsmgpu_workspace_set_fp64_policy: unknown bits");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  ws->fp64_policy = policy;
+  return LSMGPU_SUCCESS;
+}
+
 int lsmgpu_workspace_set_time(lsmgpu_workspace* ws, double t) {
   if (!ws_ok(ws, "lsmgpu_workspace_set_time")) return LSMGPU_ERR_NULL_POINTER;
   double v[2] = {0.0, t};
@@ -411,7 +434,7 @@ int lsmgpu_lse_stage(int kind, int precision, void* out, const void* phi_s,
   a.dt = dt;
   a.rk_kind = rk_kind;
   a.use_phi0 = use_phi0;
-  a.fp64_kinks = precision == 4;
+  a.fp64_policy = precision == 4 ? kFp64Sign : 0;
   cudaStream_t st = cur_stream();
   if (!cuda_ok(stage(kind, precision, a, st), R)) return LSMGPU_ERR_CUDA;
   if (sync_mode() && !cuda_ok(cudaStreamSynchronize(st), R)) return LSMGPU_ERR_CUDA;
@@ -479,11 +502,11 @@ int lsmgpu_advect_tvdrk3(lsmgpu_workspace* ws, void* phi, const void* vx,
     StageArgs a = base_args(ws, f, dx);
     for (int d = 0; d < 3; d++) a.aux[d] = vel[d];
     a.out = ws->phi1; a.phi_s = phi; a.phi_n = phi; a.rk_kind = 1;
-    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
     a.out = ws->phi2; a.phi_s = ws->phi1; a.rk_kind = 32;
-    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
     a.out = phi; a.phi_s = ws->phi2; a.rk_kind = 33;
-    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
     k_advance_t<<<1, 1, 0, st>>>(ws->scal);
     ++launch_counter();
     ws->steps++;
@@ -544,13 +567,13 @@ int lsmgpu_deformation_tvdrk3(lsmgpu_workspace* ws, void* phi, const int fb[6],
     StageArgs a = base_args(ws, f, dx);
     for (int d = 0; d < 3; d++) a.aux[d] = ws->vel[d];
     a.out = ws->phi1; a.phi_s = phi; a.phi_n = phi; a.rk_kind = 1;
-    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
     velocity(1.0);
     a.out = ws->phi2; a.phi_s = ws->phi1; a.rk_kind = 32;
-    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
     velocity(0.5);
     a.out = phi; a.phi_s = ws->phi2; a.rk_kind = 33;
-    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
     k_advance_t<<<1, 1, 0, st>>>(ws->scal);
     ++launch_counter();
     ws->steps++;
@@ -583,18 +606,19 @@ int lsmgpu_normal_tvdrk3(lsmgpu_workspace* ws, void* phi, const void* F,
     a.aux[0] = F;
     // WENO5 +- of phi^n once: L(phi^n) for stage 1 and the CFL maxima
     a.rhs_out = ws->rhs; a.partials = ws->partials; a.phi_s = phi;
-    if (!cuda_ok(stage(kStageNormalRhs, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(stage(kStageNormalRhs, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
     k_dt_finish<<<1, 256, 0, st>>>(ws->partials, nblk, cfl, tiny, ws->scal, 0.0);
     ++launch_counter();
     // stage 1: phi1 = phi + dt L (LSM3D_TVD_RK3_STAGE1)
     if (!cuda_ok(launch_rk(ws->prec, 1, ws->phi1, ws->gb, nullptr, ws->gb, phi,
-                           ws->gb, ws->rhs, ws->gb, f, 0.0, ws->scal + kDt, st),
+                           ws->gb, ws->rhs, ws->gb, f, 0.0, ws->scal + kDt, st,
+                           next_sr_seed(ws)),
                  R))
       return LSMGPU_ERR_CUDA;
     a.out = ws->phi2; a.phi_s = ws->phi1; a.phi_n = phi; a.rk_kind = 32;
-    if (!cuda_ok(stage(kStageNormal, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(stage(kStageNormal, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
     a.out = phi; a.phi_s = ws->phi2; a.rk_kind = 33;
-    if (!cuda_ok(stage(kStageNormal, ws->prec, a, st), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(stage(kStageNormal, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
     k_advance_t<<<1, 1, 0, st>>>(ws->scal);
     ++launch_counter();
     ws->steps++;

@@ -60,7 +60,7 @@ cudaError_t launch_rk(int prec, int kind, void* out, const Box& gout,
                       const void* us, const Box& gus, const void* uc,
                       const Box& guc, const void* rhs, const Box& grhs,
                       const FillBox& fb, double dt, const double* dt_dev,
-                      cudaStream_t st);
+                      cudaStream_t st, unsigned sr_seed = 0u);
 // face 0..5; copy = 0 linear extrapolation, 1 copy extrapolation
 cudaError_t launch_bc(int prec, int copy, void* phi, const Box& gphi,
                       const FillBox& fb, int face, cudaStream_t st);

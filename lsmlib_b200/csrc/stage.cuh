@@ -55,9 +55,17 @@ struct StageParams {
   double dt;
   int rk_kind;         // 1, 22, 32, 33 (see rk_update)
   int use_phi0;
-  int fp64_kinks;      // FP32 form: recompute kink stencils in FP64
+  int fp64_policy;     // FP32 form: kFp64Kinks | kFp64Sign (see below)
+  unsigned sr_seed;    // FP32 form: nonzero = stochastic rounding of out
   T vel_const[3];      // kStageAdvectConst: the grid's constant velocity
 };
+
+// FP64 parts of the FP32 form: kFp64Kinks recomputes in FP64 the WENO5
+// stencils whose smoothness indicators differ by more than a factor 1e3;
+// kFp64Sign evaluates the smoothed sign of the reinitialization RHS in FP64;
+// kStochRound forms the Runge-Kutta combination in FP64 and rounds it to
+// FP32 stochastically (sr_float).
+constexpr int kFp64Kinks = 1, kFp64Sign = 2, kStochRound = 4;
 
 template <typename T>
 __device__ __forceinline__ T rk_combine(int kind, T uc, T us, T r, T dt) {
@@ -67,6 +75,19 @@ __device__ __forceinline__ T rk_combine(int kind, T uc, T us, T r, T dt) {
     case 33: return (T(1) / T(3)) * uc + (T(2) / T(3)) * (us + dt * r);
     default: return us + dt * r;
   }
+}
+
+// the stage output of cell offset o: the Runge-Kutta combination, in the FP32
+// form with stochastic rounding when the launch has a seed
+template <typename T>
+__device__ __forceinline__ T stage_out(const StageParams<T>& p, long o, T uc, T us,
+                                       T r, T dt) {
+  if (sizeof(T) == 4 && p.sr_seed != 0u) {
+    const double dtd = p.dt_dev ? *p.dt_dev : p.dt;
+    const double v = rk_combine<double>(p.rk_kind, uc, us, r, dtd);
+    return (T)sr_float(v, sr_hash((unsigned)o * 0x9e3779b9u ^ p.sr_seed));
+  }
+  return rk_combine(p.rk_kind, uc, us, r, dt);
 }
 
 // Boundary kinds per face f (0..5 = x-lo, x-hi, y-lo, y-hi, z-lo, z-hi) in
@@ -181,10 +202,11 @@ __device__ __forceinline__ T godunov_sq2(T vn, T xp, T yp, T zp, T xm, T ym,
 }
 
 // reinitialization RHS of one cell (lsm_reinitialization3d.f.in:158-199,
-// :218-256); the FP32 form evaluates the smoothed sign in FP64
+// :218-256); with fp64_sign the FP32 form evaluates the smoothed sign in FP64
 template <typename T>
 __device__ __forceinline__ T reinit_cell(T pc, T xp, T yp, T zp, T xm, T ym,
-                                         T zm, T dx_sq, bool use0) {
+                                         T zm, T dx_sq, bool use0,
+                                         bool fp64_sign) {
   const T z = T(0);
   T gp[3] = {xp, yp, zp}, gm[3] = {xm, ym, zm}, gs[3];
 #pragma unroll
@@ -201,7 +223,7 @@ __device__ __forceinline__ T reinit_cell(T pc, T xp, T yp, T zp, T xm, T ym,
   // FP64 build's zero_tol for both precisions (see stage_zero_tol)
   if (!(fabsT(pc) >= T(1.0e-11))) return z;
   const T nsq = gs[0] * gs[0] + gs[1] * gs[1] + gs[2] * gs[2];
-  if (sizeof(T) == 4) {
+  if (sizeof(T) == 4 && fp64_sign) {
     const double pd = pc, nd = nsq, dd = dx_sq;
     const double sgn = use0 ? pd / sqrt(pd * pd + dd) : pd / sqrt(pd * pd + nd * dd);
     return (T)(sgn * (1.0 - sqrt(nd)));
@@ -268,7 +290,7 @@ __device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
                       yhi <= p.dom.hi[1] && kb - 3 >= p.dom.lo[2] &&
                       ke + 3 <= p.dom.hi[2];
   const bool need_bc = p.bc_mask != 0u && !inside;
-  const bool kink64 = p.fp64_kinks != 0;
+  const bool kink64 = (p.fp64_policy & kFp64Kinks) != 0;
   double hmax = -1.0;
 
   // Tile roles.  Active threads put their own phi(i,j,k) in the tile.  In a
@@ -357,7 +379,8 @@ __device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
         weno_axis<T, FAST>(w, p.inv[2], kink64, zp, zm);
         if (KIND == kStageReinit) {
           const T pc = p.use_phi0 == 1 ? a0 : w[3];
-          L = reinit_cell(pc, xp, yp, zp, xm, ym, zm, p.dx_sq, p.use_phi0 == 1);
+          L = reinit_cell(pc, xp, yp, zp, xm, ym, zm, p.dx_sq, p.use_phi0 == 1,
+                          (p.fp64_policy & kFp64Sign) != 0);
         } else {
           // LSM3D_ADD_NORMAL_VEL_TERM_TO_LSE_RHS (:209-231)
           const T f = a0;
@@ -380,19 +403,208 @@ __device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
       if (KIND == kStageNormalRhs) {
         p.rhs_out[o] = L;
       } else {
-        p.out[o] = rk_combine(p.rk_kind, uc, w[3], L, dt);
+        p.out[o] = stage_out(p, o, uc, w[3], L, dt);
       }
     }
   }
   return hmax;
 }
 
+// Right-hand side of the two-sided kinds (normal speed, reinitialization)
+// from the six one-sided derivatives; accumulates the CFL speed of
+// kStageNormalRhs into hmax.
+template <typename T, int KIND>
+__device__ __forceinline__ T two_sided_rhs(const StageParams<T>& p, T a0, T pc,
+                                           T xp, T yp, T zp, T xm, T ym, T zm,
+                                           double& hmax) {
+  if (KIND == kStageReinit) {
+    const T s = p.use_phi0 == 1 ? a0 : pc;
+    return reinit_cell(s, xp, yp, zp, xm, ym, zm, p.dx_sq, p.use_phi0 == 1,
+                       (p.fp64_policy & kFp64Sign) != 0);
+  }
+  // LSM3D_ADD_NORMAL_VEL_TERM_TO_LSE_RHS (:209-231)
+  const T f = a0;
+  T L = T(0);
+  if (fabsT(f) >= stage_zero_tol<T>())
+    L = T(0) - f * sqrtT(godunov_sq2(f, xp, yp, zp, xm, ym, zm));
+  if (KIND == kStageNormalRhs) {
+    // LSM3D_COMPUTE_STABLE_NORMAL_VEL_DT per-cell speed (FP64)
+    const double cx = fmax2(fabs((double)xp), fabs((double)xm));
+    const double cy = fmax2(fabs((double)yp), fabs((double)ym));
+    const double cz = fmax2(fabs((double)zp), fabs((double)zm));
+    const double ng = sqrt(cx * cx + cy * cy + cz * cz + (double)p.dx_sq);
+    const double h = fabs((double)f) / ng *
+                     (cx * (double)p.inv[0] + cy * (double)p.inv[1] +
+                      cz * (double)p.inv[2]);
+    hmax = (h > hmax) ? h : hmax;
+  }
+  return L;
+}
+
+// value of the lane to the left (lane 0 gets its own back)
+template <typename T>
+__device__ __forceinline__ T shfl_up_T(T v) {
+  return __shfl_up_sync(0xffffffffu, v, 1);
+}
+
+template <typename T>
+__device__ __forceinline__ void face_pm(const T* u, T inv, bool kink64, T& vp,
+                                        T& vm) {
+  if (sizeof(T) == 4 && kink64) weno5_face<T, true>(u, inv, vp, vm);
+  else weno5_face<T, false>(u, inv, vp, vm);
+}
+
+// The two-sided kinds in the FMA/FP32 arithmetic, one WENO5 weight
+// evaluation per cell face instead of one per cell side (weno5_face): the
+// thread of cell c evaluates the face c+1/2 of each axis, giving phi^+(c)
+// and phi^-(c+1).  phi^-(c) comes from the neighbour that owns face c-1/2:
+// along x the lane to the left (warp shuffle; a tile row is one warp), along
+// y the row below (shared memory), along z the previous plane of the march
+// (a register).  The faces in front of the first cell of each row, column
+// and z run are evaluated once more (rows by warp 0, columns by the last
+// warp, z at the first plane).  Tile staging, boundary values and prefetch
+// are those of stage_tile.
+template <typename T, int KIND, int TX, int TY, int TZ>
+__device__ __forceinline__ double stage_tile_faces(const StageParams<T>& p, int bx,
+                                                   int by, int bz,
+                                                   T (*tile)[TY + 6][TX + 6],
+                                                   T (*fy)[TX], T* fx) {
+  static_assert(TX == 32, "a tile row is one warp");
+  static_assert(TY <= 32, "row-start faces are spread over one warp");
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = p.fb.lo[0] + bx * TX + tx;
+  const int j = p.fb.lo[1] + by * TY + ty;
+  const int kb = p.fb.lo[2] + bz * TZ;
+  const int ke = min(kb + TZ - 1, p.fb.hi[2]);
+  const bool act = (i <= p.fb.hi[0]) && (j <= p.fb.hi[1]);
+  const Grid3<const T> phi = make_grid(p.phi_s, p.gb);
+  const long sy = p.gb.sy(), sz = p.gb.sz();
+  const long base0 = -((long)p.gb.lo[0] + sy * p.gb.lo[1] + sz * p.gb.lo[2]);
+  const T dt = p.dt_dev ? (T)(*p.dt_dev) : (T)p.dt;
+  const int xlo = p.fb.lo[0] + bx * TX - 3, xhi = min(p.fb.lo[0] + bx * TX + TX - 1, p.fb.hi[0]) + 3;
+  const int ylo = p.fb.lo[1] + by * TY - 3, yhi = min(p.fb.lo[1] + by * TY + TY - 1, p.fb.hi[1]) + 3;
+  const bool inside = xlo >= p.dom.lo[0] && xhi <= p.dom.hi[0] && ylo >= p.dom.lo[1] &&
+                      yhi <= p.dom.hi[1] && kb - 3 >= p.dom.lo[2] &&
+                      ke + 3 <= p.dom.hi[2];
+  const bool need_bc = p.bc_mask != 0u && !inside;
+  const bool kink64 = (p.fp64_policy & kFp64Kinks) != 0;
+  double hmax = -1.0;
+
+  const int hi0 = p.fb.hi[0], hi1 = p.fb.hi[1];
+  const bool ctr_halo = !act && i <= hi0 + 3 && j <= hi1 + 3 && !(i > hi0 && j > hi1);
+  const int hx = (tx < 3) ? (i - 3) : (i + 3);
+  const bool has_hx = (j <= hi1) && ((tx < 3) || (tx >= TX - 3 && i <= hi0));
+  const int hj = (ty < 3) ? (j - 3) : (j + 3);
+  const bool has_hy = (i <= hi0) && ((ty < 3) || (ty >= TY - 3 && j <= hi1));
+  const int tcol = (tx < 3) ? tx : tx + 6;
+  const int trow = (ty < 3) ? ty : ty + 6;
+  // row-start face of row tx (warp 0) / column-start face of column tx
+  // (last warp): is that row / column part of the fill box?
+  const bool row_start = ty == 0 && tx < TY && p.fb.lo[1] + by * TY + tx <= hi1;
+  const bool col_start = ty == TY - 1 && i <= hi0;
+
+  auto ld = [&](int a, int b, int c) -> T {
+    return need_bc ? fetch_bc(phi, p, a, b, c) : __ldg(phi.ptr(a, b, c));
+  };
+  T nx_c = T(0), nx_hx = T(0), nx_hy = T(0);
+  auto prefetch = [&](int k) {
+    if (act) nx_c = ld(i, j, k + 3);
+    else if (ctr_halo) nx_c = ld(i, j, k);
+    if (has_hx) nx_hx = ld(hx, j, k);
+    if (has_hy) nx_hy = ld(i, hj, k);
+  };
+
+  T w[7];
+  if (act) {
+#pragma unroll
+    for (int m = 0; m < 6; m++) w[m + 1] = ld(i, j, kb - 3 + m);
+  }
+  T zm_run = T(0);  // phi_z^-(k), from face k-1/2 of the previous plane
+  prefetch(kb);
+  for (int k = kb; k <= ke; ++k) {
+    const int buf = (k - kb) & 1;
+    if (act) {
+#pragma unroll
+      for (int m = 0; m < 6; m++) w[m] = w[m + 1];
+      w[6] = nx_c;
+      tile[buf][ty + 3][tx + 3] = w[3];
+    } else if (ctr_halo) {
+      tile[buf][ty + 3][tx + 3] = nx_c;
+    }
+    if (has_hx) tile[buf][ty + 3][tcol] = nx_hx;
+    if (has_hy) tile[buf][trow][tx + 3] = nx_hy;
+    __syncthreads();
+    if (k < ke) prefetch(k + 1);
+    const long o = base0 + (long)i + sy * j + sz * k;
+    T a0 = T(0), uc = T(0);
+    T xp = T(0), xm_next = T(0), yp = T(0), zp = T(0), zm_next = T(0);
+    if (act) {
+      if (KIND == kStageNormal || KIND == kStageNormalRhs ||
+          (KIND == kStageReinit && p.use_phi0 == 1))
+        a0 = __ldg(p.aux0 + o);
+      if (KIND != kStageNormalRhs && p.rk_kind != 1) uc = __ldg(p.phi_n + o);
+      T u[6], ym_next;
+#pragma unroll
+      for (int m = 0; m < 6; m++) u[m] = tile[buf][ty + 3][tx + 1 + m];
+      face_pm(u, p.inv[0], kink64, xp, xm_next);
+#pragma unroll
+      for (int m = 0; m < 6; m++) u[m] = tile[buf][ty + 1 + m][tx + 3];
+      face_pm(u, p.inv[1], kink64, yp, ym_next);
+      if (ty + 1 < TY) fy[ty + 1][tx] = ym_next;
+      if (k == kb) {
+        T unused;
+        face_pm(w, p.inv[2], kink64, unused, zm_run);
+      }
+      face_pm(w + 1, p.inv[2], kink64, zp, zm_next);
+    }
+    const T xm_left = shfl_up_T(xm_next);
+    if (row_start) {
+      T u[6], unused;
+#pragma unroll
+      for (int m = 0; m < 6; m++) u[m] = tile[buf][tx + 3][m];
+      face_pm(u, p.inv[0], kink64, unused, fx[tx]);
+    }
+    if (col_start) {
+      T u[6], unused;
+#pragma unroll
+      for (int m = 0; m < 6; m++) u[m] = tile[buf][m][tx + 3];
+      face_pm(u, p.inv[1], kink64, unused, fy[0][tx]);
+    }
+    __syncthreads();
+    if (act) {
+      const T xm = tx == 0 ? fx[ty] : xm_left;
+      const T ym = fy[ty][tx];
+      const T zm = zm_run;
+      zm_run = zm_next;
+      const T L = two_sided_rhs<T, KIND>(p, a0, w[3], xp, yp, zp, xm, ym, zm, hmax);
+      if (KIND == kStageNormalRhs) p.rhs_out[o] = L;
+      else p.out[o] = stage_out(p, o, uc, w[3], L, dt);
+    }
+  }
+  return hmax;
+}
+
+template <typename T, int KIND, bool FAST, int TX>
+struct UseFaces {
+  static constexpr bool value =
+      (FAST || sizeof(T) == 4) && TX == 32 &&
+      (KIND == kStageNormal || KIND == kStageReinit || KIND == kStageNormalRhs);
+};
+
 template <typename T, int KIND, bool FAST, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(TX * TY, 2)
 k_stage(StageParams<T> p) {
   __shared__ T tile[2][TY + 6][TX + 6];
-  const double hmax = stage_tile<T, KIND, FAST, TX, TY, TZ>(
-      p, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, tile);
+  double hmax;
+  if constexpr (UseFaces<T, KIND, FAST, TX>::value) {
+    __shared__ T fy[TY][TX];
+    __shared__ T fx[TY];
+    hmax = stage_tile_faces<T, KIND, TX, TY, TZ>(p, (int)blockIdx.x, (int)blockIdx.y,
+                                                 (int)blockIdx.z, tile, fy, fx);
+  } else {
+    hmax = stage_tile<T, KIND, FAST, TX, TY, TZ>(p, (int)blockIdx.x, (int)blockIdx.y,
+                                                 (int)blockIdx.z, tile);
+  }
   const int tx = threadIdx.x, ty = threadIdx.y;
   if (KIND == kStageNormalRhs) {
     // block maximum with the reference's "if (h > m) m = h" comparison

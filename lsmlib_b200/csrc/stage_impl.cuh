@@ -29,7 +29,8 @@ StageParams<T> to_params(const StageArgs& a) {
   p.dt = a.dt;
   p.rk_kind = a.rk_kind;
   p.use_phi0 = a.use_phi0;
-  p.fp64_kinks = a.fp64_kinks;
+  p.fp64_policy = a.fp64_policy;
+  p.sr_seed = a.sr_seed;
   return p;
 }
 

@@ -23,7 +23,8 @@ struct StageArgs {
   double dt;
   int rk_kind;
   int use_phi0;
-  int fp64_kinks;
+  int fp64_policy;  // kFp64Kinks | kFp64Sign | kStochRound (FP32 form)
+  unsigned sr_seed; // nonzero: stochastic rounding of the output (FP32)
 };
 
 // tile of the stage kernels: TX x TY cells per block, TZ planes per block

@@ -250,11 +250,19 @@ __device__ __forceinline__ T rk_update(int kind, T uc, T us, T r, T dt) {
 template <typename T>
 __global__ void __launch_bounds__(128)
 k_rk(Grid3<T> out, Grid3<const T> us, Grid3<const T> uc, Grid3<const T> rhs,
-     FillBox fb, int kind, T dt, const double* dt_dev) {
+     FillBox fb, int kind, T dt, const double* dt_dev, unsigned sr_seed) {
   const T h = dt_dev ? (T)(*dt_dev) : dt;
   CELL_LOOP_BEGIN(fb)
   const T s = (kind == 1) ? T(0) : us(i, j, k);
-  out(i, j, k) = rk_update(kind, uc(i, j, k), s, rhs(i, j, k), h);
+  if (sizeof(T) == 4 && sr_seed != 0u) {
+    // FP32 state with stochastic rounding (common.cuh): the update in FP64
+    const double hd = dt_dev ? *dt_dev : (double)dt;
+    const double v = rk_update<double>(kind, uc(i, j, k), s, rhs(i, j, k), hd);
+    const unsigned o = (unsigned)(i + out.sy * j + out.sz * k);
+    out(i, j, k) = (T)sr_float(v, sr_hash(o * 0x9e3779b9u ^ sr_seed));
+  } else {
+    out(i, j, k) = rk_update(kind, uc(i, j, k), s, rhs(i, j, k), h);
+  }
   CELL_LOOP_END
 }
 
@@ -610,14 +618,14 @@ cudaError_t launch_rk(int prec, int kind, void* out, const Box& gout,
                       const void* us, const Box& gus, const void* uc,
                       const Box& guc, const void* rhs, const Box& grhs,
                       const FillBox& fb, double dt, const double* dt_dev,
-                      cudaStream_t st) {
+                      cudaStream_t st, unsigned sr_seed) {
   dim3 grid = cell_grid(fb), blk(kBX, kBY, 1);
   const void* usp = us ? us : uc;
   const Box& gusb = us ? gus : guc;
 #define C(T)                                                                  \
   (k_rk<T><<<grid, blk, 0, st>>>(G<T>(out, gout), GC<T>(usp, gusb),           \
                                  GC<T>(uc, guc), GC<T>(rhs, grhs), fb, kind,  \
-                                 (T)dt, dt_dev),                              \
+                                 (T)dt, dt_dev, sr_seed),                     \
    0)
   DISPATCH_PREC(prec, C);
 #undef C

@@ -151,6 +151,77 @@ __device__ __forceinline__ void weno5_pm_fast(const T* w, T inv, T& vp, T& vm) {
   }
 }
 
+// FP64 recomputation of one face for the FP32 form (defined below; kept out
+// of line so that the rarely taken path does not grow every call site)
+static __device__ __noinline__ float2 weno5_face_fp64(float u0, float u1, float u2,
+                                                     float u3, float u4, float u5,
+                                                     float inv);
+
+// The two HJ-WENO5 values that share the face between cells c and c+1, from
+// u[0..5] = phi(c-2..c+3): vp = phi^+(c) and vm = phi^-(c+1).  Both read the
+// same five differences V1..V5 (faces c-3/2..c+5/2), minus in the order
+// V1..V5 and plus in the order V5..V1 (lsm_spatial_derivatives3d.f.in:
+// 1286-1290, :1330-1334), so they share eps, the three smoothness indicators
+// Sa, Sb, Sc (plus sees them as S3, S2, S1) and the products
+// P_xy = (q_x q_y)^2 of the single-reciprocal normalisation; only the
+// assignment of the linear weights {0.1, 0.6, 0.3} differs.  With
+// w2 = 1 - w1 - w3 the reconstruction is
+//   phi = p2 + w1 (p1 - p2) + w3 (p3 - p2),
+//   p1 - p2 = (ta - tb)/3,  p3 - p2 = (tb - tc)/6,
+// where ta, tb, tc are the second differences of V already formed for the
+// smoothness indicators; for the reversed (plus) stencil the two third
+// differences swap and change sign.  When KINK64 is set (FP32 form) a face
+// whose indicators differ by more than a factor 1e3 is recomputed in FP64.
+template <typename T, bool KINK64>
+__device__ __forceinline__ void weno5_face(const T* u, T inv, T& vp, T& vm) {
+  const T V1 = (u[1] - u[0]) * inv, V2 = (u[2] - u[1]) * inv,
+          V3 = (u[3] - u[2]) * inv, V4 = (u[4] - u[3]) * inv,
+          V5 = (u[5] - u[4]) * inv;
+  const T m = fmax(fmax(fmax(V1 * V1, V2 * V2), fmax(V3 * V3, V4 * V4)), V5 * V5);
+  const T eps = T(1e-6) * m + Consts<T>::tiny;
+  const T c13_12 = T(13.0 / 12.0), c14 = T(0.25);
+  const T ta = V1 - T(2) * V2 + V3, tb = V2 - T(2) * V3 + V4, tc = V3 - T(2) * V4 + V5;
+  T t = V1 - T(4) * V2 + T(3) * V3;
+  const T Sa = c13_12 * (ta * ta) + c14 * (t * t);
+  t = V2 - V4;
+  const T Sb = c13_12 * (tb * tb) + c14 * (t * t);
+  t = T(3) * V3 - T(4) * V4 + V5;
+  const T Sc = c13_12 * (tc * tc) + c14 * (t * t);
+  if (KINK64) {
+    const T mx = fmax(fmax(Sa, Sb), Sc), mn = fmin(fmin(Sa, Sb), Sc);
+    if (mx > T(1e3) * mn + T(1e-4) * m) {
+      if constexpr (sizeof(T) == 4) {
+        const float2 r = weno5_face_fp64(u[0], u[1], u[2], u[3], u[4], u[5], inv);
+        vp = r.x;
+        vm = r.y;
+        return;
+      }
+    }
+  }
+  const T sc = inv_pow2_of(eps);
+  const T es = eps * sc;
+  const T qa = Sa * sc + es, qb = Sb * sc + es, qc = Sc * sc + es;
+  const T Qa = qa * qa, Qb = qb * qb, Qc = qc * qc;
+  const T Pbc = Qb * Qc, Pac = Qa * Qc, Pab = Qa * Qb;
+  const T T1 = ta - tb, T2 = tb - tc;
+  const T sm = T(0.1) * Pbc + T(0.6) * Pac + T(0.3) * Pab;
+  const T sp = T(0.1) * Pab + T(0.6) * Pac + T(0.3) * Pbc;
+  const T d6 = T(1.0 / 6.0), e6 = T(5.0 / 6.0), a3 = T(1.0 / 3.0);
+  const T p2m = a3 * V4 + e6 * V3 - d6 * V2;
+  const T p2p = a3 * V2 + e6 * V3 - d6 * V4;
+  vm = p2m + (Pbc * (T1 * T(1.0 / 30.0)) + Pab * (T2 * T(1.0 / 20.0))) * rcp_nr(sm);
+  vp = p2p - (Pab * (T2 * T(1.0 / 30.0)) + Pbc * (T1 * T(1.0 / 20.0))) * rcp_nr(sp);
+}
+
+static __device__ __noinline__ float2 weno5_face_fp64(float u0, float u1, float u2,
+                                                     float u3, float u4, float u5,
+                                                     float inv) {
+  const double ud[6] = {u0, u1, u2, u3, u4, u5};
+  double dp, dm;
+  weno5_face<double, false>(ud, (double)inv, dp, dm);
+  return make_float2((float)dp, (float)dm);
+}
+
 // True when the smoothness indicators of a stencil differ by more than a
 // factor 1e3, i.e. the stencil straddles a kink.  Used by the FP32 form to
 // recompute such values in FP64.

@@ -15,6 +15,7 @@ SIGNATURES = {
     "lsmgpu_workspace_create": (I, [ctypes.POINTER(P), IA, I]),
     "lsmgpu_workspace_destroy": (I, [P]),
     "lsmgpu_workspace_set_bc": (I, [P, U]),
+    "lsmgpu_workspace_set_fp64_policy": (I, [P, I]),
     "lsmgpu_workspace_set_time": (I, [P, D]),
     "lsmgpu_workspace_get_time": (I, [P, DA, DA]),
     "lsmgpu_workspace_device_scalars": (P, [P]),
@@ -35,6 +36,7 @@ SIGNATURES = {
     "lsmgpu_batch_set_tile": (I, [P, I]),
     "lsmgpu_batch_get_tile": (I, [P, IA, IA]),
     "lsmgpu_batch_set_fp64_kinks": (I, [P, I]),
+    "lsmgpu_batch_set_fp64_policy": (I, [P, I]),
     "lsmgpu_batch_set_bc": (I, [P, I]),
     "lsmgpu_batch_autotune": (I, [P, ctypes.POINTER(ctypes.c_float)]),
     "lsmgpu_batch_advect_tvdrk3": (I, [P, I, I, I]),

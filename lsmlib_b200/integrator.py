@@ -22,6 +22,9 @@ from .ext_abi import dbls, ints
 FP_STRICT, FP_FAST = 0, 1
 # boundary masks (per face f = x-lo .. z-hi): linear, copy, periodic
 BC_LINEAR, BC_COPY, BC_PERIODIC = 0x3F, 0x3F << 8, 0x3F << 16
+# FP64 parts of the FP32 form (Workspace.set_fp64_policy): kink stencils in
+# FP64, reinitialization sign in FP64, stochastic rounding of stage outputs
+FP64_KINKS, FP64_SIGN, STOCH_ROUND = 1, 2, 4
 
 
 def set_fp_mode(mode):
@@ -55,6 +58,11 @@ class Workspace:
 
     def set_bc(self, mask):
         gpu.check_rc(gpu.load().lsmgpu_workspace_set_bc(self.h, int(mask)), "set_bc")
+
+    def set_fp64_policy(self, policy):
+        """FP32 workspaces: FP64_KINKS | FP64_SIGN | STOCH_ROUND."""
+        gpu.check_rc(gpu.load().lsmgpu_workspace_set_fp64_policy(self.h, int(policy)),
+                     "set_fp64_policy")
 
     def set_time(self, t):
         gpu.check_rc(gpu.load().lsmgpu_workspace_set_time(self.h, float(t)), "set_time")

@@ -56,7 +56,9 @@ class Grid:
         return Field.zeros(self.gb_lo, self.gb_hi)
 
     def field(self, data):
-        return Field(np.asfortranarray(data, dtype=np.float64), self.gb_lo)
+        """A ghost-box Field holding a copy of data (the steppers update their
+        Fields in place, so the caller's array is never modified)."""
+        return Field(np.array(data, dtype=np.float64, order="F", copy=True), self.gb_lo)
 
     def interior(self, f):
         return f.view(self.fb_lo, self.fb_hi)

@@ -198,10 +198,12 @@ def test_single_stage_with_caller_ghosts(mode):
     check(mode, g.interior(g.field(d_out.download())), g.interior(out))
 
 
-def test_fp32_form_error_against_fp64():
-    """FP32 storage and arithmetic (FP64 CFL reduction, dt and t, FP64 WENO5
-    on kink stencils, FP64 smoothed sign) stays within 1e-5 of the FP64
-    oracle over 10 normal-velocity steps with a reinitialization."""
+FP32_POLICIES = [None, 0, 1, 4, 7]   # None: the workspace default (sign | SR)
+
+
+def fp32_normal_run(policy):
+    """10 normal-velocity steps with a reinitialization every 5 steps on a
+    48^3 union of spheres; the FP32 workspace result and the FP64 oracle's."""
     from lsmlib_b200 import gpu, integrator
     n = (48, 48, 48)
     g = Grid(n, dx=(2.0 / 48,) * 3)
@@ -217,13 +219,36 @@ def test_fp32_form_error_against_fp64():
         if (s + 1) % 5 == 0:
             st.reinit(ref, 0.5, 4)
     ws = integrator.Workspace(g.gb, 4)
+    if policy is not None:
+        ws.set_fp64_policy(policy)
     d = gpu.DeviceArray.from_host(phi0.astype(np.float32))
     dF = gpu.DeviceArray.from_host(F.astype(np.float32))
     ws.normal(d, dF, g.fb, g.dx, cfl=0.5, nsteps=10, reinit_interval=5,
               reinit_iters=4)
     got = g.interior(g.field(d.download().astype(np.float64)))
-    err = np.abs(got - g.interior(ref))
+    return got, g.interior(ref)
+
+
+@pytest.mark.parametrize("policy", FP32_POLICIES)
+def test_fp32_form_error_against_fp64(policy):
+    """FP32 storage and arithmetic (FP64 CFL reduction, dt and t) under each
+    FP64 policy (kink stencils in FP64, smoothed sign in FP64, stochastic
+    rounding of the stage outputs) stays within 1e-5 of the FP64 oracle."""
+    got, want = fp32_normal_run(policy)
+    err = np.abs(got - want)
     assert err.max() <= ABS_FP32, err.max()
+
+
+def test_fp32_stochastic_rounding_is_reproducible_and_unbiased():
+    """Two fresh workspaces draw the same seeds (bit-identical results), and
+    the mean error of the stochastically rounded run is below the
+    round-to-nearest run's."""
+    from lsmlib_b200 import integrator
+    a, want = fp32_normal_run(integrator.STOCH_ROUND)
+    b, _ = fp32_normal_run(integrator.STOCH_ROUND)
+    assert same_bits(a, b)
+    rn, _ = fp32_normal_run(0)
+    assert np.mean(np.abs(a - want)) < np.mean(np.abs(rn - want))
 
 
 @pytest.mark.parametrize("bc", ["copy", "periodic"])
