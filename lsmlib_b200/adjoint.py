@@ -85,6 +85,21 @@ class AdvectionAdjoint:
         return out
 
 
+def heaviside(x, eps):
+    """LSM_HEAVISIDE (lsm_calculus_toolbox.h:41-45), elementwise."""
+    x = np.asarray(x, dtype=np.float64)
+    h = 0.5 * (1.0 + x / eps + np.sin(np.pi * x / eps) / np.pi)
+    return np.where(x < -eps, 0.0, np.where(x > eps, 1.0, h))
+
+
+def loss_difference(phi_a, phi_b, target, eps, vol):
+    """J(phi_a) - J(phi_b) for two final states (interior arrays), formed
+    cell by cell as (Ha - Hb)(Ha + Hb - 2 Ht) so that a finite difference of
+    nearby states does not lose its digits to the rounding of two totals."""
+    ha, hb, ht = heaviside(phi_a, eps), heaviside(phi_b, eps), heaviside(target, eps)
+    return float(np.sum((ha - hb) * (ha + hb - 2.0 * ht)) * vol)
+
+
 def spline_velocity(theta, n, dx, x_lo, lattice, ghost=3):
     """Host evaluation of the trilinear B-spline velocity on the ghost box
     (the same hat functions as the device kernel); zero in ghost cells."""

@@ -42,6 +42,10 @@ constexpr int kTX = 32, kTY = 8, kTZ = 32;
 //   D = sum w_k p_k,  w_k = a_k / sum a,  a_k = d_k / (S_k + eps)^2
 //   dD/dv = sum w_k dp_k + sum b_k (dS_k + deps),
 //   b_k = -2 w_k (p_k - D) / (S_k + eps)
+// The weights use the single-reciprocal normalisation of the forward stage
+// kernels (weno_fast.cuh): q_k = (S_k + eps) s with s a power of two,
+// w_k = d_k prod_{j!=k} q_j^2 / sum_m (...), and the three 1/(S_k + eps)
+// come from one more reciprocal, 1/q_k = s prod_{j!=k} q_j / (q_1 q_2 q_3).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void weno5_value_grad(const double v[5], double& D,
                                                  double g[5]) {
@@ -65,14 +69,18 @@ __device__ __forceinline__ void weno5_value_grad(const double v[5], double& D,
   const double S1 = 13.0 / 12.0 * t1 * t1 + 0.25 * u1 * u1;
   const double S2 = 13.0 / 12.0 * t2 * t2 + 0.25 * u2 * u2;
   const double S3 = 13.0 / 12.0 * t3 * t3 + 0.25 * u3 * u3;
-  const double q1 = S1 + eps, q2 = S2 + eps, q3 = S3 + eps;
-  const double a1 = 0.1 / (q1 * q1), a2 = 0.6 / (q2 * q2), a3 = 0.3 / (q3 * q3);
-  const double is = 1.0 / (a1 + a2 + a3);
-  const double w1 = a1 * is, w2 = a2 * is, w3 = a3 * is;
+  const double sc = inv_pow2_of(eps);
+  const double es = eps * sc;
+  const double q1 = S1 * sc + es, q2 = S2 * sc + es, q3 = S3 * sc + es;
+  const double Q1 = q1 * q1, Q2 = q2 * q2, Q3 = q3 * q3;
+  const double n1 = 0.1 * (Q2 * Q3), n2 = 0.6 * (Q1 * Q3), n3 = 0.3 * (Q1 * Q2);
+  const double rn = rcp_nr(n1 + n2 + n3);
+  const double w1 = n1 * rn, w2 = n2 * rn, w3 = n3 * rn;
   D = w1 * p1 + w2 * p2 + w3 * p3;
-  const double b1 = -2.0 * w1 * (p1 - D) / q1;
-  const double b2 = -2.0 * w2 * (p2 - D) / q2;
-  const double b3 = -2.0 * w3 * (p3 - D) / q3;
+  const double rq = rcp_nr(q1 * q2 * q3) * sc;   // 1 / ((S1+eps)(S2+eps)(S3+eps)) / s^2
+  const double b1 = -2.0 * w1 * (p1 - D) * (q2 * q3 * rq);
+  const double b2 = -2.0 * w2 * (p2 - D) * (q1 * q3 * rq);
+  const double b3 = -2.0 * w3 * (p3 - D) * (q1 * q2 * rq);
   const double k1 = 13.0 / 6.0 * t1, l1 = 0.5 * u1;
   const double k2 = 13.0 / 6.0 * t2, l2 = 0.5 * u2;
   const double k3 = 13.0 / 6.0 * t3, l3 = 0.5 * u3;
@@ -123,7 +131,8 @@ struct AdjParams {
   const double* phi;      // stage input state u (stencil)
   const double* vel[3];   // velocity arrays
   const double* src_a;    // mu = coef * (ca * src_a + cb * src_b)
-  const double* src_b;
+  double* src_b;          // zeroed after reading when zero_b (a consumed T)
+  bool zero_b;
   double ca, cb, coef;
   double* src_out;        // optional: stores ca * src_a + cb * src_b
   double* T;              // += J(u)^T mu (atomic, zeroed by the caller)
@@ -181,15 +190,18 @@ __device__ __forceinline__ double load_bc(const AdjParams& p, int i, int j, int 
   return __ldg(p.phi + aix(p.gb, i, j, k));
 }
 
-// Transposed Jacobian of the upwind advection RHS, scatter form: every cell
-// c adds its partials -V_d(c) mu(c) dD_d(c)/du(p) to the cells p of its
-// stencil.  The z contributions go through a 7-plane register ring, the x/y
-// contributions through a shared accumulation plane; each plane's sums and
-// the tile-border contributions are added to T with atomics.
+// Transposed Jacobian of the upwind advection RHS.  Every cell c owns the
+// partials -V_d(c) mu(c) dD_d(c)/du(p) of its stencil points p.  The z
+// contributions go through a 7-plane register ring along the march; the x/y
+// contributions of a plane are written to shared memory (seven per axis per
+// cell) and gathered by the thread of each target cell, without atomics.
+// Each finished plane of the ring and the contributions to the neighbouring
+// tiles (3-cell strips) are added to T with atomics.
 __global__ void __launch_bounds__(kTX * kTY, 2)
 k_adjoint_stage(AdjParams p) {
   __shared__ double tile[kTY + 6][kTX + 6];
-  __shared__ double acc[kTY + 6][kTX + 6];
+  __shared__ double Cx[7][kTY][kTX];
+  __shared__ double Cy[7][kTY][kTX];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i = p.fb.lo[0] + (int)blockIdx.x * kTX + tx;
   const int j = p.fb.lo[1] + (int)blockIdx.y * kTY + ty;
@@ -204,97 +216,162 @@ k_adjoint_stage(AdjParams p) {
   const bool has_hy = (i <= hi0) && ((ty < 3) || (ty >= kTY - 3 && j <= hi1));
   const int tcol = (tx < 3) ? tx : tx + 6;
   const int trow = (ty < 3) ? ty : ty + 6;
+  // tiles whose stencils stay inside the domain load without boundary tests
+  const int x0 = p.fb.lo[0] + (int)blockIdx.x * kTX, y0 = p.fb.lo[1] + (int)blockIdx.y * kTY;
+  const bool inside = x0 - 3 >= p.fb.lo[0] && min(x0 + kTX - 1, hi0) + 3 <= hi0 &&
+                      y0 - 3 >= p.fb.lo[1] && min(y0 + kTY - 1, hi1) + 3 <= hi1 &&
+                      kb - 3 >= p.fb.lo[2] && ke + 3 <= p.fb.hi[2];
+  auto ld = [&](int a, int b, int c) -> double {
+    return inside ? __ldg(p.phi + aix(p.gb, a, b, c)) : load_bc(p, a, b, c);
+  };
 
-  // zero the accumulation plane (every cell of it, corners included)
-  for (int q = ty * kTX + tx; q < (kTY + 6) * (kTX + 6); q += kTX * kTY)
-    (&acc[0][0])[q] = 0.0;
+  // registers of the next plane (loaded while the current one is worked):
+  // the new top of the z window or the own cell (halo threads), the strip
+  // cells, and the own cell's velocity and adjoint sources
+  double nx_c = 0.0, nx_hx = 0.0, nx_hy = 0.0, nv0 = 0.0, nv1 = 0.0, nv2 = 0.0,
+         nsa = 0.0, nsb = 0.0;
+  auto prefetch = [&](int k) {
+    if (act) {
+      nx_c = ld(i, j, k + 3);
+      const long o = aix(p.gb, i, j, k);
+      nv0 = __ldg(p.vel[0] + o);
+      nv1 = __ldg(p.vel[1] + o);
+      nv2 = __ldg(p.vel[2] + o);
+      nsa = p.src_a[o];
+      if (p.src_b) nsb = p.src_b[o];
+    } else if (ctr_halo) {
+      nx_c = ld(i, j, k);
+    }
+    if (has_hx) nx_hx = ld(hx, j, k);
+    if (has_hy) nx_hy = ld(i, hj, k);
+  };
 
   double w[7], ring[7];
 #pragma unroll
   for (int m = 0; m < 7; m++) ring[m] = 0.0;
   if (act) {
 #pragma unroll
-    for (int m = 0; m < 6; m++) w[m + 1] = load_bc(p, i, j, kb - 3 + m);
+    for (int m = 0; m < 6; m++) w[m + 1] = ld(i, j, kb - 3 + m);
   }
+  prefetch(kb);
   for (int k = kb; k <= ke; ++k) {
+    const double vx = nv0, vy = nv1, vz = nv2, sa = nsa, sb = nsb;
     if (act) {
 #pragma unroll
       for (int m = 0; m < 6; m++) w[m] = w[m + 1];
-      w[6] = load_bc(p, i, j, k + 3);
+      w[6] = nx_c;
       tile[ty + 3][tx + 3] = w[3];
     } else if (ctr_halo) {
-      tile[ty + 3][tx + 3] = load_bc(p, i, j, k);
+      tile[ty + 3][tx + 3] = nx_c;
     }
-    if (has_hx) tile[ty + 3][tcol] = load_bc(p, hx, j, k);
-    if (has_hy) tile[trow][tx + 3] = load_bc(p, i, hj, k);
+    if (has_hx) tile[ty + 3][tcol] = nx_hx;
+    if (has_hy) tile[trow][tx + 3] = nx_hy;
     __syncthreads();
+    if (k < ke) prefetch(k + 1);
     if (act) {
       const long o = aix(p.gb, i, j, k);
-      double src = p.ca * p.src_a[o];
-      if (p.src_b) src += p.cb * p.src_b[o];
+      const double a0 = p.A[0][o], a1 = p.A[1][o], a2 = p.A[2][o];
+      double src = p.ca * sa;
+      if (p.src_b) {
+        src += p.cb * sb;
+        if (p.zero_b) p.src_b[o] = 0.0;
+      }
       if (p.src_out) p.src_out[o] = src;
       const double mu = p.coef * src;
-      double wx[7], wy[7], dx7[7], dy7[7], dz7[7];
+      // one axis at a time: its seven partials are consumed before the next
+      // axis is differentiated; targets outside the domain are folded back
+      // at once, the others wait in shared memory for the gather
+      double Dx, Dy, Dz;
+      {
+        double wx[7], d7[7];
 #pragma unroll
-      for (int m = 0; m < 7; m++) {
-        wx[m] = tile[ty + 3][tx + m];
-        wy[m] = tile[ty + m][tx + 3];
+        for (int m = 0; m < 7; m++) wx[m] = tile[ty + 3][tx + m];
+        Dx = upwind_grad(wx, p.inv[0], vx, d7);
+        const double sx = -vx * mu;
+#pragma unroll
+        for (int m = 0; m < 7; m++) {
+          double c = sx * d7[m];
+          const int ti = i + m - 3;
+          if (ti < p.fb.lo[0] || ti > hi0) {
+            if (c != 0.0) add_target(p, ti, j, k, c);
+            c = 0.0;
+          }
+          Cx[m][ty][tx] = c;
+        }
       }
-      const double vx = __ldg(p.vel[0] + o), vy = __ldg(p.vel[1] + o),
-                   vz = __ldg(p.vel[2] + o);
-      const double Dx = upwind_grad(wx, p.inv[0], vx, dx7);
-      const double Dy = upwind_grad(wy, p.inv[1], vy, dy7);
-      const double Dz = upwind_grad(w, p.inv[2], vz, dz7);
-      p.A[0][o] += -mu * Dx;
-      p.A[1][o] += -mu * Dy;
-      p.A[2][o] += -mu * Dz;
-      const double sx = -vx * mu, sy = -vy * mu, sz = -vz * mu;
+      {
+        double wy[7], d7[7];
+#pragma unroll
+        for (int m = 0; m < 7; m++) wy[m] = tile[ty + m][tx + 3];
+        Dy = upwind_grad(wy, p.inv[1], vy, d7);
+        const double sy = -vy * mu;
+#pragma unroll
+        for (int m = 0; m < 7; m++) {
+          double c = sy * d7[m];
+          const int tj = j + m - 3;
+          if (tj < p.fb.lo[1] || tj > hi1) {
+            if (c != 0.0) add_target(p, i, tj, k, c);
+            c = 0.0;
+          }
+          Cy[m][ty][tx] = c;
+        }
+      }
+      {
+        double d7[7];
+        Dz = upwind_grad(w, p.inv[2], vz, d7);
+        const double sz = -vz * mu;
+#pragma unroll
+        for (int m = 0; m < 7; m++) ring[m] += sz * d7[m];   // ring[m]: plane k+m-3
+      }
+      p.A[0][o] = a0 - mu * Dx;
+      p.A[1][o] = a1 - mu * Dy;
+      p.A[2][o] = a2 - mu * Dz;
+    } else {
 #pragma unroll
       for (int m = 0; m < 7; m++) {
-        // x and y targets: inside the domain through the shared plane,
-        // ghost targets folded back directly
-        const int ti = i + m - 3, tj = j + m - 3;
-        if (dx7[m] != 0.0) {
-          if (ti < p.fb.lo[0] || ti > p.fb.hi[0]) add_target(p, ti, j, k, sx * dx7[m]);
-          else atomicAdd(&acc[ty + 3][tx + m], sx * dx7[m]);
-        }
-        if (dy7[m] != 0.0) {
-          if (tj < p.fb.lo[1] || tj > p.fb.hi[1]) add_target(p, i, tj, k, sy * dy7[m]);
-          else atomicAdd(&acc[ty + m][tx + 3], sy * dy7[m]);
-        }
-        ring[m] += sz * dz7[m];   // ring[m] is plane k + m - 3
+        Cx[m][ty][tx] = 0.0;
+        Cy[m][ty][tx] = 0.0;
       }
     }
     __syncthreads();
-    // own cell: plane k's in-plane sum joins the ring; the ring's oldest
-    // plane (k-3) is complete and leaves through an atomic add
+    // the x/y contributions of this plane to target column c / row r of the
+    // tile (c, r may lie up to 3 outside it): sources s = c-3..c+3 in the tile
+    auto gather_x = [&](int c) {
+      double v = 0.0;
+#pragma unroll
+      for (int m = 0; m < 7; m++) {
+        const int s = c + 3 - m;
+        if (s >= 0 && s < kTX) v += Cx[m][ty][s];
+      }
+      return v;
+    };
+    auto gather_y = [&](int r) {
+      double v = 0.0;
+#pragma unroll
+      for (int m = 0; m < 7; m++) {
+        const int s = r + 3 - m;
+        if (s >= 0 && s < kTY) v += Cy[m][s][tx];
+      }
+      return v;
+    };
     if (act) {
-      ring[3] += acc[ty + 3][tx + 3];
-      acc[ty + 3][tx + 3] = 0.0;
+      // own cell: plane k's in-plane sum joins the ring; the ring's oldest
+      // plane (k-3) is complete and leaves through an atomic add
+      ring[3] += gather_x(tx) + gather_y(ty);
       if (ring[0] != 0.0) add_target(p, i, j, k - 3, ring[0]);
 #pragma unroll
       for (int m = 0; m < 6; m++) ring[m] = ring[m + 1];
       ring[6] = 0.0;
     }
-    // the tile's side strips hold contributions to neighbouring tiles
+    // contributions to the neighbouring tiles' cells next to this tile
     if (has_hx) {
-      const double v = acc[ty + 3][tcol];
+      const double v = gather_x(tcol - 3);
       if (v != 0.0) add_target(p, hx, j, k, v);
-      acc[ty + 3][tcol] = 0.0;
     }
     if (has_hy) {
-      const double v = acc[trow][tx + 3];
+      const double v = gather_y(trow - 3);
       if (v != 0.0) add_target(p, i, hj, k, v);
-      acc[trow][tx + 3] = 0.0;
     }
-    // partial tiles: cells past the fill box inside the tile got x/y
-    // contributions in the centre slots of inactive threads
-    if (ctr_halo) {
-      const double v = acc[ty + 3][tx + 3];
-      if (v != 0.0) add_target(p, i, j, k, v);
-      acc[ty + 3][tx + 3] = 0.0;
-    }
-    __syncthreads();
   }
   // planes ke-2 .. ke+3 still in the ring
   if (act) {
@@ -304,15 +381,17 @@ k_adjoint_stage(AdjParams p) {
   }
 }
 
-// lam' = 1/3 lam + 3/4 lam2 + lam1 + T1 (pointwise, fill box)
+// lam' = 1/3 lam + 3/4 lam2 + lam1 + T1 (pointwise, fill box); T1 is
+// consumed (zeroed for the next step's accumulation)
 __global__ void k_adj_combine(double* out, const double* lam, const double* lam2,
-                              const double* lam1, const double* T1, Box gb, FillBox fb) {
+                              const double* lam1, double* T1, Box gb, FillBox fb) {
   const int i = fb.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = fb.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
   if (i > fb.hi[0] || j > fb.hi[1]) return;
   for (int k = fb.lo[2] + blockIdx.z; k <= fb.hi[2]; k += gridDim.z) {
     const long o = aix(gb, i, j, k);
     out[o] = (1.0 / 3.0) * lam[o] + 0.75 * lam2[o] + lam1[o] + T1[o];
+    T1[o] = 0.0;
   }
 }
 
@@ -463,11 +542,20 @@ struct lsmgpu_adjoint {
   double* s1 = nullptr;         // stage buffers
   double* s2 = nullptr;
   std::vector<double*> ckpt;    // checkpoint states
-  std::vector<double*> seg;     // states of the segment being reversed
+  // two sets of segment buffers: [set][0] the states u_s of a segment,
+  // [set][1] and [set][2] their TVD-RK3 stage-1 and stage-2 states.  The
+  // segment before the one being reversed is recomputed into the other set
+  // on the auxiliary stream.
+  std::vector<double*> segs[2][3];
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ready[2] = {nullptr, nullptr};
+  cudaEvent_t freed[2] = {nullptr, nullptr};
+  cudaEvent_t start = nullptr;
   double* lam = nullptr;
   double* lam2 = nullptr;
   double* lam1 = nullptr;
-  double* T = nullptr;
+  double* T = nullptr;          // two accumulation buffers of J^T mu; each is
+  double* Tb = nullptr;         // zeroed by the kernel that consumes it
   double* A[3] = {nullptr, nullptr, nullptr};
   double* partials = nullptr;
   int nsteps = 0, every = 1;
@@ -521,11 +609,11 @@ cudaError_t fwd_step(lsmgpu_adjoint* h, double* out, const double* in, cudaStrea
   return fwd_stage(h, out, h->s2, in, 33, st);
 }
 
+// T += J(u)^T mu with mu = coef (ca sa + cb sb); T must be zero on entry, sb
+// (a consumed accumulation buffer, or null) is zeroed as it is read
 cudaError_t adj_kernel(lsmgpu_adjoint* h, const double* u, const double* sa, double ca,
-                       const double* sb, double cb, double coef, double* sout,
+                       double* sb, double cb, double coef, double* sout, double* T,
                        cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(h->T, 0, h->bytes, st);
-  if (e) return e;
   AdjParams p;
   p.phi = u;
   for (int d = 0; d < 3; d++) {
@@ -534,7 +622,8 @@ cudaError_t adj_kernel(lsmgpu_adjoint* h, const double* u, const double* sa, dou
     p.inv[d] = 1.0 / h->dx[d];
   }
   p.src_a = sa; p.ca = ca; p.src_b = sb; p.cb = cb; p.coef = coef; p.src_out = sout;
-  p.T = h->T;
+  p.zero_b = sb != nullptr;
+  p.T = T;
   p.gb = h->gb;
   p.fb = h->fb;
   dim3 grid((h->fb.n(0) + kTX - 1) / kTX, (h->fb.n(1) + kTY - 1) / kTY,
@@ -544,26 +633,40 @@ cudaError_t adj_kernel(lsmgpu_adjoint* h, const double* u, const double* sa, dou
   return cudaGetLastError();
 }
 
-// reverse one RK3 step whose input state is u: lam <- dJ/du
-cudaError_t adj_step(lsmgpu_adjoint* h, const double* u, cudaStream_t st) {
+// states u_s (s > first) of checkpoint segment c and the stage states of
+// every step of it, recomputed from the segment's checkpoint into buffer set b
+cudaError_t recompute_segment(lsmgpu_adjoint* h, int c, int b, cudaStream_t st) {
+  const int s0 = c * h->every, s1 = std::min(s0 + h->every, h->nsteps);
+  std::vector<double*>* set = h->segs[b];
   cudaError_t e;
-  // recompute the stage states phi1, phi2 of this step
-  if ((e = fwd_stage(h, h->s1, u, u, 1, st))) return e;
-  if ((e = fwd_stage(h, h->s2, h->s1, u, 32, st))) return e;
+  for (int s = s0; s < s1; s++) {
+    const int q = s - s0;
+    const double* u = q == 0 ? h->ckpt[c] : set[0][q];
+    if ((e = fwd_stage(h, set[1][q], u, u, 1, st))) return e;
+    if ((e = fwd_stage(h, set[2][q], set[1][q], u, 32, st))) return e;
+    if (s + 1 < s1 && (e = fwd_stage(h, set[0][q + 1], set[2][q], u, 33, st))) return e;
+  }
+  return cudaSuccess;
+}
+
+// reverse one RK3 step whose input state is u and stage states s1, s2:
+// lam <- dJ/du
+cudaError_t adj_step(lsmgpu_adjoint* h, const double* u, const double* s1,
+                     const double* s2, cudaStream_t st) {
+  cudaError_t e;
   const double dt = h->dt;
   // stage 3: mu3 = 2/3 dt lam; T <- J(phi2)^T mu3
-  if ((e = adj_kernel(h, h->s2, h->lam, 1.0, nullptr, 0.0, (2.0 / 3.0) * dt, nullptr, st)))
+  if ((e = adj_kernel(h, s2, h->lam, 1.0, nullptr, 0.0, (2.0 / 3.0) * dt, nullptr, h->T,
+                      st)))
     return e;
-  // stage 2: lam2 = 2/3 lam + T3 (T3 moved to lam1 because the kernel
-  // zeroes T); mu2 = 1/4 dt lam2; T <- J(phi1)^T mu2
-  if ((e = cudaMemcpyAsync(h->lam1, h->T, h->bytes, cudaMemcpyDeviceToDevice, st))) return e;
-  if ((e = adj_kernel(h, h->s1, h->lam, 2.0 / 3.0, h->lam1, 1.0, 0.25 * dt, h->lam2, st)))
+  // stage 2: lam2 = 2/3 lam + T3 (T consumed); mu2 = 1/4 dt lam2;
+  // Tb <- J(phi1)^T mu2
+  if ((e = adj_kernel(h, s1, h->lam, 2.0 / 3.0, h->T, 1.0, 0.25 * dt, h->lam2, h->Tb, st)))
     return e;
-  // stage 1: lam1 = 1/4 lam2 + T2 (T2 moved to lam1); mu1 = dt lam1;
+  // stage 1: lam1 = 1/4 lam2 + T2 (Tb consumed); mu1 = dt lam1;
   // T <- J(u)^T mu1
-  if ((e = cudaMemcpyAsync(h->lam1, h->T, h->bytes, cudaMemcpyDeviceToDevice, st))) return e;
-  if ((e = adj_kernel(h, u, h->lam2, 0.25, h->lam1, 1.0, dt, h->lam1, st))) return e;
-  // lam <- 1/3 lam + 3/4 lam2 + lam1 + T1
+  if ((e = adj_kernel(h, u, h->lam2, 0.25, h->Tb, 1.0, dt, h->lam1, h->T, st))) return e;
+  // lam <- 1/3 lam + 3/4 lam2 + lam1 + T1 (T consumed)
   dim3 blk(32, 4, 1), grid((h->fb.n(0) + 31) / 32, (h->fb.n(1) + 3) / 4,
                            h->fb.n(2) < 65535 ? h->fb.n(2) : 65535);
   k_adj_combine<<<grid, blk, 0, st>>>(h->lam, h->lam, h->lam2, h->lam1, h->T, h->gb, h->fb);
@@ -660,9 +763,17 @@ int lsmgpu_adjoint_create(lsmgpu_adjoint** out, const int n[3], const double dx[
   h->lam2 = dalloc(h->bytes, ok);
   h->lam1 = dalloc(h->bytes, ok);
   h->T = dalloc(h->bytes, ok);
+  h->Tb = dalloc(h->bytes, ok);
   h->partials = dalloc(kLossBlocks * sizeof(double), ok);
   for (int c = 0; c < nck; c++) h->ckpt.push_back(dalloc(h->bytes, ok));
-  for (int c = 0; c < checkpoint_every; c++) h->seg.push_back(dalloc(h->bytes, ok));
+  for (int b = 0; b < 2; b++)
+    for (int v = 0; v < 3; v++)
+      for (int c = 0; c < checkpoint_every; c++) h->segs[b][v].push_back(dalloc(h->bytes, ok));
+  ok = ok && cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking) == cudaSuccess;
+  for (int b = 0; ok && b < 2; b++)
+    ok = cudaEventCreateWithFlags(&h->ready[b], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h->freed[b], cudaEventDisableTiming) == cudaSuccess;
+  ok = ok && cudaEventCreateWithFlags(&h->start, cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
     set_error(LSMGPU_ERR_ALLOC, std::string(R) + ": device allocation failed");
     lsmgpu_adjoint_destroy(h);
@@ -676,13 +787,19 @@ int lsmgpu_adjoint_destroy(lsmgpu_adjoint* h) {
   if (!h) return LSMGPU_SUCCESS;
   double* ps[] = {h->vel[0], h->vel[1], h->vel[2], h->A[0], h->A[1], h->A[2],
                   h->theta, h->grad_theta, h->target, h->phi, h->s1, h->s2,
-                  h->lam, h->lam2, h->lam1, h->T, h->partials};
+                  h->lam, h->lam2, h->lam1, h->T, h->Tb, h->partials};
   for (double* p : ps)
     if (p) cudaFree(p);
   for (double* p : h->ckpt)
     if (p) cudaFree(p);
-  for (double* p : h->seg)
-    if (p) cudaFree(p);
+  if (h->aux) cudaStreamSynchronize(h->aux);
+  for (auto& set : h->segs)
+    for (auto& v : set)
+      for (double* p : v)
+        if (p) cudaFree(p);
+  for (cudaEvent_t ev : {h->ready[0], h->ready[1], h->freed[0], h->freed[1], h->start})
+    if (ev) cudaEventDestroy(ev);
+  if (h->aux) cudaStreamDestroy(h->aux);
   delete h;
   return LSMGPU_SUCCESS;
 }
@@ -817,18 +934,33 @@ int lsmgpu_adjoint_backward(lsmgpu_adjoint* h, double seed, double* grad_theta,
   bool ok = cuda_ok(cudaGetLastError(), R);
   const size_t m3 = (size_t)h->spl.m * h->spl.m * h->spl.m;
   for (int d = 0; ok && d < 3; d++) ok = cuda_ok(cudaMemsetAsync(h->A[d], 0, h->bytes, st), R);
+  // the accumulation buffers start at zero (a failed earlier sweep may have
+  // left partial sums); afterwards their consumers keep them zeroed
+  ok = ok && cuda_ok(cudaMemsetAsync(h->T, 0, h->bytes, st), R) &&
+       cuda_ok(cudaMemsetAsync(h->Tb, 0, h->bytes, st), R);
   ok = ok && cuda_ok(cudaMemsetAsync(h->grad_theta, 0, 3 * m3 * sizeof(double), st), R);
   const int nck = (int)h->ckpt.size();
+  // the auxiliary stream starts after the forward run's checkpoints
+  ok = ok && cuda_ok(cudaEventRecord(h->start, st), R) &&
+       cuda_ok(cudaStreamWaitEvent(h->aux, h->start, 0), R);
+  if (ok) ok = cuda_ok(recompute_segment(h, nck - 1, (nck - 1) & 1, st), R);
   for (int c = nck - 1; ok && c >= 0; c--) {
-    const int s0 = c * h->every, s1 = std::min(s0 + h->every, h->nsteps);
-    // states u_s of the segment, recomputed from its checkpoint
-    std::vector<double*> u(s1 - s0);
-    u[0] = h->ckpt[c];
-    for (int s = s0 + 1; ok && s < s1; s++) {
-      u[s - s0] = h->seg[s - s0];
-      ok = cuda_ok(fwd_step(h, u[s - s0], u[s - s0 - 1], st), R);
+    const int b = c & 1;
+    if (c > 0) {
+      // segment c-1 into the other set once its last reader has finished
+      const int ob = (c - 1) & 1;
+      ok = cuda_ok(cudaStreamWaitEvent(h->aux, h->freed[ob], 0), R) &&
+           cuda_ok(recompute_segment(h, c - 1, ob, h->aux), R) &&
+           cuda_ok(cudaEventRecord(h->ready[ob], h->aux), R);
     }
-    for (int s = s1 - 1; ok && s >= s0; s--) ok = cuda_ok(adj_step(h, u[s - s0], st), R);
+    if (ok && c < nck - 1) ok = cuda_ok(cudaStreamWaitEvent(st, h->ready[b], 0), R);
+    const int s0 = c * h->every, s1 = std::min(s0 + h->every, h->nsteps);
+    for (int s = s1 - 1; ok && s >= s0; s--) {
+      const int q = s - s0;
+      const double* u = q == 0 ? h->ckpt[c] : h->segs[b][0][q];
+      ok = cuda_ok(adj_step(h, u, h->segs[b][1][q], h->segs[b][2][q], st), R);
+    }
+    ok = ok && cuda_ok(cudaEventRecord(h->freed[b], st), R);
   }
   if (ok) {
     const int m = h->spl.m;
