@@ -296,6 +296,11 @@ def run_ours(args, world, rank, local, pg):
     if not args.no_adjoint:
         adjoint_res = run_adjoint()
 
+    deformation_res = None
+    if not args.no_deformation:
+        deformation_res = run_config3(lib, pg, world,
+                                      n_full=512 if args.config3_full else 256)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(cfg)
@@ -312,6 +317,7 @@ def run_ours(args, world, rank, local, pg):
                    "l2": "inputs larger than L2 (144 MB per field, 6 fields live)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "fp32": fp32, "batched": batched_res, "adjoint": adjoint_res,
+        "deformation": deformation_res,
         "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk,
     }
@@ -385,6 +391,91 @@ def run_adjoint(n_fd=20, h=1e-6):
                          "max_err_over_max_grad": worst_abs,
                          "max_rel_err_components_above_1pct": worst_sig,
                          "loss_difference": "cell by cell from the two final states"}}
+
+
+def deformation_run(ws, d_phi, fb, cfg, timer):
+    """Advance to t_end in chunks sized from the last dt (the driver clips
+    the final dt at t_end, so no step is taken past it); device time and
+    step count."""
+    from lsmlib_b200 import gpu
+    t_end, ms, steps, chunk = cfg["t_end"], 0.0, 0, 16
+    while True:
+        timer.start()
+        ws.deformation(d_phi, fb, cfg["dx"], cfg["x_lo"], period=cfg["period"],
+                       cfl=cfg["cfl"], t_end=t_end, nsteps=chunk)
+        timer.stop()
+        ms += timer.ms()
+        steps += chunk
+        t, dt = ws.time()
+        left = t_end - t
+        if left <= 1e-13 * t_end:
+            return ms, steps, t
+        chunk = max(1, min(2048, int(0.9 * left / max(dt, 1e-300))))
+
+
+def interface_errors(phi, ref, dx, band_dx=3):
+    """max and mean |phi - ref| in the band |ref| < band_dx dx, and the relative
+    change of the enclosed volume sum H(-phi) dx^3 (LSM_HEAVISIDE, eps 1.5 dx)."""
+    from lsmlib_b200.adjoint import heaviside
+    band = np.abs(ref) < band_dx * dx
+    d = np.abs(phi - ref)
+    v = float(np.sum(heaviside(-phi, 1.5 * dx)))
+    v0 = float(np.sum(heaviside(-ref, 1.5 * dx)))
+    return {"max_abs_band": float(d[band].max()), "mean_abs_band": float(d[band].mean()),
+            "band": "|phi0| < %d dx" % band_dx, "volume_rel_change": (v - v0) / v0}
+
+
+def run_config3(lib, pg, world, n_window=512, window=100, n_full=256):
+    """Config 3: LeVeque's deformation of a sphere (r 0.15 at (0.35,0.35,0.35)
+    on [0,1]^3, period 3) by WENO5 + TVD-RK3 at CFL 0.5, velocity evaluated
+    in the stage kernels.  Throughput of FP64 and FP32 over the first
+    `window` steps at n_window^3; the full reversal to t = 3 at n_full^3 with
+    the errors against the initial interface and FP32 against FP64."""
+    from lsmlib_b200 import gpu, integrator, workloads
+    timer = gpu.Timer()
+    res = {"workload": "LeVeque deformation of a sphere, period 3, WENO5 + TVD-RK3, "
+                       "CFL 0.5, velocity in-kernel (no velocity arrays)"}
+    cfg = workloads.config3(n_window)
+    gb, fb = workloads.boxes(cfg["n"])
+    cells = cfg["n"][0] * cfg["n"][1] * cfg["n"][2]
+    for prec, key in ((8, "fp64"), (4, "fp32")):
+        dtype = np.float64 if prec == 8 else np.float32
+        ws = integrator.Workspace(gb, prec)
+        d = gpu.DeviceArray.from_host(cfg["phi"].astype(dtype))
+        ws.deformation(d, fb, cfg["dx"], cfg["x_lo"], period=cfg["period"], cfl=cfg["cfl"],
+                       t_end=cfg["t_end"], nsteps=3)
+        barrier(pg)
+        timer.start()
+        ws.deformation(d, fb, cfg["dx"], cfg["x_lo"], period=cfg["period"], cfl=cfg["cfl"],
+                       t_end=cfg["t_end"], nsteps=window)
+        timer.stop()
+        ms = max_over_ranks(pg, timer.ms())
+        res["window_%d_%s" % (n_window, key)] = {
+            "value": world * cells * window / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms / window, "steps": window}
+        del d, ws
+    cfg = workloads.config3(n_full)
+    gb, fb = workloads.boxes(cfg["n"])
+    inner = tuple(slice(3, 3 + v) for v in cfg["n"])
+    phi0 = cfg["phi"][inner]
+    finals = {}
+    for prec, key in ((8, "fp64"), (4, "fp32")):
+        dtype = np.float64 if prec == 8 else np.float32
+        ws = integrator.Workspace(gb, prec)
+        d = gpu.DeviceArray.from_host(cfg["phi"].astype(dtype))
+        ms, steps, t = deformation_run(ws, d, fb, cfg, timer)
+        finals[key] = d.download()[inner].astype(np.float64)
+        res["reversal_%d_%s" % (n_full, key)] = dict(
+            {"steps": steps, "t": t, "ms": ms,
+             "value": n_full ** 3 * steps / (ms / 1e3), "unit": UNIT},
+            vs_initial=interface_errors(finals[key], phi0, cfg["dx"][0]))
+        del d, ws
+    diff = np.abs(finals["fp32"] - finals["fp64"])
+    band = np.abs(finals["fp64"]) < 5 * cfg["dx"][0]
+    res["reversal_%d_fp32" % n_full]["error_vs_fp64"] = {
+        "max_abs": float(diff.max()), "l1_mean": float(diff.mean()),
+        "max_abs_band_5dx": float(diff[band].max())}
+    return res
 
 
 def run_batched(lib, pg, world, steps=50, warmup=3):
@@ -570,6 +661,10 @@ def main():
                     help="skip the adjoint leg (config 5)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched uneven-grid leg (config 4)")
+    ap.add_argument("--no-deformation", action="store_true",
+                    help="skip the deformation leg (config 3)")
+    ap.add_argument("--config3-full", action="store_true",
+                    help="run the config-3 full reversal at 512^3 (minutes) instead of 256^3")
     ap.add_argument("--size", type=int, default=256, help="interior cells per axis")
     ap.add_argument("--profile", action="store_true",
                     help="only launch the two fused stage kernels twice each "

@@ -2,7 +2,7 @@
 // include/lsmgpu/lsmgpu.h).
 //
 // A workspace owns the stage buffers of one grid (phi^(1), phi^(2), the stage
-// RHS, phi0 for the reinitialization sign, velocity buffers, device scalars
+// RHS, phi0 for the reinitialization sign, deformation sine tables, device scalars
 // dt and t, and the CFL partial maxima).  The drivers reproduce the call
 // order of the reference's integrators
 //   LevelSetFunctionIntegrator::advanceLevelSetEqnUsingTVDRK3
@@ -31,8 +31,9 @@ struct lsmgpu_workspace {
   void* phi2 = nullptr;
   void* rhs = nullptr;
   void* phi0 = nullptr;
-  void* vel[3] = {nullptr, nullptr, nullptr};
-  double* scal = nullptr;   // [0] dt, [1] t, [2] dt of the last step
+  double* defo_tab = nullptr;   // deformation sine tables (see stage.cuh)
+  size_t defo_len = 0;
+  double* scal = nullptr;   // device scalars (kDt, kT, kDtLast, kG0..kG0+2)
   double* partials = nullptr;
   int npart = 0;
   unsigned bc_mask = 0x3fu;
@@ -43,7 +44,9 @@ struct lsmgpu_workspace {
 
 namespace {
 
-enum { kDt = 0, kT = 1, kDtLast = 2, kNumScal = 4 };
+// device scalars of a workspace: dt, t, the dt of the last step, and g of
+// the deformation field at t, t + dt, t + dt/2 (the three stage times)
+enum { kDt = 0, kT = 1, kDtLast = 2, kG0 = 3, kNumScal = 8 };
 
 __device__ __forceinline__ double gmax(double m, double v) { return v > m ? v : m; }
 
@@ -72,35 +75,81 @@ __global__ void k_advance_t(double* scal) {
   scal[kDtLast] = scal[kDt];
 }
 
-// LeVeque's 3D deformation field at time t + c*dt, g(t) = cos(pi t / period):
-// u = 2 sin^2(pi x) sin(2 pi y) sin(2 pi z) g, v = -sin(2 pi x) sin^2(pi y)
-// sin(2 pi z) g, w = -sin(2 pi x) sin(2 pi y) sin^2(pi z) g, cell centres
-// x_i = x_lo + (i + 1/2) dx.
-template <typename T>
-__global__ void k_deformation(T* vx, T* vy, T* vz, Box gb, FillBox fb,
-                              double x0, double y0, double z0, double dx,
-                              double dy, double dz, const double* scal,
-                              double c, double period) {
-  const int i = fb.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = fb.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
-  if (i > fb.hi[0] || j > fb.hi[1]) return;
+// LeVeque's 3D deformation field (deformation_velocity, stage.cuh) at cell
+// centres x_i = x_lo + (i + 1/2) dx, with g(t) = cos(pi t / period).  The
+// sines of every fill-box coordinate are tabulated once per call and g once
+// per stage time, so the stage kernels and the CFL reduction evaluate the
+// field without velocity arrays; both are computed here, in the translation
+// unit without FMA contraction, from the same expressions as before the
+// tabulation.
+__global__ void k_deform_tables(double* tab, FillBox fb, double x0, double y0,
+                                double z0, double dx, double dy, double dz) {
+  const int n0 = fb.n(0), n1 = fb.n(1), n2 = fb.n(2);
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  double x;
+  double* out;
+  int n;
+  if (q < n0) {
+    x = x0 + (fb.lo[0] + q + 0.5) * dx; out = tab + q; n = n0;
+  } else if (q < n0 + n1) {
+    x = y0 + (fb.lo[1] + (q - n0) + 0.5) * dy; out = tab + 2 * n0 + (q - n0); n = n1;
+  } else if (q < n0 + n1 + n2) {
+    x = z0 + (fb.lo[2] + (q - n0 - n1) + 0.5) * dz;
+    out = tab + 2 * n0 + 2 * n1 + (q - n0 - n1); n = n2;
+  } else {
+    return;
+  }
+  out[0] = sin(M_PI * x);
+  out[n] = sin(2.0 * M_PI * x);
+}
+
+__device__ __forceinline__ double deform_g(const double* scal, double c, double period) {
   const double t = scal[kT] + c * scal[kDt];
-  const double g = cos(M_PI * t / period);
-  const double x = x0 + (i + 0.5) * dx, y = y0 + (j + 0.5) * dy;
-  const double sx = sin(M_PI * x), s2x = sin(2.0 * M_PI * x);
-  const double sy = sin(M_PI * y), s2y = sin(2.0 * M_PI * y);
-  for (int k = fb.lo[2] + blockIdx.z; k <= fb.hi[2]; k += gridDim.z) {
-    const double z = z0 + (k + 0.5) * dz;
-    const double sz = sin(M_PI * z), s2z = sin(2.0 * M_PI * z);
-    const long o = (long)(i - gb.lo[0]) + gb.sy() * (j - gb.lo[1]) +
-                   gb.sz() * (k - gb.lo[2]);
-    vx[o] = (T)(2.0 * sx * sx * s2y * s2z * g);
-    vy[o] = (T)(-s2x * sy * sy * s2z * g);
-    vz[o] = (T)(-s2x * s2y * sz * sz * g);
+  return cos(M_PI * t / period);
+}
+
+// g at the three stage times t, t + dt, t + dt/2 (after this step's dt)
+__global__ void k_deform_g(double* scal, double period) {
+  const double c[3] = {0.0, 1.0, 0.5};
+  if (threadIdx.x < 3) scal[kG0 + threadIdx.x] = deform_g(scal, c[threadIdx.x], period);
+}
+
+// the CFL reduction of the deformation field at time t (FP64), over the
+// velocity components rounded to the working precision T as the stage
+// kernels see them
+template <typename T>
+__global__ void k_deform_partials(const double* tab, FillBox fb, const double* scal,
+                                  double period, double ix, double iy, double iz,
+                                  double* partials) {
+  const double g = deform_g(scal, 0.0, period);
+  const int n0 = fb.n(0), n1 = fb.n(1), n2 = fb.n(2);
+  double m = -1.0;
+  const long n = fb.count();
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+       t += (long)gridDim.x * blockDim.x) {
+    const int a = (int)(t % n0);
+    const long r = t / n0;
+    const int b = (int)(r % n1), c = (int)(r / n1);
+    DeformSines s;
+    s.sx = tab[a]; s.s2x = tab[n0 + a];
+    s.sy = tab[2 * n0 + b]; s.s2y = tab[2 * n0 + n1 + b];
+    s.sz = tab[2 * n0 + 2 * n1 + c]; s.s2z = tab[2 * n0 + 2 * n1 + n2 + c];
+    T u, v, w;
+    deformation_velocity(s, g, u, v, w);
+    const double h = fabs((double)u) * ix + fabs((double)v) * iy + fabs((double)w) * iz;
+    m = gmax(m, h);
+  }
+  __shared__ double red[8];
+  for (int o = 16; o > 0; o >>= 1) m = gmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = gmax(m, red[w]);
+    partials[blockIdx.x] = gmax(red[0], m);
   }
 }
 
-// the CFL reduction of the deformation field at time t (FP64)
+// the CFL reduction of velocity arrays (FP64)
 template <typename T>
 __global__ void k_adv_partials(const T* vx, const T* vy, const T* vz, Box gb,
                                FillBox fb, double ix, double iy, double iz,
@@ -321,8 +370,8 @@ int lsmgpu_workspace_create(lsmgpu_workspace** out, const int gb[6],
 
 int lsmgpu_workspace_destroy(lsmgpu_workspace* ws) {
   if (!ws) return LSMGPU_SUCCESS;
-  void* ps[] = {ws->phi1, ws->phi2, ws->rhs, ws->phi0, ws->vel[0], ws->vel[1],
-                ws->vel[2], ws->scal, ws->partials};
+  void* ps[] = {ws->phi1, ws->phi2, ws->rhs, ws->phi0, ws->defo_tab, ws->scal,
+                ws->partials};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete ws;
@@ -532,48 +581,48 @@ int lsmgpu_deformation_tvdrk3(lsmgpu_workspace* ws, void* phi, const int fb[6],
     set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": bad x_lo/period");
     return LSMGPU_ERR_INVALID_VALUE;
   }
-  for (int d = 0; d < 3; d++)
-    if (!ws->vel[d] && !(ws->vel[d] = ws_alloc(ws->bytes, R))) return LSMGPU_ERR_ALLOC;
+  // sine tables of the fill-box coordinates (sin(pi x), sin(2 pi x) per axis)
+  const size_t len = 2 * ((size_t)f.n(0) + f.n(1) + f.n(2));
+  if (ws->defo_len < len) {
+    if (ws->defo_tab) cudaFree(ws->defo_tab);
+    ws->defo_len = 0;
+    if (!(ws->defo_tab = (double*)ws_alloc(len * sizeof(double), R))) return LSMGPU_ERR_ALLOC;
+    ws->defo_len = len;
+  }
   cudaStream_t st = cur_stream();
+  const int nt = f.n(0) + f.n(1) + f.n(2);
+  k_deform_tables<<<(nt + 127) / 128, 128, 0, st>>>(ws->defo_tab, f, x_lo[0], x_lo[1],
+                                                    x_lo[2], dx[0], dx[1], dx[2]);
+  ++launch_counter();
   const double tiny = ws->prec == 8 ? Consts<double>::tiny : (double)Consts<float>::tiny;
   const double inv[3] = {1.0 / dx[0], 1.0 / dx[1], 1.0 / dx[2]};
-  dim3 vb(32, 4, 1), vg((f.n(0) + 31) / 32, (f.n(1) + 3) / 4,
-                        f.n(2) < 65535 ? f.n(2) : 65535);
-  auto velocity = [&](double c) {
-    if (ws->prec == 8)
-      k_deformation<double><<<vg, vb, 0, st>>>(
-          (double*)ws->vel[0], (double*)ws->vel[1], (double*)ws->vel[2], ws->gb,
-          f, x_lo[0], x_lo[1], x_lo[2], dx[0], dx[1], dx[2], ws->scal, c, period);
-    else
-      k_deformation<float><<<vg, vb, 0, st>>>(
-          (float*)ws->vel[0], (float*)ws->vel[1], (float*)ws->vel[2], ws->gb, f,
-          x_lo[0], x_lo[1], x_lo[2], dx[0], dx[1], dx[2], ws->scal, c, period);
-    ++launch_counter();
-  };
   for (int s = 0; s < nsteps; s++) {
-    // dt from the velocity at t (the stage-1 field)
-    velocity(0.0);
+    // dt from the field at t (the stage-1 field)
     if (ws->prec == 8)
-      k_adv_partials<double><<<kAdvRedBlocks, 256, 0, st>>>(
-          (const double*)ws->vel[0], (const double*)ws->vel[1],
-          (const double*)ws->vel[2], ws->gb, f, inv[0], inv[1], inv[2], ws->partials);
+      k_deform_partials<double><<<kAdvRedBlocks, 256, 0, st>>>(
+          ws->defo_tab, f, ws->scal, period, inv[0], inv[1], inv[2], ws->partials);
     else
-      k_adv_partials<float><<<kAdvRedBlocks, 256, 0, st>>>(
-          (const float*)ws->vel[0], (const float*)ws->vel[1],
-          (const float*)ws->vel[2], ws->gb, f, inv[0], inv[1], inv[2], ws->partials);
+      k_deform_partials<float><<<kAdvRedBlocks, 256, 0, st>>>(
+          ws->defo_tab, f, ws->scal, period, inv[0], inv[1], inv[2], ws->partials);
     k_dt_finish<<<1, 256, 0, st>>>(ws->partials, kAdvRedBlocks, cfl, tiny, ws->scal,
                                    t_end);
-    launch_counter() += 2;
+    k_deform_g<<<1, 32, 0, st>>>(ws->scal, period);
+    launch_counter() += 3;
     StageArgs a = base_args(ws, f, dx);
-    for (int d = 0; d < 3; d++) a.aux[d] = ws->vel[d];
+    a.defo_tab = ws->defo_tab;
+    a.defo_off[0] = 0;
+    a.defo_off[1] = 2 * f.n(0);
+    a.defo_off[2] = 2 * (f.n(0) + f.n(1));
+    // velocity at t, t + dt, t + dt/2 for the three stages
+    a.g_dev = ws->scal + kG0;
     a.out = ws->phi1; a.phi_s = phi; a.phi_n = phi; a.rk_kind = 1;
-    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
-    velocity(1.0);
+    if (!cuda_ok(stage(kStageDeformation, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
+    a.g_dev = ws->scal + kG0 + 1;
     a.out = ws->phi2; a.phi_s = ws->phi1; a.rk_kind = 32;
-    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
-    velocity(0.5);
+    if (!cuda_ok(stage(kStageDeformation, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
+    a.g_dev = ws->scal + kG0 + 2;
     a.out = phi; a.phi_s = ws->phi2; a.rk_kind = 33;
-    if (!cuda_ok(stage(kStageAdvect, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(stage(kStageDeformation, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
     k_advance_t<<<1, 1, 0, st>>>(ws->scal);
     ++launch_counter();
     ws->steps++;

@@ -32,7 +32,8 @@ enum StageKind {
   kStageNormal = 1,    // normal speed array: WENO5 +-, Godunov, -F|grad phi|
   kStageReinit = 2,    // reinitialization RHS, sign from phi_s (or phi0)
   kStageNormalRhs = 3, // normal speed, writes L(phi) and CFL maxima only
-  kStageAdvectConst = 4  // constant velocity vel_const: upwind WENO5, -V.grad
+  kStageAdvectConst = 4, // constant velocity vel_const: upwind WENO5, -V.grad
+  kStageDeformation = 5  // LeVeque's deformation field from sine tables
 };
 
 template <typename T>
@@ -58,7 +59,29 @@ struct StageParams {
   int fp64_policy;     // FP32 form: kFp64Kinks | kFp64Sign (see below)
   unsigned sr_seed;    // FP32 form: nonzero = stochastic rounding of out
   T vel_const[3];      // kStageAdvectConst: the grid's constant velocity
+  // kStageDeformation: sin(pi x), sin(2 pi x) of the fill-box cell centres
+  // of axis d at defo_tab + defo_off[d] (n_d values each, one after the
+  // other) and g(t + c dt) at *g_dev
+  const double* defo_tab;
+  int defo_off[3];
+  const double* g_dev;
 };
+
+// LeVeque's 3D deformation velocity of a cell from its sine values and g,
+// in the expression order of the reference-layout velocity arrays
+// (u = 2 sin^2(pi x) sin(2 pi y) sin(2 pi z) g, v = -sin(2 pi x) sin^2(pi y)
+// sin(2 pi z) g, w = -sin(2 pi x) sin(2 pi y) sin^2(pi z) g); products only,
+// so no FMA contraction can change them.
+struct DeformSines {
+  double sx, s2x, sy, s2y, sz, s2z;
+};
+template <typename T>
+__device__ __forceinline__ void deformation_velocity(const DeformSines& s, double g,
+                                                     T& u, T& v, T& w) {
+  u = (T)(2.0 * s.sx * s.sx * s.s2y * s.s2z * g);
+  v = (T)(-s.s2x * s.sy * s.sy * s.s2z * g);
+  w = (T)(-s.s2x * s.s2y * s.sz * s.sz * g);
+}
 
 // FP64 parts of the FP32 form: kFp64Kinks recomputes in FP64 the WENO5
 // stencils whose smoothness indicators differ by more than a factor 1e3;
@@ -347,6 +370,17 @@ __device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
       T a0 = T(0), a1 = T(0), a2 = T(0), uc = T(0);
       if (KIND == kStageAdvect) {
         a0 = __ldg(p.aux0 + o); a1 = __ldg(p.aux1 + o); a2 = __ldg(p.aux2 + o);
+      } else if (KIND == kStageDeformation) {
+        const int nx = p.fb.hi[0] - p.fb.lo[0] + 1, ny = p.fb.hi[1] - p.fb.lo[1] + 1,
+                  nz = p.fb.hi[2] - p.fb.lo[2] + 1;
+        const double* tx_ = p.defo_tab + p.defo_off[0] + (i - p.fb.lo[0]);
+        const double* ty_ = p.defo_tab + p.defo_off[1] + (j - p.fb.lo[1]);
+        const double* tz_ = p.defo_tab + p.defo_off[2] + (k - p.fb.lo[2]);
+        DeformSines s;
+        s.sx = __ldg(tx_); s.s2x = __ldg(tx_ + nx);
+        s.sy = __ldg(ty_); s.s2y = __ldg(ty_ + ny);
+        s.sz = __ldg(tz_); s.s2z = __ldg(tz_ + nz);
+        deformation_velocity(s, __ldg(p.g_dev), a0, a1, a2);
       } else if (KIND == kStageAdvectConst) {
         a0 = p.vel_const[0]; a1 = p.vel_const[1]; a2 = p.vel_const[2];
       } else if (KIND == kStageNormal || KIND == kStageNormalRhs ||
@@ -362,7 +396,7 @@ __device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
       }
       const T ztol = stage_zero_tol<T>();
       T L;
-      if (KIND == kStageAdvect || KIND == kStageAdvectConst) {
+      if (KIND == kStageAdvect || KIND == kStageAdvectConst || KIND == kStageDeformation) {
         // LSM3D_UPWIND_HJ_WENO5 + LSM3D_ADD_ADVECTION_TERM_TO_LSE_RHS
         T gx = T(0), gy = T(0), gz = T(0);
         if (!(fabsT(a0) < ztol))

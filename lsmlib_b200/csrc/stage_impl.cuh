@@ -31,6 +31,9 @@ StageParams<T> to_params(const StageArgs& a) {
   p.use_phi0 = a.use_phi0;
   p.fp64_policy = a.fp64_policy;
   p.sr_seed = a.sr_seed;
+  p.defo_tab = a.defo_tab;
+  for (int d = 0; d < 3; d++) p.defo_off[d] = a.defo_off[d];
+  p.g_dev = a.g_dev;
   return p;
 }
 
@@ -52,9 +55,14 @@ cudaError_t launch_t(int kind, const StageArgs& a, cudaStream_t st) {
     case kStageReinit:
       k_stage<T, kStageReinit, STAGE_FAST, TX, TY, TZ><<<grid, blk, 0, st>>>(p);
       break;
-    default:
+    case kStageDeformation:
+      k_stage<T, kStageDeformation, STAGE_FAST, TX, TY, TZ><<<grid, blk, 0, st>>>(p);
+      break;
+    case kStageNormalRhs:
       k_stage<T, kStageNormalRhs, STAGE_FAST, TX, TY, TZ><<<grid, blk, 0, st>>>(p);
       break;
+    default:
+      return cudaErrorInvalidValue;
   }
   ++launch_counter();
   return cudaGetLastError();

@@ -25,6 +25,9 @@ struct StageArgs {
   int use_phi0;
   int fp64_policy;  // kFp64Kinks | kFp64Sign | kStochRound (FP32 form)
   unsigned sr_seed; // nonzero: stochastic rounding of the output (FP32)
+  const double* defo_tab;  // kStageDeformation (see StageParams)
+  int defo_off[3];
+  const double* g_dev;
 };
 
 // tile of the stage kernels: TX x TY cells per block, TZ planes per block
