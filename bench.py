@@ -47,6 +47,13 @@ WORKLOAD = ("256^3 normal-velocity level set (6 spheres, F = 1 + 0.2 sin sin sin
             "HJ-WENO5 + Godunov + TVD-RK3, CFL 0.5, reinit every 10 steps x 20")
 
 
+
+# DRAM bytes (read + write) per launch and FP64-pipe utilisation of the fused
+# stage kernels on the 256^3 workload, from the ncu capture summarised in
+# profiles/k_stage_fp64_config2_256.md (distinct phi_s and phi^n)
+NCU_TRAFFIC = {"stage_reinit_rk32": 393.7e6, "stage_normal_rk32": 535.6e6}
+NCU_FP64_PIPE = {"stage_reinit_rk32": 44.9, "stage_normal_rk32": 47.8}
+
 def env_int(name, default):
     try:
         return int(os.environ.get(name, default))
@@ -240,13 +247,11 @@ def run_ours(args, world, rank, local, pg):
     share_no = 3 * kern["stage_normal_rk32"]["ms"]
     dom = "stage_reinit_rk32" if share_re >= share_no else "stage_normal_rk32"
     achieved = kern[dom]["bytes"] / (kern[dom]["ms"] / 1e3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            traffic = json.load(f).get(dom)
+    traffic = NCU_TRAFFIC.get(dom) if N_CELLS == 256 else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                "traffic_source": "ncu capture, profiles/k_stage_fp64_config2_256.md",
+                "fp64_pipe_active_pct_ncu": NCU_FP64_PIPE.get(dom),
                 "kernel": dom, "kernel_ms": round(kern[dom]["ms"], 4),
                 "algorithmic_bytes_per_launch": kern[dom]["bytes"],
                 "peak_source": peak_kind,
