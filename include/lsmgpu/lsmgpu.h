@@ -528,9 +528,9 @@ int lsmgpu_adjoint_phi_final(lsmgpu_adjoint *h, double *host);
  * cells; the ghost cells of phi are read as stored.  dt is a host or device
  * double; a host dt makes the call wait for the result.
  *
- * Scratch: one partial maximum per tile of 32x8x32 cells lives in a static
- * device array of 4096 + 1 doubles (32 KB) that every GPU loading the library
- * holds until exit; a fill box needing more than 4096 tiles is rejected with
+ * Scratch: one partial maximum per tile of 32x8x16 cells lives in a static
+ * device array of 8192 + 1 doubles (64 KB) that every GPU loading the library
+ * holds until exit; a fill box needing more than 8192 tiles is rejected with
  * LSMGPU_ERR_INVALID_BOX.  The first call on a device looks up that array's
  * device address, so make it before any stream capture.  Every call reuses
  * the same array: calls that overlap on the GPU (other streams, other host

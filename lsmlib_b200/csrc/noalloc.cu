@@ -25,9 +25,9 @@ using namespace lsmgpu;
 namespace {
 
 // Scratch capacity: partial maxima of up to kNoAllocMaxTiles tiles of
-// kStageTX x kStageTY x kStageTZ = 32 x 8 x 32 cells (4096 tiles cover
-// 33.5 M cells, e.g. a 256^3 fill box needs 2048) plus one slot for dt.
-constexpr int kNoAllocMaxTiles = 4096;
+// kStageTX x kStageTY x kStageTZ = 32 x 8 x 16 cells (8192 tiles cover
+// 33.5 M cells, e.g. a 256^3 fill box needs 4096) plus one slot for dt.
+constexpr int kNoAllocMaxTiles = 8192;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxTiles + 1];
 
 constexpr int kMaxDevices = 64;
@@ -104,7 +104,8 @@ extern "C" int lsmgpu_normal_rhs_dt_noalloc(double* rhs, double* dt,
   if (tiles > kNoAllocMaxTiles) {
     set_error(LSMGPU_ERR_INVALID_BOX,
               std::string(R) + ": fill box needs " + std::to_string(tiles) +
-                  " tiles of 32x8x32 cells; the static scratch holds " +
+                  " tiles of " + std::to_string(kStageTX) + "x" + std::to_string(kStageTY) +
+                  "x" + std::to_string(kStageTZ) + " cells; the static scratch holds " +
                   std::to_string(kNoAllocMaxTiles));
     return LSMGPU_ERR_INVALID_BOX;
   }

@@ -625,8 +625,13 @@ struct UseFaces {
       (KIND == kStageNormal || KIND == kStageReinit || KIND == kStageNormalRhs);
 };
 
+// blocks per SM the register allocation must allow (default: 16 warps)
+#ifndef LSMGPU_STAGE_MIN_BLOCKS
+#define LSMGPU_STAGE_MIN_BLOCKS (512 / (TX * TY))
+#endif
+
 template <typename T, int KIND, bool FAST, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX * TY, 2)
+__global__ void __launch_bounds__(TX * TY, LSMGPU_STAGE_MIN_BLOCKS)
 k_stage(StageParams<T> p) {
   __shared__ T tile[2][TY + 6][TX + 6];
   double hmax;

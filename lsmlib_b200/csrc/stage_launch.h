@@ -31,7 +31,14 @@ struct StageArgs {
 };
 
 // tile of the stage kernels: TX x TY cells per block, TZ planes per block
-constexpr int kStageTX = 32, kStageTY = 8, kStageTZ = 32;
+// (build-time settings; TX is one warp)
+#ifndef LSMGPU_STAGE_TY
+#define LSMGPU_STAGE_TY 8
+#endif
+#ifndef LSMGPU_STAGE_TZ
+#define LSMGPU_STAGE_TZ 16
+#endif
+constexpr int kStageTX = 32, kStageTY = LSMGPU_STAGE_TY, kStageTZ = LSMGPU_STAGE_TZ;
 
 inline int stage_blocks(const FillBox& fb) {
   const int gx = (fb.n(0) + kStageTX - 1) / kStageTX;

@@ -113,7 +113,7 @@ def test_rejects_fill_box_beyond_the_static_scratch():
     from lsmlib_b200.ext_abi import dbls, ints
     lib = gpu.load()
     small = gpu.DeviceArray((4, 4, 4))
-    fb = (0, 32 * 17 - 1, 0, 8 * 16 - 1, 0, 32 * 16 - 1)   # 4352 tiles > 4096
+    fb = (0, 32 * 17 - 1, 0, 8 * 16 - 1, 0, 32 * 16 - 1)   # 17*16*32 = 8704 tiles > 8192
     gb = (-3, fb[1] + 3, -3, fb[3] + 3, -3, fb[5] + 3)
     dt = ctypes.c_double(0.0)
     rc = lib.lsmgpu_normal_rhs_dt_noalloc(small.ptr, ctypes.byref(dt), small.ptr,
@@ -121,7 +121,7 @@ def test_rejects_fill_box_beyond_the_static_scratch():
                                           dbls((0.1, 0.1, 0.1)), 0.5)
     assert rc == 1
     msg = lib.lsmgpu_get_last_error_string().decode()
-    assert "4096" in msg and "tiles" in msg
+    assert "8192" in msg and "tiles" in msg
     lib.lsmgpu_get_last_error()
 
 
