@@ -293,6 +293,106 @@ void lsm3dhomogeneousneumannweno5_(LSMLIB_REAL *phi, LSMGPU_BOX6(gb),
                                    LSMGPU_BOX6(fb),
                                    const int *bdry_location_idx);
 
+/* ---- central differences, Laplacian, upwind grad F, gradient magnitude ---
+ * lsm_spatial_derivatives3d.h:673-956 (LSM3D_CENTRAL_GRAD_ORDER2/4,
+ * LSM3D_LAPLACIAN_ORDER2, LSM3D_PHI_UPWIND_GRAD_F, LSM3D_AVERAGE_GRAD_PHI,
+ * LSM3D_GRADIENT_MAGNITUDE).  phi needs 1 ghost cell (2 for ORDER4) around
+ * the fill box.  LSM3D_PHI_UPWIND_GRAD_F leaves F_x/y/z unchanged where
+ * phi == 0, as the reference does. */
+void lsm3dcentralgradorder2_(LSMLIB_REAL *phi_x, LSMLIB_REAL *phi_y,
+                             LSMLIB_REAL *phi_z, LSMGPU_BOX6(grad_phi_gb),
+                             const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb),
+                             LSMGPU_BOX6(fb), const LSMLIB_REAL *dx,
+                             const LSMLIB_REAL *dy, const LSMLIB_REAL *dz);
+void lsm3dcentralgradorder4_(LSMLIB_REAL *phi_x, LSMLIB_REAL *phi_y,
+                             LSMLIB_REAL *phi_z, LSMGPU_BOX6(grad_phi_gb),
+                             const LSMLIB_REAL *phi, LSMGPU_BOX6(phi_gb),
+                             LSMGPU_BOX6(fb), const LSMLIB_REAL *dx,
+                             const LSMLIB_REAL *dy, const LSMLIB_REAL *dz);
+void lsm3dlaplacianorder2_(LSMLIB_REAL *laplacian_phi,
+                           LSMGPU_BOX6(laplacian_phi_gb), const LSMLIB_REAL *phi,
+                           LSMGPU_BOX6(phi_gb), LSMGPU_BOX6(fb),
+                           const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+                           const LSMLIB_REAL *dz);
+void lsm3dphiupwindgradf_(LSMLIB_REAL *F_x, LSMLIB_REAL *F_y, LSMLIB_REAL *F_z,
+                          LSMGPU_BOX6(grad_F_gb), const LSMLIB_REAL *F_x_plus,
+                          const LSMLIB_REAL *F_y_plus, const LSMLIB_REAL *F_z_plus,
+                          LSMGPU_BOX6(grad_F_plus_gb),
+                          const LSMLIB_REAL *F_x_minus,
+                          const LSMLIB_REAL *F_y_minus,
+                          const LSMLIB_REAL *F_z_minus,
+                          LSMGPU_BOX6(grad_F_minus_gb), const LSMLIB_REAL *phi,
+                          LSMGPU_BOX6(phi_gb), LSMGPU_BOX6(fb));
+void lsm3daveragegradphi_(LSMLIB_REAL *phi_x, LSMLIB_REAL *phi_y,
+                          LSMLIB_REAL *phi_z, LSMGPU_BOX6(grad_phi_gb),
+                          const LSMLIB_REAL *phi_x_plus,
+                          const LSMLIB_REAL *phi_y_plus,
+                          const LSMLIB_REAL *phi_z_plus,
+                          LSMGPU_BOX6(grad_phi_plus_gb),
+                          const LSMLIB_REAL *phi_x_minus,
+                          const LSMLIB_REAL *phi_y_minus,
+                          const LSMLIB_REAL *phi_z_minus,
+                          LSMGPU_BOX6(grad_phi_minus_gb), LSMGPU_BOX6(fb));
+void lsm3dgradientmagnitude_(const LSMLIB_REAL *phi_x, const LSMLIB_REAL *phi_y,
+                             const LSMLIB_REAL *phi_z, LSMLIB_REAL *grad_phi_mag,
+                             LSMGPU_BOX6(grad_phi_gb), LSMGPU_BOX6(grad_phi_fb));
+
+/* ---- curvature and external + normal terms --------------------------------
+ * lsm_level_set_evolution3d.h:277, :334, :398.  The precomputed-curvature and
+ * external+normal terms run the reference's loop nest over k in
+ * [klo_fb, khi_rhs_gb], j in [jlo_fb, jhi_rhs_gb], i in [ilo_rhs_gb,
+ * ihi_rhs_gb] (lsm_level_set_evolution3d.f.in:505-507, :586-588); the input
+ * arrays must cover that region. */
+void lsm3daddconstcurvtermtolserhs_(
+    LSMLIB_REAL *lse_rhs, LSMGPU_BOX6(rhs_gb), const LSMLIB_REAL *phi_x,
+    const LSMLIB_REAL *phi_y, const LSMLIB_REAL *phi_z, LSMGPU_BOX6(grad_phi_gb),
+    const LSMLIB_REAL *phi_xx, const LSMLIB_REAL *phi_xy,
+    const LSMLIB_REAL *phi_xz, const LSMLIB_REAL *phi_yy,
+    const LSMLIB_REAL *phi_yz, const LSMLIB_REAL *phi_zz,
+    LSMGPU_BOX6(grad2_phi_gb), const LSMLIB_REAL *b, LSMGPU_BOX6(fb));
+void lsm3daddconstprecomputedcurvtermtolserhs_(
+    LSMLIB_REAL *lse_rhs, LSMGPU_BOX6(rhs_gb), const LSMLIB_REAL *kappa,
+    LSMGPU_BOX6(kappa_gb), const LSMLIB_REAL *grad_phi_mag,
+    LSMGPU_BOX6(grad_phi_gb), const LSMLIB_REAL *b, LSMGPU_BOX6(rhs_fb));
+void lsm3daddexternalandnormalveltermtolserhs_(
+    LSMLIB_REAL *lse_rhs, LSMGPU_BOX6(rhs_gb), const LSMLIB_REAL *phi_x_plus,
+    const LSMLIB_REAL *phi_y_plus, const LSMLIB_REAL *phi_z_plus,
+    LSMGPU_BOX6(grad_phi_plus_gb), const LSMLIB_REAL *phi_x_minus,
+    const LSMLIB_REAL *phi_y_minus, const LSMLIB_REAL *phi_z_minus,
+    LSMGPU_BOX6(grad_phi_minus_gb), const LSMLIB_REAL *vel_n,
+    const LSMLIB_REAL *vel_x, const LSMLIB_REAL *vel_y, const LSMLIB_REAL *vel_z,
+    LSMGPU_BOX6(vel_gb), LSMGPU_BOX6(rhs_fb));
+
+/* ---- orthogonalization and subcell fix ------------------------------------
+ * lsm_reinitialization3d.h:163, :247, :295 */
+void lsm3dcomputeorthogonalizationeqnrhs_(
+    LSMLIB_REAL *ortho_rhs, LSMGPU_BOX6(rhs_gb), const LSMLIB_REAL *phi_x_plus,
+    const LSMLIB_REAL *phi_y_plus, const LSMLIB_REAL *phi_z_plus,
+    LSMGPU_BOX6(grad_phi_plus_gb), const LSMLIB_REAL *phi_x_minus,
+    const LSMLIB_REAL *phi_y_minus, const LSMLIB_REAL *phi_z_minus,
+    LSMGPU_BOX6(grad_phi_minus_gb), const LSMLIB_REAL *psi, LSMGPU_BOX6(psi_gb),
+    const LSMLIB_REAL *psi_x_plus, const LSMLIB_REAL *psi_y_plus,
+    const LSMLIB_REAL *psi_z_plus, LSMGPU_BOX6(grad_psi_plus_gb),
+    const LSMLIB_REAL *psi_x_minus, const LSMLIB_REAL *psi_y_minus,
+    const LSMLIB_REAL *psi_z_minus, LSMGPU_BOX6(grad_psi_minus_gb),
+    LSMGPU_BOX6(fb), const LSMLIB_REAL *dx, const LSMLIB_REAL *dy,
+    const LSMLIB_REAL *dz);
+void lsm3dcomputedistanceforsubcellfix_(LSMLIB_REAL *distance0,
+                                        const LSMLIB_REAL *phi0,
+                                        LSMGPU_BOX6(phi0_gb), LSMGPU_BOX6(fb),
+                                        const LSMLIB_REAL *dx,
+                                        const LSMLIB_REAL *dy,
+                                        const LSMLIB_REAL *dz);
+void lsm3dcomputereinitializationeqnrhssubcellfixorder1_(
+    LSMLIB_REAL *reinit_rhs, LSMGPU_BOX6(rhs_gb), const LSMLIB_REAL *phi,
+    LSMGPU_BOX6(phi_gb), const LSMLIB_REAL *phi0, const LSMLIB_REAL *distance0,
+    LSMGPU_BOX6(phi0_gb), const LSMLIB_REAL *phi_x_plus,
+    const LSMLIB_REAL *phi_y_plus, const LSMLIB_REAL *phi_z_plus,
+    LSMGPU_BOX6(grad_phi_plus_gb), const LSMLIB_REAL *phi_x_minus,
+    const LSMLIB_REAL *phi_y_minus, const LSMLIB_REAL *phi_z_minus,
+    LSMGPU_BOX6(grad_phi_minus_gb), LSMGPU_BOX6(fb), const LSMLIB_REAL *dx,
+    const LSMLIB_REAL *dy, const LSMLIB_REAL *dz);
+
 /* ======================================================================== */
 /* Part 2 -- extension API                                                   */
 /* ======================================================================== */

@@ -82,6 +82,35 @@ SIGNATURES = {
     "lsm3dhomogeneousneumanneno2_": "X:phi G F N:bdry_location_idx",
     "lsm3dhomogeneousneumanneno3_": "X:phi G F N:bdry_location_idx",
     "lsm3dhomogeneousneumannweno5_": "X:phi G F N:bdry_location_idx",
+    # lsm_spatial_derivatives3d.h:673-956 (central, Laplacian, upwind grad F,
+    # averaged and magnitude of the gradient)
+    "lsm3dcentralgradorder2_": "O:phi_x O:phi_y O:phi_z G I:phi G F" + DXYZ,
+    "lsm3dcentralgradorder4_": "O:phi_x O:phi_y O:phi_z G I:phi G F" + DXYZ,
+    "lsm3dlaplacianorder2_": "O:laplacian_phi G I:phi G F" + DXYZ,
+    "lsm3dphiupwindgradf_": ("X:F_x X:F_y X:F_z G I:F_x_plus I:F_y_plus I:F_z_plus G "
+                             "I:F_x_minus I:F_y_minus I:F_z_minus G I:phi G F"),
+    "lsm3daveragegradphi_": ("O:phi_x O:phi_y O:phi_z G I:phi_x_plus I:phi_y_plus "
+                             "I:phi_z_plus G I:phi_x_minus I:phi_y_minus "
+                             "I:phi_z_minus G F"),
+    "lsm3dgradientmagnitude_": "I:phi_x I:phi_y I:phi_z O:grad_phi_mag G F",
+    # lsm_level_set_evolution3d.h:277-440 (curvature, external + normal)
+    "lsm3daddconstcurvtermtolserhs_": ("X:lse_rhs G I:phi_x I:phi_y I:phi_z G "
+                                       "I:phi_xx I:phi_xy I:phi_xz I:phi_yy I:phi_yz "
+                                       "I:phi_zz G R:b F"),
+    "lsm3daddconstprecomputedcurvtermtolserhs_": (
+        "X:lse_rhs G I:kappa G I:grad_phi_mag G R:b F"),
+    "lsm3daddexternalandnormalveltermtolserhs_": (
+        "X:lse_rhs G I:phi_x_plus I:phi_y_plus I:phi_z_plus G I:phi_x_minus "
+        "I:phi_y_minus I:phi_z_minus G I:vel_n I:vel_x I:vel_y I:vel_z G F"),
+    # lsm_reinitialization3d.h:163-340 (orthogonalization, subcell fix)
+    "lsm3dcomputeorthogonalizationeqnrhs_": (
+        "O:ortho_rhs G I:phi_x_plus I:phi_y_plus I:phi_z_plus G I:phi_x_minus "
+        "I:phi_y_minus I:phi_z_minus G I:psi G I:psi_x_plus I:psi_y_plus "
+        "I:psi_z_plus G I:psi_x_minus I:psi_y_minus I:psi_z_minus G F" + DXYZ),
+    "lsm3dcomputedistanceforsubcellfix_": "O:distance0 I:phi0 G F" + DXYZ,
+    "lsm3dcomputereinitializationeqnrhssubcellfixorder1_": (
+        "O:reinit_rhs G I:phi G I:phi0 I:distance0 G I:phi_x_plus I:phi_y_plus "
+        "I:phi_z_plus G I:phi_x_minus I:phi_y_minus I:phi_z_minus G F" + DXYZ),
 }
 
 

@@ -28,6 +28,7 @@ COMMON = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 # source -> extra flags
 SOURCES = {
     "toolbox_kernels.cu": ["--fmad=false"],
+    "toolbox_extra.cu": ["--fmad=false"],
     "capi.cu": ["--fmad=false"],
     "stage_strict.cu": ["--fmad=false"],
     "stage_fast.cu": ["--fmad=true"],

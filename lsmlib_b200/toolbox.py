@@ -98,6 +98,21 @@ _MACROS = {
     "lsm3dhomogeneousneumanneno2_": "LSM3D_HOMOGENEOUS_NEUMANN_ENO2",
     "lsm3dhomogeneousneumanneno3_": "LSM3D_HOMOGENEOUS_NEUMANN_ENO3",
     "lsm3dhomogeneousneumannweno5_": "LSM3D_HOMOGENEOUS_NEUMANN_WENO5",
+    "lsm3dcentralgradorder2_": "LSM3D_CENTRAL_GRAD_ORDER2",
+    "lsm3dcentralgradorder4_": "LSM3D_CENTRAL_GRAD_ORDER4",
+    "lsm3dlaplacianorder2_": "LSM3D_LAPLACIAN_ORDER2",
+    "lsm3dphiupwindgradf_": "LSM3D_PHI_UPWIND_GRAD_F",
+    "lsm3daveragegradphi_": "LSM3D_AVERAGE_GRAD_PHI",
+    "lsm3dgradientmagnitude_": "LSM3D_GRADIENT_MAGNITUDE",
+    "lsm3daddconstcurvtermtolserhs_": "LSM3D_ADD_CONST_CURV_TERM_TO_LSE_RHS",
+    "lsm3daddconstprecomputedcurvtermtolserhs_":
+        "LSM3D_ADD_CONST_PRECOMPUTED_CURV_TERM_TO_LSE_RHS",
+    "lsm3daddexternalandnormalveltermtolserhs_":
+        "LSM3D_ADD_EXTERNAL_AND_NORMAL_VEL_TERM_TO_LSE_RHS",
+    "lsm3dcomputeorthogonalizationeqnrhs_": "LSM3D_COMPUTE_ORTHOGONALIZATION_EQN_RHS",
+    "lsm3dcomputedistanceforsubcellfix_": "LSM3D_COMPUTE_DISTANCE_FOR_SUBCELL_FIX",
+    "lsm3dcomputereinitializationeqnrhssubcellfixorder1_":
+        "LSM3D_COMPUTE_REINITIALIZATION_EQN_RHS_SUBCELL_FIX_ORDER1",
 }
 
 

@@ -22,8 +22,10 @@ The translation keeps what decides the floating-point result bit for bit:
 * DO loop bounds are evaluated once before the loop, as Fortran requires.
 
 Only the statement forms used by the translated routines are supported
-(declarations, PARAMETER, DO/ENDDO, block IF/ELSEIF/ELSE/ENDIF, CALL, RETURN,
-assignment); anything else raises an error instead of being guessed.
+(declarations incl. LOGICAL, PARAMETER, DO/ENDDO, block IF/ELSEIF/ELSE/ENDIF,
+CALL, RETURN, assignment; .EQV./.NEQV. and SIGN(a,b) as gfortran evaluates
+them: |a| with the sign bit of b); anything else raises an error instead of
+being guessed.
 
 Usage: f77toc.py OUT.c SRC.f[.in]... -- reads the sources where they lie and
 writes one C file whose functions are named ref_<lower-case fortran name>_.
@@ -88,7 +90,7 @@ def logical_lines(text, path):
 # ----------------------------------------------------------------------------
 TOK = re.compile(r"""
   (?P<num>(\d+\.\d*|\.\d+|\d+)([ed][+-]?\d+)?)
- |(?P<dotop>\.(lt|le|gt|ge|eq|ne|and|or|not|true|false)\.)
+ |(?P<dotop>\.(lt|le|gt|ge|eq|ne|and|or|not|true|false|eqv|neqv)\.)
  |(?P<id>[a-z_][a-z0-9_]*)
  |(?P<pow>\*\*)
  |(?P<op>[-+*/(),=:])
@@ -129,9 +131,14 @@ class P:
         self.i += 1
         return tok
 
-    # Fortran precedence: .or. < .and. < .not. < relational < +,- < *,/ < **
+    # Fortran precedence: .eqv./.neqv. < .or. < .and. < .not. < relational
+    # < +,- < *,/ < **
     def expr(self):
-        return self.orx()
+        a = self.orx()
+        while self.peek()[1] in (".eqv.", ".neqv."):
+            op = self.take()[1]
+            a = ("eqv" if op == ".eqv." else "neqv", a, self.orx())
+        return a
 
     def orx(self):
         a = self.andx()
@@ -214,6 +221,8 @@ class P:
         if val == "(":
             self.take(); a = self.expr(); self.take(")")
             return ("paren", a)
+        if val in (".true.", ".false."):
+            self.take(); return ("bool", val == ".true.")
         raise SyntaxError("unexpected token %r" % (val,))
 
 
@@ -272,7 +281,7 @@ class Sub:
             return "real" if "real" in (a, b) else "int"
         if k == "pow":
             return self.etype(e[1])
-        if k in ("rel", "and", "or", "not"):
+        if k in ("rel", "and", "or", "not", "eqv", "neqv", "bool"):
             return "logical"
         if k == "ref":
             f = e[1]
@@ -324,6 +333,11 @@ class Sub:
             return "(%s || %s)" % (self.cx(e[1]), self.cx(e[2]))
         if k == "not":
             return "(!%s)" % self.cx(e[1])
+        if k == "bool":
+            return "1" if e[1] else "0"
+        if k in ("eqv", "neqv"):
+            return "((!!%s) %s (!!%s))" % (self.cx(e[1]), "==" if k == "eqv" else "!=",
+                                           self.cx(e[2]))
         if k == "ref":
             f, args = e[1], e[2]
             if f in self.dims:
@@ -340,6 +354,9 @@ class Sub:
                 return acc
             if f == "sqrt":
                 return "sqrt(%s)" % self.cx(args[0])
+            if f == "sign" and "real" in [self.etype(a) for a in args]:
+                # |a| with the sign of b (gfortran: the sign bit of b)
+                return "copysign(fabs(%s), %s)" % (self.cx(args[0]), self.cx(args[1]))
             if f == "mod":
                 return "(%s %% %s)" % (self.cx(args[0]), self.cx(args[1]))
             if f in ("dble", "real", "float"):
@@ -401,9 +418,9 @@ def parse_units(lines, path):
             continue
         if s == "implicit none":
             continue
-        m = re.match(r"(integer|real|double precision)\s+(.*)$", s)
-        if m and not re.match(r"(integer|real)\s*=", s):
-            t = "int" if m.group(1) == "integer" else "real"
+        m = re.match(r"(integer|real|double precision|logical)\s+(.*)$", s)
+        if m and not re.match(r"(integer|real|logical)\s*=", s):
+            t = {"integer": "int", "logical": "int"}.get(m.group(1), "real")
             for item in split_top(m.group(2)):
                 mm = re.match(r"([a-z0-9_]+)\s*(\((.*)\))?$", item)
                 if not mm:

@@ -820,3 +820,348 @@ double orc_lsm_heaviside(double x, double eps) {
   if (x > eps) return 1.0;
   return 0.5 * (1 + x / eps + 1 / M_PI * sin(M_PI * x / eps));
 }
+
+/* ------------------------------------------------------------------------ */
+/* Central differences, Laplacian, upwind selection, gradient magnitude      */
+/* lsm_spatial_derivatives3d.f.in:3016-3660                                  */
+/* ------------------------------------------------------------------------ */
+/* lsm3dCentralGradOrder2 :3016-3085 (factor 0.5/dx :3060, update :3068-3070) */
+void orc_lsm3dcentralgradorder2_(real *px, real *py, real *pz, GB6(g),
+    const real *phi, GB6(phi), FB6, const real *dx, const real *dy, const real *dz) {
+  box_t gg = MK(g), gp = MK(phi);
+  const real fx = 0.5 / *dx, fy = 0.5 / *dy, fz = 0.5 / *dz;
+  long i, j, k;
+  for (k = *klo_fb; k <= *khi_fb; k++)
+    for (j = *jlo_fb; j <= *jhi_fb; j++)
+      for (i = *ilo_fb; i <= *ihi_fb; i++) {
+        long o = IX(&gg, i, j, k);
+        px[o] = (phi[IX(&gp, i + 1, j, k)] - phi[IX(&gp, i - 1, j, k)]) * fx;
+        py[o] = (phi[IX(&gp, i, j + 1, k)] - phi[IX(&gp, i, j - 1, k)]) * fy;
+        pz[o] = (phi[IX(&gp, i, j, k + 1)] - phi[IX(&gp, i, j, k - 1)]) * fz;
+      }
+}
+
+/* lsm3dCentralGradOrder4 :3094-3171 (factor :3140-3142, update :3150-3158):
+   (-phi(+2) + 8 phi(+1) + phi(-2) - 8 phi(-1)) * (1/12)/dx, left to right */
+static inline real cgrad4(const real *q, long s, real f) {
+  return (-q[2 * s] + 8.0 * q[s] + q[-2 * s] - 8.0 * q[-s]) * f;
+}
+void orc_lsm3dcentralgradorder4_(real *px, real *py, real *pz, GB6(g),
+    const real *phi, GB6(phi), FB6, const real *dx, const real *dy, const real *dz) {
+  box_t gg = MK(g), gp = MK(phi);
+  const real c = 0.0833333333333333333333;
+  const real fx = c / *dx, fy = c / *dy, fz = c / *dz;
+  long i, j, k;
+  for (k = *klo_fb; k <= *khi_fb; k++)
+    for (j = *jlo_fb; j <= *jhi_fb; j++)
+      for (i = *ilo_fb; i <= *ihi_fb; i++) {
+        long o = IX(&gg, i, j, k);
+        const real *q = phi + IX(&gp, i, j, k);
+        px[o] = cgrad4(q, 1, fx);
+        py[o] = cgrad4(q, stride_of(&gp, 1), fy);
+        pz[o] = cgrad4(q, stride_of(&gp, 2), fz);
+      }
+}
+
+/* lsm3dLaplacianOrder2 :3180-3261 (1/dx/dx :3236-3238, sum :3244-3250) */
+void orc_lsm3dlaplacianorder2_(real *lap, GB6(l), const real *phi, GB6(phi), FB6,
+    const real *dx, const real *dy, const real *dz) {
+  box_t gl = MK(l), gp = MK(phi);
+  const real ix = 1.0 / *dx / *dx, iy = 1.0 / *dy / *dy, iz = 1.0 / *dz / *dz;
+  const long sy = stride_of(&gp, 1), sz = stride_of(&gp, 2);
+  long i, j, k;
+  for (k = *klo_fb; k <= *khi_fb; k++)
+    for (j = *jlo_fb; j <= *jhi_fb; j++)
+      for (i = *ilo_fb; i <= *ihi_fb; i++) {
+        const real *q = phi + IX(&gp, i, j, k);
+        lap[IX(&gl, i, j, k)] = ix * (q[1] - 2.0 * q[0] + q[-1])
+                              + iy * (q[sy] - 2.0 * q[0] + q[-sy])
+                              + iz * (q[sz] - 2.0 * q[0] + q[-sz]);
+      }
+}
+
+/* lsm3dPhiUpwindGradF :3270-3477: per axis, the one-sided derivative of F on
+   the side of the neighbour closer to the interface (phi > 0: the smaller
+   neighbour not above phi; phi < 0: the larger not below), 0 if neither; the
+   cell is left unchanged where phi == 0 */
+static inline real upwind_gradf_pos(real pc, real pm, real pp, real fp, real fm) {
+  if (pm <= pc) return (pp < pm) ? fp : fm;
+  if (pp <= pc) return fp;
+  return 0.0;
+}
+static inline real upwind_gradf_neg(real pc, real pm, real pp, real fp, real fm) {
+  if (pm >= pc) return (pp > pm) ? fp : fm;
+  if (pp >= pc) return fp;
+  return 0.0;
+}
+void orc_lsm3dphiupwindgradf_(real *Fx, real *Fy, real *Fz, GB6(g),
+    const real *Fxp, const real *Fyp, const real *Fzp, GB6(gp),
+    const real *Fxm, const real *Fym, const real *Fzm, GB6(gm),
+    const real *phi, GB6(phi), FB6) {
+  box_t gg = MK(g), gpl = MK(gp), gmi = MK(gm), gph = MK(phi);
+  real *F[3] = {Fx, Fy, Fz};
+  const real *P[3] = {Fxp, Fyp, Fzp}, *M[3] = {Fxm, Fym, Fzm};
+  long i, j, k;
+  int d;
+  for (k = *klo_fb; k <= *khi_fb; k++)
+    for (j = *jlo_fb; j <= *jhi_fb; j++)
+      for (i = *ilo_fb; i <= *ihi_fb; i++) {
+        const real *q = phi + IX(&gph, i, j, k);
+        real pc = q[0];
+        long o = IX(&gg, i, j, k), op = IX(&gpl, i, j, k), om = IX(&gmi, i, j, k);
+        for (d = 0; d < 3; d++) {
+          long s = stride_of(&gph, d);
+          if (pc > 0)
+            F[d][o] = upwind_gradf_pos(pc, q[-s], q[s], P[d][op], M[d][om]);
+          else if (pc < 0)
+            F[d][o] = upwind_gradf_neg(pc, q[-s], q[s], P[d][op], M[d][om]);
+        }
+      }
+}
+
+/* lsm3dAverageGradPhi :3486-3577 (:3561-3566) */
+void orc_lsm3daveragegradphi_(real *px, real *py, real *pz, GB6(g),
+    const real *pxp, const real *pyp, const real *pzp, GB6(gp),
+    const real *pxm, const real *pym, const real *pzm, GB6(gm), FB6) {
+  box_t gg = MK(g), gpl = MK(gp), gmi = MK(gm);
+  long i, j, k;
+  for (k = *klo_fb; k <= *khi_fb; k++)
+    for (j = *jlo_fb; j <= *jhi_fb; j++)
+      for (i = *ilo_fb; i <= *ihi_fb; i++) {
+        long o = IX(&gg, i, j, k), op = IX(&gpl, i, j, k), om = IX(&gmi, i, j, k);
+        px[o] = 0.5 * (pxp[op] + pxm[om]);
+        py[o] = 0.5 * (pyp[op] + pym[om]);
+        pz[o] = 0.5 * (pzp[op] + pzm[om]);
+      }
+}
+
+/* lsm3dGradientMagnitude :3586-3660: squares below 1e-8 dropped, magnitude
+   below 1e-8 set to 0 (:3626-3651) */
+void orc_lsm3dgradientmagnitude_(const real *px, const real *py, const real *pz,
+    real *mag, GB6(g), GB6(fb)) {
+  box_t gg = MK(g);
+  const real tol = 1.0e-8;
+  long i, j, k;
+  for (k = *klo_fb; k <= *khi_fb; k++)
+    for (j = *jlo_fb; j <= *jhi_fb; j++)
+      for (i = *ilo_fb; i <= *ihi_fb; i++) {
+        long o = IX(&gg, i, j, k);
+        real sx = px[o] * px[o], sy = py[o] * py[o], sz = pz[o] * pz[o];
+        if (sx < tol) sx = 0.0;
+        if (sy < tol) sy = 0.0;
+        if (sz < tol) sz = 0.0;
+        real t = sqrt(sx + sy + sz);
+        mag[o] = (t < tol) ? 0.0 : t;
+      }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Curvature and external + normal terms  lsm_level_set_evolution3d.f.in     */
+/* ------------------------------------------------------------------------ */
+/* lsm3dAddConstCurvTermToLSERHS :356-456: rhs += b * kappa |grad phi| with
+   the mean-curvature numerator over |grad phi|^2 (:431-448) */
+void orc_lsm3daddconstcurvtermtolserhs_(real *rhs, GB6(r),
+    const real *px, const real *py, const real *pz, GB6(g1),
+    const real *pxx, const real *pxy, const real *pxz, const real *pyy,
+    const real *pyz, const real *pzz, GB6(g2), const real *b, FB6) {
+  box_t gr = MK(r), ga = MK(g1), gb2 = MK(g2);
+  long i, j, k;
+  for (k = *klo_fb; k <= *khi_fb; k++)
+    for (j = *jlo_fb; j <= *jhi_fb; j++)
+      for (i = *ilo_fb; i <= *ihi_fb; i++) {
+        long o1 = IX(&ga, i, j, k), o2 = IX(&gb2, i, j, k);
+        real x = px[o1], y = py[o1], z = pz[o1];
+        real g2 = x * x + y * y + z * z, curv;
+        if (g2 < ZERO_TOL) {
+          curv = 0.0;
+        } else {
+          curv = pxx[o2] * y * y + pyy[o2] * x * x - 2.0 * pxy[o2] * x * y
+               + pxx[o2] * z * z + pzz[o2] * x * x - 2.0 * pxz[o2] * x * z
+               + pyy[o2] * z * z + pzz[o2] * y * y - 2.0 * pyz[o2] * y * z;
+          curv = curv / g2;
+        }
+        long o = IX(&gr, i, j, k);
+        rhs[o] = rhs[o] + *b * curv;
+      }
+}
+
+/* The loop nest of the two routines below runs k over [klo_fb, khi_gb],
+   j over [jlo_fb, jhi_gb] and i over [ilo_gb, ihi_gb] of the RHS array, as
+   written in the reference (:505-507, :586-588). */
+
+/* lsm3dAddConstPrecomputedCurvTermToLSERHS :465-523 (:509-510) */
+void orc_lsm3daddconstprecomputedcurvtermtolserhs_(real *rhs, GB6(r),
+    const real *kappa, GB6(kap), const real *gmag, GB6(g), const real *b, GB6(fb)) {
+  box_t gr = MK(r), gk = MK(kap), gg = MK(g);
+  long i, j, k;
+  for (k = *klo_fb; k <= *khi_r; k++)
+    for (j = *jlo_fb; j <= *jhi_r; j++)
+      for (i = *ilo_r; i <= *ihi_r; i++) {
+        long o = IX(&gr, i, j, k);
+        rhs[o] = rhs[o] + *b * kappa[IX(&gk, i, j, k)] * gmag[IX(&gg, i, j, k)];
+      }
+}
+
+/* lsm3dAddExternalAndNormalVelTermToLSERHS :532-710: per axis the Godunov
+   choice for H = V.grad phi + Vn |grad phi| (:593-667), then
+   rhs -= V.grad phi (+ Vn |grad phi| when |Vn| and |grad phi|^2 pass the
+   zero tolerance, :672-684) */
+static inline real ext_normal_pick(real v, real vn, real dp, real dm) {
+  real hp = v + vn * dp, hm = v + vn * dm;
+  if (hp > 0.0) {
+    if (hm > 0.0) return dm;
+    return -(v / vn);
+  }
+  if (hm < 0.0) return dp;
+  return (fabs(hp) > fabs(hm)) ? dp : dm;
+}
+void orc_lsm3daddexternalandnormalveltermtolserhs_(real *rhs, GB6(r),
+    const real *pxp, const real *pyp, const real *pzp, GB6(gp),
+    const real *pxm, const real *pym, const real *pzm, GB6(gm),
+    const real *vn, const real *vx, const real *vy, const real *vz, GB6(v), GB6(fb)) {
+  box_t gr = MK(r), gpl = MK(gp), gmi = MK(gm), gv = MK(v);
+  long i, j, k;
+  for (k = *klo_fb; k <= *khi_r; k++)
+    for (j = *jlo_fb; j <= *jhi_r; j++)
+      for (i = *ilo_r; i <= *ihi_r; i++) {
+        long o = IX(&gr, i, j, k), op = IX(&gpl, i, j, k), om = IX(&gmi, i, j, k),
+             ov = IX(&gv, i, j, k);
+        real n = vn[ov], x = vx[ov], y = vy[ov], z = vz[ov];
+        real gx = ext_normal_pick(x, n, pxp[op], pxm[om]);
+        real gy = ext_normal_pick(y, n, pyp[op], pym[om]);
+        real gz = ext_normal_pick(z, n, pzp[op], pzm[om]);
+        real nsq = gx * gx + gy * gy + gz * gz;
+        if (fabs(n) >= ZERO_TOL && nsq >= ZERO_TOL)
+          rhs[o] = rhs[o] - x * gx - y * gy - z * gz - n * sqrt(nsq);
+        else
+          rhs[o] = rhs[o] - x * gx - y * gy - z * gz;
+      }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Orthogonalization and subcell fix  lsm_reinitialization3d.f.in            */
+/* ------------------------------------------------------------------------ */
+/* lsm3dComputeOrthogonalizationEqnRHS :296-468: upwinding of grad phi along
+   the smoothed sign of psi times the averaged grad psi (:416-457) */
+void orc_lsm3dcomputeorthogonalizationeqnrhs_(real *rhs, GB6(r),
+    const real *pxp, const real *pyp, const real *pzp, GB6(gp),
+    const real *pxm, const real *pym, const real *pzm, GB6(gm),
+    const real *psi, GB6(psi),
+    const real *sxp, const real *syp, const real *szp, GB6(sp),
+    const real *sxm, const real *sym, const real *szm, GB6(sm), FB6,
+    const real *dx, const real *dy, const real *dz) {
+  box_t gr = MK(r), gpl = MK(gp), gmi = MK(gm), gps = MK(psi), gsp = MK(sp),
+        gsm = MK(sm);
+  real dx_sq = fmax2(fmax2(*dx, *dy), *dz);
+  long i, j, k;
+  dx_sq = dx_sq * dx_sq;
+  for (k = *klo_fb; k <= *khi_fb; k++)
+    for (j = *jlo_fb; j <= *jhi_fb; j++)
+      for (i = *ilo_fb; i <= *ihi_fb; i++) {
+        long osp = IX(&gsp, i, j, k), osm = IX(&gsm, i, j, k);
+        long op = IX(&gpl, i, j, k), om = IX(&gmi, i, j, k), o = IX(&gr, i, j, k);
+        real g1 = 0.5 * (sxp[osp] + sxm[osm]);
+        real g2 = 0.5 * (syp[osp] + sym[osm]);
+        real g3 = 0.5 * (szp[osp] + szm[osm]);
+        real nrm = g1 * g1 + g2 * g2 + g3 * g3;
+        real ps = psi[IX(&gps, i, j, k)];
+        nrm = sqrt(nrm);
+        if (fabs(ps) > ZERO_TOL && nrm > ZERO_TOL) {
+          real sgn = ps / sqrt(ps * ps + dx_sq * (nrm * nrm));
+          rhs[o] = -(1.0 / nrm * (fmax2(sgn * g1, 0.0) * pxm[om]
+                                + fmin2(sgn * g1, 0.0) * pxp[op]
+                                + fmax2(sgn * g2, 0.0) * pym[om]
+                                + fmin2(sgn * g2, 0.0) * pyp[op]
+                                + fmax2(sgn * g3, 0.0) * pzm[om]
+                                + fmin2(sgn * g3, 0.0) * pzp[op]));
+        } else {
+          rhs[o] = 0.0;
+        }
+      }
+}
+
+/* lsm3dComputeDistanceForSubcellFix :477-577: cells with a sign change to a
+   face neighbour get phi0 / max(one-sided and central |differences|,
+   zero_tol) (:544-571), the others -1000 max(dx) (:541) */
+static inline int sign_change(real a, real c) {
+  return (a > 0.0 && c <= 0.0) || (a <= 0.0 && c > 0.0);
+}
+void orc_lsm3dcomputedistanceforsubcellfix_(real *dist, const real *phi0, GB6(p),
+    FB6, const real *dx, const real *dy, const real *dz) {
+  box_t gp = MK(p);
+  const real max_dx = fmax2(fmax2(*dx, *dy), *dz);
+  const real flag = -1000.0 * max_dx;
+  long i, j, k;
+  int d;
+  for (k = *klo_fb; k <= *khi_fb; k++)
+    for (j = *jlo_fb; j <= *jhi_fb; j++)
+      for (i = *ilo_fb; i <= *ihi_fb; i++) {
+        long o = IX(&gp, i, j, k);
+        const real *q = phi0 + o;
+        real c = q[0];
+        int near = 0;
+        for (d = 0; d < 3; d++) {
+          long s = stride_of(&gp, d);
+          near = near || sign_change(q[s], c) || sign_change(q[-s], c);
+        }
+        if (!near) {
+          dist[o] = flag;
+        } else {
+          real delta = ZERO_TOL;
+          for (d = 0; d < 3; d++) {
+            long s = stride_of(&gp, d);
+            real d1 = fabs(q[s] - q[-s]) / 2.0;
+            real d2 = fabs(q[s] - c);
+            real d3 = fabs(c - q[-s]);
+            delta = fmax2(fmax2(fmax2(d1, d2), d3), delta);
+          }
+          dist[o] = c / delta;
+        }
+      }
+}
+
+/* lsm3dComputeReinitializationEqnRHSSubcellFixOrder1 :586-754: away from the
+   interface the Godunov RHS with the sign of phi0 (:680-721); next to it
+   distance0 - sgn(phi0)|phi|/max(dx) (:723-726) */
+void orc_lsm3dcomputereinitializationeqnrhssubcellfixorder1_(real *rhs, GB6(r),
+    const real *phi, GB6(phi), const real *phi0, const real *dist, GB6(p0),
+    const real *pxp, const real *pyp, const real *pzp, GB6(gp),
+    const real *pxm, const real *pym, const real *pzm, GB6(gm), FB6,
+    const real *dx, const real *dy, const real *dz) {
+  box_t gr = MK(r), gph = MK(phi), g0 = MK(p0), gpl = MK(gp), gmi = MK(gm);
+  const real max_dx = fmax2(fmax2(*dx, *dy), *dz);
+  const real flag = -1000.0 * max_dx;
+  long i, j, k;
+  int d;
+  for (k = *klo_fb; k <= *khi_fb; k++)
+    for (j = *jlo_fb; j <= *jhi_fb; j++)
+      for (i = *ilo_fb; i <= *ihi_fb; i++) {
+        long o = IX(&gr, i, j, k), o0 = IX(&g0, i, j, k);
+        real p0 = phi0[o0];
+        real sgn0 = fabs(p0) > ZERO_TOL ? copysign(1.0, p0) : 0.0;
+        real pc = phi[IX(&gph, i, j, k)];
+        if (dist[o0] == flag) {
+          long op = IX(&gpl, i, j, k), om = IX(&gmi, i, j, k);
+          real gp3[3] = {pxp[op], pyp[op], pzp[op]}, gm3[3] = {pxm[om], pym[om], pzm[om]};
+          real gs[3];
+          for (d = 0; d < 3; d++) {
+            if (pc > 0.0) {
+              gp3[d] = fmax2(-gp3[d], 0.0);
+              gm3[d] = fmax2(gm3[d], 0.0);
+            } else {
+              gp3[d] = fmax2(gp3[d], 0.0);
+              gm3[d] = fmax2(-gm3[d], 0.0);
+            }
+            gs[d] = fmax2(gp3[d], gm3[d]);
+          }
+          if (fabs(pc) > ZERO_TOL) {
+            real nsq = gs[0] * gs[0] + gs[1] * gs[1] + gs[2] * gs[2];
+            rhs[o] = sgn0 - sgn0 * sqrt(nsq);
+          } else {
+            rhs[o] = 0.0;
+          }
+        } else {
+          rhs[o] = dist[o0] - sgn0 * fabs(pc) / max_dx;
+        }
+      }
+}

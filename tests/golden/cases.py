@@ -67,6 +67,11 @@ def make_inputs(sym, case, seed):
                 data = level_set() + (rng.standard_normal(shape) * 1e-3)
             elif name.startswith("vel") or name.startswith("signed_normal"):
                 data = velocity()
+            elif name == "distance0":
+                # the subcell-fix flag -1000 max(dx) in about half the cells
+                data = np.where(rng.random(shape) < 0.5, -1000.0 * 0.17, generic())
+            elif name == "psi":
+                data = level_set()[::-1, :, :] + 0.1
             else:
                 data = generic()
             # float32-representable inputs keep the fixture small; the
@@ -75,12 +80,21 @@ def make_inputs(sym, case, seed):
             fields[name] = Field(np.asfortranarray(data), glo)
         elif kind == "R":
             scalars[name] = {"dx": 0.13, "dy": 0.11, "dz": 0.17, "dt": 0.021,
-                             "cfl_number": 0.5}.get(name)
+                             "cfl_number": 0.5, "b": 0.37}.get(name)
             if name == "vel_n":
                 scalars[name] = 0.7 if case == "smooth" else -1.25
         elif kind == "N":
             scalars[name] = 0
     return fields, scalars, fb
+
+
+# routines that write beyond the fill box: the zeroing of the whole ghost box,
+# and the two RHS terms whose loops run k over [klo_fb, khi_gb], j over
+# [jlo_fb, jhi_gb] and i over [ilo_gb, ihi_gb] of the RHS array
+# (lsm_level_set_evolution3d.f.in:505-507, :586-588)
+WHOLE_ARRAY_OUTPUT = ("lsm3dzerooutlevelseteqnrhs_",
+                      "lsm3daddconstprecomputedcurvtermtolserhs_",
+                      "lsm3daddexternalandnormalveltermtolserhs_")
 
 
 def run(tb, sym, fields, scalars, fb):
@@ -101,7 +115,7 @@ def run(tb, sym, fields, scalars, fb):
     for kind, name in abi.parse(abi.SIGNATURES[sym]):
         if kind in ("O", "X"):
             lo, hi = (fb[0], fb[2], fb[4]), (fb[1], fb[3], fb[5])
-            if sym == "lsm3dzerooutlevelseteqnrhs_":
+            if sym in WHOLE_ARRAY_OUTPUT:
                 out[name] = fs[name].data.copy()
             else:
                 out[name] = fs[name].view(lo, hi).copy()

@@ -8,7 +8,7 @@ would call the Fortran symbol, and compared bit for bit with
 import numpy as np
 import pytest
 
-from cases import run
+from cases import WHOLE_ARRAY_OUTPUT, run
 from golden_util import assert_bitwise, load_cases
 from lsmlib_b200 import abi
 from lsmlib_b200.toolbox import Field
@@ -40,7 +40,7 @@ def run_on_device(tb, sym, fields, scalars, fb):
     for kind, name in abi.parse(abi.SIGNATURES[sym]):
         if kind in ("O", "X"):
             h = gpu.host_field(dev[name])
-            if sym == "lsm3dzerooutlevelseteqnrhs_":
+            if sym in WHOLE_ARRAY_OUTPUT:
                 out[name] = h.data
             else:
                 out[name] = h.view((fb[0], fb[2], fb[4]), (fb[1], fb[3], fb[5])).copy()
@@ -65,10 +65,13 @@ def random_case(sym, n, seed, lo=(0, 0, 0), ghost=3):
     x = np.meshgrid(*[np.linspace(-1, 1, s) for s in shape], indexing="ij")
     sdf = np.sqrt((x[0] - 0.1) ** 2 + (x[1] + 0.05) ** 2 + x[2] ** 2) - 0.5
     fields, scalars = {}, {}
+    flag = -1000.0 * max(2.0 / n[0], 2.0 / n[1], 2.0 / n[2])   # subcell-fix flag
     for kind, name in abi.parse(abi.SIGNATURES[sym]):
         if kind in "IOX":
             if name.startswith("vel") or name.startswith("signed_normal"):
                 d = rng.standard_normal(shape)
+            elif name == "distance0":
+                d = np.where(rng.random(shape) < 0.5, flag, rng.standard_normal(shape))
             elif name.startswith("phi_") or name.startswith("S_"):
                 d = rng.standard_normal(shape)
             else:
@@ -76,7 +79,8 @@ def random_case(sym, n, seed, lo=(0, 0, 0), ghost=3):
             fields[name] = Field(np.asfortranarray(d), glo)
         elif kind == "R":
             scalars[name] = {"dx": 2.0 / n[0], "dy": 2.0 / n[1], "dz": 2.0 / n[2],
-                             "dt": 0.01, "cfl_number": 0.5, "vel_n": 0.8}[name]
+                             "dt": 0.01, "cfl_number": 0.5, "vel_n": 0.8,
+                             "b": 0.37}[name]
         elif kind == "N":
             scalars[name] = 0
     return fields, scalars, fb
