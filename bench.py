@@ -301,6 +301,10 @@ def run_ours(args, world, rank, local, pg):
     if not args.no_adjoint:
         adjoint_res = run_adjoint()
 
+    toolbox_res = None
+    if not args.no_toolbox:
+        toolbox_res = run_toolbox(peak)
+
     deformation_res = None
     if not args.no_deformation:
         deformation_res = run_config3(lib, pg, world,
@@ -322,7 +326,7 @@ def run_ours(args, world, rank, local, pg):
                    "l2": "inputs larger than L2 (144 MB per field, 6 fields live)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "fp32": fp32, "batched": batched_res, "adjoint": adjoint_res,
-        "deformation": deformation_res,
+        "deformation": deformation_res, "toolbox": toolbox_res,
         "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk,
     }
@@ -396,6 +400,82 @@ def run_adjoint(n_fd=20, h=1e-6):
                          "max_err_over_max_grad": worst_abs,
                          "max_rel_err_components_above_1pct": worst_sig,
                          "loss_difference": "cell by cell from the two final states"}}
+
+
+# drop-in routines timed one by one on the 256^3 grid with device arrays
+TOOLBOX_TIMED = [
+    "lsm3dhjweno5_", "lsm3dupwindhjweno5_", "lsm3dhjeno3_", "lsm3daddnormalveltermtolserhs_",
+    "lsm3dcomputereinitializationeqnrhs_", "lsm3dtvdrk3stage3_",
+    "lsm3dcomputestablenormalveldt_", "lsm3dcentralgradorder2_", "lsm3dcentralgradorder4_",
+    "lsm3dlaplacianorder2_", "lsm3dphiupwindgradf_", "lsm3daveragegradphi_",
+    "lsm3dgradientmagnitude_", "lsm3daddconstcurvtermtolserhs_",
+    "lsm3daddconstprecomputedcurvtermtolserhs_", "lsm3daddexternalandnormalveltermtolserhs_",
+    "lsm3dcomputeorthogonalizationeqnrhs_", "lsm3dcomputedistanceforsubcellfix_",
+    "lsm3dcomputereinitializationeqnrhssubcellfixorder1_"]
+
+
+def run_toolbox(peak, n=256, reps=10):
+    """Each routine of TOOLBOX_TIMED through the C ABI on device arrays over
+    the n^3 fill box (FP64, reference expression order): mean device time of
+    `reps` calls and the algorithmic bytes over the fill box (each input
+    array read once, each output written once, in/out arrays both)."""
+    from lsmlib_b200 import abi, gpu, workloads
+    from lsmlib_b200.toolbox import Field
+    tb = gpu.toolbox()
+    cfg = workloads.config2(n)
+    gb, fb = workloads.boxes(cfg["n"])
+    lo = (gb[0], gb[2], gb[4])
+    shape = cfg["phi"].shape
+    rng = np.random.default_rng(7)
+    # every array of a call is its own 144 MB buffer (larger than L2), so no
+    # input is served from L2 on behalf of another
+    noise = np.asfortranarray(rng.standard_normal(shape))
+    ins = [gpu.DeviceArray.from_host(noise) for _ in range(14)]   # [-1]: scratch
+    level_set = gpu.DeviceArray.from_host(cfg["phi"])
+    pool = [gpu.DeviceArray.from_host(noise) for _ in range(6)]
+    # subcell fix: every cell away from the interface (the far-field flag
+    # -1000 max dx), so the Godunov branch reads all gradient arrays
+    far = gpu.DeviceArray.from_host(np.full(shape, -1000.0 * max(cfg["dx"]), order="F"))
+    cells = n ** 3
+    timer = gpu.Timer()
+    res = {}
+    for sym in TOOLBOX_TIMED:
+        fields, scal, nbytes, k_out, k_in = {}, {}, 0, 0, 0
+        for kind, name in abi.parse(abi.SIGNATURES[sym]):
+            if kind == "S":
+                fields[name] = Field(ins[-1], lo)     # scratch, never touched
+            elif kind == "I":
+                if name == "distance0":
+                    d = far
+                elif name in ("phi", "phi0", "u_cur") and level_set not in [
+                        f.data for f in fields.values()]:
+                    d = level_set
+                else:
+                    d = ins[k_in]
+                    k_in += 1
+                fields[name] = Field(d, lo)
+                nbytes += 8 * cells
+            elif kind in ("O", "X"):
+                fields[name] = Field(pool[k_out], lo)
+                k_out += 1
+                nbytes += (2 if kind == "X" else 1) * 8 * cells
+            elif kind == "R":
+                scal[name] = {"dx": cfg["dx"][0], "dy": cfg["dx"][1], "dz": cfg["dx"][2],
+                              "dt": 1e-3, "cfl_number": 0.5, "vel_n": 0.8, "b": 0.1}[name]
+            elif kind == "N":
+                scal[name] = 0
+        for _ in range(2):
+            tb.call(sym, fields, fb, **scal)
+        timer.start()
+        for _ in range(reps):
+            tb.call(sym, fields, fb, **scal)
+        timer.stop()
+        ms = timer.ms() / reps
+        gbs = nbytes / (ms / 1e3) / 1e9
+        res[sym] = {"ms": round(ms, 4), "algorithmic_bytes": nbytes,
+                    "gb_s": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 3)}
+    return {"grid": "256^3 fill box, 262^3 ghost boxes, FP64, device arrays, mean of "
+                    "%d calls" % reps, "routines": res}
 
 
 def deformation_run(ws, d_phi, fb, cfg, timer):
@@ -652,6 +732,22 @@ def profile_kernels():
         del a, b, c, f
 
 
+def profile_adjoint():
+    """The config-5 problem's forward run and reverse sweep, twice (for ncu
+    captures of the adjoint stage kernel)."""
+    from lsmlib_b200 import adjoint, workloads
+    cfg = workloads.config5()
+    p = adjoint.AdvectionAdjoint(cfg["n"], cfg["dx"], cfg["x_lo"], cfg["lattice"],
+                                 cfg["steps"], 15)
+    p.set_theta(cfg["theta"])
+    p.set_dt(p.cfl_dt(cfg["cfl"]))
+    p.set_fields(cfg["phi0"], cfg["target"], cfg["eps"])
+    for _ in range(2):
+        p.forward()
+        p.backward()
+    p.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -666,11 +762,16 @@ def main():
                     help="skip the adjoint leg (config 5)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched uneven-grid leg (config 4)")
+    ap.add_argument("--no-toolbox", action="store_true",
+                    help="skip the per-routine drop-in timings")
     ap.add_argument("--no-deformation", action="store_true",
                     help="skip the deformation leg (config 3)")
     ap.add_argument("--config3-full", action="store_true",
                     help="run the config-3 full reversal at 512^3 (minutes) instead of 256^3")
     ap.add_argument("--size", type=int, default=256, help="interior cells per axis")
+    ap.add_argument("--profile-adjoint", action="store_true",
+                    help="only run the config-5 forward and reverse sweep twice "
+                         "(for ncu captures) and exit")
     ap.add_argument("--profile", action="store_true",
                     help="only launch the two fused stage kernels twice each "
                          "(for ncu captures) and exit")
@@ -682,6 +783,9 @@ def main():
     world, rank, local, pg = dist_setup(args.gpus)
     if args.profile:
         profile_kernels()
+        return
+    if args.profile_adjoint:
+        profile_adjoint()
         return
     if args.impl == "reference":
         line = run_reference(args, world, rank)
