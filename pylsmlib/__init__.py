@@ -1,9 +1,18 @@
 """pylsmlib -- Python home of the level-set tools.
 
-The reference's pylsmlib wraps only its fast marching routines; here it holds
-the differentiable level-set advection: :class:`LevelSetAdvectionLoss`, a
-``torch.autograd.Function`` whose backward pass is the hand-written discrete
-adjoint of upwind HJ-WENO5 + TVD-RK3 in liblsmgpu.so.  PyTorch is used only in
-this package.
+The reference's pylsmlib wraps only its fast marching routines.  Here it holds
+the torch-facing front door of the GPU library:
+
+* :class:`Grid` -- the serial package's grid (ghost layers by accuracy, index
+  spaces, grid-point coordinates);
+* :class:`LevelSetIntegrator` -- fused TVD-RK3 time stepping of CUDA tensors
+  (normal speed with reinitialization, external velocity, the deformation
+  field, reinitialization alone), on torch's current stream;
+* :class:`LevelSetAdvectionLoss` / :func:`advection_loss` -- a
+  ``torch.autograd.Function`` whose backward pass is the hand-written discrete
+  adjoint of upwind HJ-WENO5 + TVD-RK3.
+
+PyTorch is used only in this package.
 """
 from .adjoint import LevelSetAdvectionLoss, advection_loss  # noqa: F401
+from .levelset import Grid, LevelSetIntegrator  # noqa: F401
