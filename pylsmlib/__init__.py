@@ -8,6 +8,8 @@ the torch-facing front door of the GPU library:
 * :class:`LevelSetIntegrator` -- fused TVD-RK3 time stepping of CUDA tensors
   (normal speed with reinitialization, external velocity, the deformation
   field, reinitialization alone), on torch's current stream;
+* :func:`write_data_array` / :func:`read_data_array` -- the serial
+  package's data-array files (dims header, x-fastest values, gzip/bzip2);
 * :class:`LevelSetAdvectionLoss` / :func:`advection_loss` -- a
   ``torch.autograd.Function`` whose backward pass is the hand-written discrete
   adjoint of upwind HJ-WENO5 + TVD-RK3.
@@ -16,3 +18,5 @@ PyTorch is used only in this package.
 """
 from .adjoint import LevelSetAdvectionLoss, advection_loss  # noqa: F401
 from .levelset import Grid, LevelSetIntegrator  # noqa: F401
+from .data_arrays import (BZIP2, GZIP, NO_ZIP, read_data_array,  # noqa: F401
+                          write_data_array)
