@@ -2,9 +2,14 @@
 
 * ``oracle_toolbox()`` -- the hand-written C restatement (lsm_oracle.c), built
   by ``make -C oracle`` into ``oracle/_build/liboracle.so``;
+* ``oracle_fmm()`` -- the C restatement of the fast marching method's distance
+  function (fmm_oracle.c), in the same library;
 * ``reference_toolbox()`` -- the reference's own Fortran routines, translated
   by ``oracle/f77toc.py`` and built by ``make -C oracle ref`` into
-  ``oracle/_ref/libref.so`` (needs the reference sources at build time only).
+  ``oracle/_ref/libref.so`` (needs the reference sources at build time only);
+* ``reference_fmm()`` -- the reference's own C fast marching method
+  (``computeDistanceFunction3d``), built by ``make -C oracle ref`` into
+  ``oracle/_ref/libfmm.so``.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU legs import this
 package; the product path in lsmlib_b200/ never does.
@@ -17,6 +22,7 @@ from lsmlib_b200.toolbox import Toolbox
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref.so")
+FMM_SO = os.path.join(HERE, "_ref", "libfmm.so")
 
 
 def _load(path):
@@ -39,6 +45,42 @@ def reference_available():
 
 def reference_toolbox():
     return Toolbox(_load(REF_SO), prefix="ref_")
+
+
+def fmm_available():
+    return os.path.exists(FMM_SO)
+
+
+def _distance_fn(fn, name):
+    import numpy as np
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+
+    def run(phi, order, dx, mask=None):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        out = np.zeros_like(phi)
+        dims = np.array(phi.shape[::-1], dtype=np.intc)
+        h = np.array(dx, dtype=np.float64)
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
+        rc = fn(out.ctypes.data, phi.ctypes.data, None if m is None else m.ctypes.data,
+                int(order), dims.ctypes.data, h.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("%s returned %d" % (name, rc))
+        return out
+    return run
+
+
+def reference_fmm():
+    """The reference's computeDistanceFunction3d (lsm_fast_marching_method.h:
+    386-392) as ``f(phi, order, dx, mask=None) -> distance`` on C-ordered
+    (nz, ny, nx) numpy arrays (x fastest in memory), dx in x, y, z order."""
+    return _distance_fn(_load(FMM_SO).computeDistanceFunction3d, "computeDistanceFunction3d")
+
+
+def oracle_fmm():
+    """The C restatement of the same heap march (fmm_oracle.c), same call."""
+    return _distance_fn(oracle_lib().orc_computeDistanceFunction3d,
+                        "orc_computeDistanceFunction3d")
 
 
 def heaviside(x, eps):

@@ -1,0 +1,354 @@
+/*
+ * fmm_oracle.c -- CPU restatement of the reference's fast marching method
+ * for the signed distance function (test infrastructure only: the tests and
+ * bench.py's CPU leg call it to check and time the GPU distance solver).
+ *
+ * It follows, step by step:
+ *   - computeDistanceFunction3d -> computeExtensionFields3d with no fields
+ *     (src/serial/lsm_FMM_field_extension.c:203-395): every value starts at
+ *     -1, points with mask < 0 are OUTSIDE_DOMAIN and hold LSMLIB_REAL_MAX;
+ *   - the first-order front initialisation, used at both orders
+ *     (:397-668): a point on the zero level set (|phi| < 1e-11) gets
+ *     +-1e-11, a point whose neighbour along an axis has phi of the other
+ *     sign (or zero) gets +-sqrt(1 / sum_axes 1/d_axis^2) with d_axis the
+ *     nearer linear-interpolated crossing; both become KNOWN;
+ *   - FMM_Core_initializeFront (src/toolbox/fast_marching_method/
+ *     FMM_Core.c:176-246): the front points, in a heap keyed on their signed
+ *     values, are popped in order and each updates its non-KNOWN neighbours;
+ *   - FMM_Core_advanceFront / FMM_Core_updateNeighbors (FMM_Core.c:321-451):
+ *     the TRIAL point of smallest |d| becomes KNOWN and recomputes the trial
+ *     value of each non-KNOWN neighbour (x-, x+, y-, y+, z-, z+);
+ *   - the trial update (lsm_FMM_field_extension.c:966-1176 first order,
+ *     :1180-1400 second order): per axis the KNOWN neighbour of smaller |d|
+ *     (minus first, plus when strictly smaller), at second order with the
+ *     next point in that direction when KNOWN and not larger in |d|; the
+ *     upwind quadratic with coefficients accumulated over x, y, z; a
+ *     negative discriminant keeps the current value;
+ *   - the binary heap of FMM_Heap.c:118-470 (insert with sift-up, extract
+ *     moving the last node into the root's slot and sifting down, update
+ *     sifting up when below the parent and down otherwise), with the same
+ *     comparisons so that ties are broken the same way.
+ */
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+
+typedef double real;
+
+#define ZERO_TOL 1.0e-11
+#define REAL_MAX DBL_MAX
+
+enum { FAR = 0, TRIAL = 1, KNOWN = 2, OUTSIDE = 3 };
+
+/* ---- indexed binary heap (FMM_Heap.c) --------------------------------- */
+typedef struct {
+  long idx;   /* linear grid index */
+  real value;
+  int pos;    /* position in the heap order */
+} hnode;
+
+typedef struct {
+  hnode *nodes; /* by handle */
+  int *heap;    /* position -> handle */
+  int size, cap;
+} fheap;
+
+static void h_init(fheap *h, int cap) {
+  h->cap = cap > 16 ? cap : 16;
+  h->size = 0;
+  h->nodes = (hnode *)malloc(sizeof(hnode) * h->cap);
+  h->heap = (int *)malloc(sizeof(int) * h->cap);
+}
+
+static void h_free(fheap *h) {
+  free(h->nodes);
+  free(h->heap);
+}
+
+static void h_grow(fheap *h) {
+  h->cap *= 2;
+  h->nodes = (hnode *)realloc(h->nodes, sizeof(hnode) * h->cap);
+  h->heap = (int *)realloc(h->heap, sizeof(int) * h->cap);
+}
+
+static inline int parent_pos(int p) { return (p + 1) / 2 - 1; }
+static inline int left_pos(int p) { return 2 * (p + 1) - 1; }
+static inline int right_pos(int p) { return 2 * (p + 1); }
+
+static void h_swap(fheap *h, int a, int b) {
+  h->nodes[h->heap[a]].pos = b;
+  h->nodes[h->heap[b]].pos = a;
+  int t = h->heap[a];
+  h->heap[a] = h->heap[b];
+  h->heap[b] = t;
+}
+
+static void h_up(fheap *h, int p) {
+  while (p > 0 &&
+         h->nodes[h->heap[p]].value < h->nodes[h->heap[parent_pos(p)]].value) {
+    h_swap(h, p, parent_pos(p));
+    p = parent_pos(p);
+  }
+}
+
+static void h_down(fheap *h, int p) {
+  for (;;) {
+    int l = left_pos(p), r = right_pos(p);
+    if (l >= h->size) return;
+    real cur = h->nodes[h->heap[p]].value;
+    real lv = h->nodes[h->heap[l]].value;
+    real rv = r < h->size ? h->nodes[h->heap[r]].value : REAL_MAX;
+    if (cur <= lv && cur <= rv) return;
+    if (lv < cur && lv <= rv) {
+      h_swap(h, p, l);
+      p = l;
+    } else if (r < h->size) {
+      h_swap(h, p, r);
+      p = r;
+    } else {
+      return;
+    }
+  }
+}
+
+static int h_insert(fheap *h, long idx, real value) {
+  int n = h->size;
+  h->heap[n] = n;
+  h->nodes[n].idx = idx;
+  h->nodes[n].value = value;
+  h->nodes[n].pos = n;
+  h_up(h, n);
+  h->size++;
+  if (h->size == h->cap) h_grow(h);
+  return h->size - 1;
+}
+
+/* Removes the root.  The node in the last handle slot moves into the root's
+ * slot; *moved_idx / *moved_handle say where it went (-1 when none moved). */
+static hnode h_extract(fheap *h, long *moved_idx, int *moved_handle) {
+  int n = h->size;
+  int root = h->heap[0];
+  hnode min = h->nodes[root];
+  *moved_idx = -1;
+  *moved_handle = -1;
+  if (root != n - 1) {
+    hnode mv = h->nodes[n - 1];
+    h->nodes[root] = mv;
+    h->heap[mv.pos] = root;
+    h->nodes[n - 1].value = REAL_MAX;
+    *moved_idx = mv.idx;
+    *moved_handle = root;
+  } else {
+    h->nodes[root].value = REAL_MAX;
+  }
+  /* the last position's node goes to the root and sifts down while the
+   * last position still counts (as FMM_Heap_extractMin does) */
+  h->nodes[h->heap[n - 1]].pos = 0;
+  h->heap[0] = h->heap[n - 1];
+  h_down(h, 0);
+  h->heap[n - 1] = -1;
+  h->size--;
+  return min;
+}
+
+static void h_update(fheap *h, int handle, real value) {
+  h->nodes[handle].value = value;
+  int p = h->nodes[handle].pos;
+  if (p > 0 && value < h->nodes[h->heap[parent_pos(p)]].value)
+    h_up(h, p);
+  else
+    h_down(h, p);
+}
+
+/* ---- the march ---------------------------------------------------------- */
+typedef struct {
+  real *d;
+  const real *phi;
+  unsigned char *st;
+  int *handle;
+  int n[3];
+  long s[3];
+  real dx[3];
+  int order;
+  fheap trial;
+} march_t;
+
+static real trial_update(march_t *m, long o, const int c[3]) {
+  real A = 0, B = 0, C = 0;
+  for (int dir = 0; dir < 3; dir++) {
+    real u1 = REAL_MAX, u2 = REAL_MAX;
+    int sw = 0;
+    for (int sg = -1; sg <= 1; sg += 2) {
+      int c1 = c[dir] + sg;
+      if (c1 < 0 || c1 >= m->n[dir]) continue;
+      long o1 = o + sg * m->s[dir];
+      if (m->st[o1] != KNOWN) continue;
+      if (sg == 1 && !(fabs(m->d[o1]) < fabs(u1))) continue;
+      u1 = m->d[o1];
+      u2 = REAL_MAX;
+      sw = 0;
+      if (m->order == 2) {
+        int c2 = c1 + sg;
+        if (c2 >= 0 && c2 < m->n[dir]) {
+          long o2 = o1 + sg * m->s[dir];
+          if (m->st[o2] == KNOWN && fabs(m->d[o2]) <= fabs(u1)) {
+            u2 = m->d[o2];
+            sw = 1;
+          }
+        }
+      }
+    }
+    if (u1 < REAL_MAX) {
+      real inv = 1 / m->dx[dir];
+      inv *= inv;
+      if (m->order == 1) {
+        A += inv;
+        B += inv * u1;
+        C += inv * u1 * u1;
+      } else {
+        real s = 1.0 + 0.5 * sw;
+        real contrib = sw == 1 ? 2.0 * u1 - 0.5 * u2 : u1;
+        A += inv * s * s;
+        B += inv * s * contrib;
+        C += inv * contrib * contrib;
+      }
+    }
+  }
+  if (fabs(A) == 0) return REAL_MAX;
+  B *= -2.0;
+  C -= 1.0;
+  real disc = B * B - 4.0 * A * C;
+  real out;
+  if (disc >= 0) {
+    if (B == 0)
+      out = 0;
+    else if (B < ZERO_TOL)
+      out = 0.5 * (-B + sqrt(disc)) / A;
+    else
+      out = 0.5 * (-B - sqrt(disc)) / A;
+  } else {
+    out = m->d[o];
+  }
+  m->d[o] = out;
+  return out;
+}
+
+static void update_neighbors(march_t *m, long o) {
+  int c[3];
+  c[0] = (int)(o % m->n[0]);
+  c[1] = (int)((o / m->n[0]) % m->n[1]);
+  c[2] = (int)(o / ((long)m->n[0] * m->n[1]));
+  for (int dir = 0; dir < 3; dir++) {
+    for (int sg = -1; sg <= 1; sg += 2) {
+      int q[3] = {c[0], c[1], c[2]};
+      q[dir] += sg;
+      if (q[dir] < 0 || q[dir] >= m->n[dir]) continue;
+      long oq = o + sg * m->s[dir];
+      if (m->st[oq] == KNOWN || m->st[oq] == OUTSIDE) continue;
+      real v = trial_update(m, oq, q);
+      if (v < 0) v = -v;
+      if (m->st[oq] == FAR) {
+        m->st[oq] = TRIAL;
+        m->handle[oq] = h_insert(&m->trial, oq, v);
+      } else {
+        h_update(&m->trial, m->handle[oq], v);
+      }
+    }
+  }
+}
+
+/* orc_computeDistanceFunction3d: arrays x fastest, grid_dims and dx in
+ * x, y, z order.  Returns 0, or 2 for an order other than 1 and 2. */
+int orc_computeDistanceFunction3d(real *distance, const real *phi, const real *mask,
+                                  int order, const int *grid_dims, const real *dx) {
+  if (order != 1 && order != 2) return 2;
+  march_t m;
+  m.d = distance;
+  m.phi = phi;
+  m.order = order;
+  for (int q = 0; q < 3; q++) {
+    m.n[q] = grid_dims[q];
+    m.dx[q] = dx[q];
+  }
+  m.s[0] = 1;
+  m.s[1] = m.n[0];
+  m.s[2] = (long)m.n[0] * m.n[1];
+  long np = m.s[2] * m.n[2];
+  m.st = (unsigned char *)calloc((size_t)np, 1);
+  m.handle = (int *)malloc(sizeof(int) * (size_t)np);
+  for (long o = 0; o < np; o++) {
+    distance[o] = -1;
+    m.handle[o] = -1;
+    if (mask && mask[o] < 0) {
+      m.st[o] = OUTSIDE;
+      distance[o] = REAL_MAX;
+    }
+  }
+  fheap known;
+  h_init(&known, m.n[0] + m.n[1] + m.n[2]);
+  h_init(&m.trial, m.n[0] + m.n[1] + m.n[2]);
+
+  /* the front (first-order initialisation at both orders) */
+  for (long o = 0; o < np; o++) {
+    if (m.st[o] == OUTSIDE) continue;
+    int c[3] = {(int)(o % m.n[0]), (int)((o / m.n[0]) % m.n[1]),
+                (int)(o / ((long)m.n[0] * m.n[1]))};
+    real pc = phi[o];
+    if (fabs(pc) < ZERO_TOL) {
+      distance[o] = pc > 0 ? ZERO_TOL : -ZERO_TOL;
+      m.st[o] = KNOWN;
+      h_insert(&known, o, distance[o]);
+      continue;
+    }
+    int borders = 0;
+    real sum = 0;
+    for (int dir = 0; dir < 3; dir++) {
+      real dp = REAL_MAX, dm = REAL_MAX;
+      if (c[dir] - 1 >= 0) {
+        real p = phi[o - m.s[dir]];
+        if (p * pc <= 0) {
+          dm = pc / (pc - p);
+          dm *= m.dx[dir];
+        }
+      }
+      if (c[dir] + 1 < m.n[dir]) {
+        real p = phi[o + m.s[dir]];
+        if (p * pc <= 0) {
+          dp = pc / (pc - p);
+          dp *= m.dx[dir];
+        }
+      }
+      if (dp < REAL_MAX || dm < REAL_MAX) {
+        borders = 1;
+        real dd = dp < dm ? dp : dm;
+        sum += 1 / dd / dd;
+      }
+    }
+    if (borders) {
+      distance[o] = pc > 0 ? sqrt(1.0 / sum) : -sqrt(1.0 / sum);
+      m.st[o] = KNOWN;
+      h_insert(&known, o, distance[o]);
+    }
+  }
+  /* the front's neighbours become trial points */
+  while (known.size > 0) {
+    long mi;
+    int mh;
+    hnode nd = h_extract(&known, &mi, &mh);
+    if (nd.value < REAL_MAX) update_neighbors(&m, nd.idx);
+  }
+  /* the march */
+  while (m.trial.size > 0) {
+    long mi;
+    int mh;
+    hnode nd = h_extract(&m.trial, &mi, &mh);
+    if (mh != -1) m.handle[mi] = mh;
+    m.st[nd.idx] = KNOWN;
+    update_neighbors(&m, nd.idx);
+  }
+  h_free(&known);
+  h_free(&m.trial);
+  free(m.st);
+  free(m.handle);
+  return 0;
+}

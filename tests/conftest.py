@@ -14,11 +14,10 @@ if GOLDEN not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
-    # the C oracle is test infrastructure; build it if this checkout lacks it
-    so = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
-    if not os.path.exists(so):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "all"],
-                       check=True, capture_output=True)
+    # the C oracle is test infrastructure; (re)build it when its sources are
+    # newer than this checkout's library
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "all"],
+                   check=True, capture_output=True)
 
 
 @pytest.fixture(scope="session")

@@ -1,0 +1,109 @@
+"""The checkers for the distance function.
+
+* The reference's own fast marching method, built from its C sources
+  (oracle/_ref/libfmm.so), reproduces the committed golden outputs bit for
+  bit (these pin the fixtures to the reference).
+* The C restatement of the heap march (oracle/fmm_oracle.c) reproduces the
+  same golden outputs, and the reference's results on seeded noisy unions of
+  spheres, bit for bit (these pin the restatement).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fmm_golden.npz")
+NAMES = ("spheres3d", "masked3d", "spheres2d")
+
+
+def _case(z, name):
+    """phi (nz, ny, nx), dx in x, y, z order, mask or None."""
+    mask = z[name + "|mask"] if name + "|mask" in z.files else None
+    return z[name + "|phi"], z[name + "|dx"][::-1], mask
+
+
+def seeded_spheres(shape, seed, noise=0.01):
+    """A noisy union of two spheres on [-1, 1] per axis: phi (nz, ny, nx) and
+    dx in x, y, z order (an axis of one point gets dx 1)."""
+    rng = np.random.default_rng(seed)
+    axes = [np.linspace(-1, 1, n) if n > 1 else np.zeros(1) for n in shape]
+    zz, yy, xx = np.meshgrid(*axes, indexing="ij")
+    c = rng.uniform(-0.3, 0.3, size=(2, 3))
+    r = rng.uniform(0.25, 0.5, size=2)
+    phi = np.minimum(np.sqrt((xx - c[0, 0]) ** 2 + (yy - c[0, 1]) ** 2 + (zz - c[0, 2]) ** 2) - r[0],
+                     np.sqrt((xx - c[1, 0]) ** 2 + (yy - c[1, 1]) ** 2 + (zz - c[1, 2]) ** 2) - r[1])
+    if noise:
+        phi = phi + noise * rng.standard_normal(shape)
+    dx = [2.0 / (n - 1) if n > 1 else 1.0 for n in shape[::-1]]
+    return phi, dx
+
+
+def seeded_mask(shape, seed):
+    """Outside-domain block for the masked seeded cases (None otherwise)."""
+    if seed != 2:
+        return None
+    mask = np.ones(shape)
+    mask[:, 5:20, 3:11] = -1.0
+    return mask
+
+
+@pytest.mark.skipif(not oracle.fmm_available(), reason="oracle/_ref/libfmm.so not built")
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_reference_fmm_reproduces_golden(name, order):
+    z = np.load(GOLDEN)
+    phi, dx, mask = _case(z, name)
+    got = oracle.reference_fmm()(phi, order, dx, mask)
+    assert np.array_equal(got.view(np.uint64), z["%s|out%d" % (name, order)].view(np.uint64))
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_oracle_fmm_reproduces_golden(name, order):
+    z = np.load(GOLDEN)
+    phi, dx, mask = _case(z, name)
+    got = oracle.oracle_fmm()(phi, order, dx, mask)
+    assert np.array_equal(got.view(np.uint64), z["%s|out%d" % (name, order)].view(np.uint64))
+
+
+@pytest.mark.skipif(not oracle.fmm_available(), reason="oracle/_ref/libfmm.so not built")
+@pytest.mark.parametrize("shape,seed", [((33, 41, 29), 1), ((20, 64, 48), 2), ((1, 80, 90), 3)])
+@pytest.mark.parametrize("order", [1, 2])
+def test_oracle_fmm_matches_reference(shape, seed, order):
+    phi, dx = seeded_spheres(shape, seed)
+    mask = seeded_mask(shape, seed)
+    a = oracle.oracle_fmm()(phi, order, dx, mask)
+    b = oracle.reference_fmm()(phi, order, dx, mask)
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def test_oracle_fmm_edge_cases():
+    fmm = oracle.oracle_fmm()
+    # no interface: no front, every point keeps the default -1
+    phi = np.ones((5, 6, 7))
+    assert np.all(fmm(phi, 1, [1.0, 1.0, 1.0]) == -1.0)
+    # a mask that excludes everything: LSMLIB_REAL_MAX everywhere
+    phi[2, 3, 3] = -1.0
+    out = fmm(phi, 2, [1.0, 1.0, 1.0], -np.ones_like(phi))
+    assert np.all(out == np.finfo(np.float64).max)
+    # points exactly on the interface hold -1e-11 (LSMLIB_ZERO_TOL, phi = 0
+    # is not > 0); the next ones are one and two cells away
+    phi = np.linspace(-1, 1, 9)[None, None, :] * np.ones((3, 4, 9))
+    out = fmm(phi, 1, [0.25, 1.0, 1.0])
+    assert np.all(out[..., 4] == -1e-11)
+    assert np.all(out[..., 5] == 0.25) and np.all(out[..., 6] == 0.5)
+    # an order other than 1 or 2 is refused with the reference's code 2
+    with pytest.raises(RuntimeError, match="returned 2"):
+        fmm(phi, 3, [1.0, 1.0, 1.0])
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_golden_distance_sign_follows_phi(name, order):
+    z = np.load(GOLDEN)
+    phi, d = z[name + "|phi"], z["%s|out%d" % (name, order)]
+    inside = np.abs(d) < 1e300
+    sel = inside & (np.abs(phi) > 1e-9)
+    assert np.all(np.sign(d[sel]) == np.sign(phi[sel]))
