@@ -393,6 +393,21 @@ void lsm3dcomputereinitializationeqnrhssubcellfixorder1_(
     LSMGPU_BOX6(grad_phi_minus_gb), LSMGPU_BOX6(fb), const LSMLIB_REAL *dx,
     const LSMLIB_REAL *dy, const LSMLIB_REAL *dz);
 
+/* ---- fast marching method: src/serial/lsm_fast_marching_method.h:386-392 --
+ * The signed distance to the zero level set of phi on a grid_dims[0] x
+ * grid_dims[1] x grid_dims[2] array (x fastest, dx[3] in x, y, z order), with
+ * the values of the reference's first- (order 1) or second-order (order 2)
+ * fast marching method: points on the interface hold +-1e-11, points no
+ * front reaches -1, points with mask < 0 (mask may be NULL)
+ * LSMLIB_REAL_MAX.  Computed on the GPU by sweeps to the march's fixed point
+ * (no heap).  Arrays are host or device pointers (see above); the call
+ * returns after the work finishes.  Returns 0, 2 for an order other than 1
+ * or 2 (LSM_FMM_ERR_INVALID_SPATIAL_DISCRETIZATION_ORDER), -1 for any other
+ * failure (the error is recorded for lsmgpu_get_last_error). */
+int computeDistanceFunction3d(LSMLIB_REAL *distance_function, LSMLIB_REAL *phi,
+                              LSMLIB_REAL *mask, int spatial_discretization_order,
+                              int *grid_dims, LSMLIB_REAL *dx);
+
 /* ======================================================================== */
 /* Part 2 -- extension API                                                   */
 /* ======================================================================== */
@@ -613,6 +628,16 @@ int lsmgpu_adjoint_gradient(lsmgpu_adjoint *h, double *loss,
                             double *grad_theta, double *grad_phi0);
 int lsmgpu_adjoint_timing(lsmgpu_adjoint *h, float *fwd_ms, float *adj_ms);
 int lsmgpu_adjoint_phi_final(lsmgpu_adjoint *h, double *host);
+
+/* ---- signed distance function -------------------------------------------------
+ * computeDistanceFunction3d with the lsmgpu error codes: LSMGPU_SUCCESS,
+ * LSMGPU_ERR_INVALID_VALUE for an order other than 1 or 2 or a dx <= 0,
+ * LSMGPU_ERR_INVALID_BOX for an empty grid; ``sweeps`` (may be NULL)
+ * receives the number of sweeps the fixed point took. */
+int lsmgpu_distance_function3d(double *distance_function, const double *phi,
+                               const double *mask, int order,
+                               const int grid_dims[3], const double dx[3],
+                               int *sweeps);
 
 /* ---- an entry point that allocates no memory --------------------------------
  * No counterpart in the reference.  For callers that must not allocate device

@@ -36,6 +36,7 @@ SOURCES = {
     "batched.cu": ["--fmad=true"],
     "adjoint.cu": ["--fmad=true"],
     "noalloc.cu": ["--fmad=false"],
+    "distance.cu": ["--fmad=false"],
 }
 
 

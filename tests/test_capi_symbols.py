@@ -16,10 +16,11 @@ def declared_functions():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     src = re.sub(r"#define[^\n]*(\\\n[^\n]*)*", "", src)
-    names = re.findall(r"\b([a-z_][a-z0-9_]*)\s*\(", src)
+    names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", src)
     skip = {"if", "defined", "sizeof"}
     return sorted({n for n in names if n not in skip and
-                   (n.startswith("lsm3d") or n.startswith("lsmgpu_"))})
+                   (n.startswith("lsm3d") or n.startswith("lsmgpu_") or
+                    n.startswith("compute"))})
 
 
 def test_header_declares_all_reference_symbols():

@@ -107,3 +107,17 @@ def test_golden_distance_sign_follows_phi(name, order):
     inside = np.abs(d) < 1e300
     sel = inside & (np.abs(phi) > 1e-9)
     assert np.all(np.sign(d[sel]) == np.sign(phi[sel]))
+
+
+def test_pylsmlib_distance_argument_errors():
+    """The reference pylsmlib's ValueErrors, raised before any GPU work."""
+    from pylsmlib import computeDistanceFunction
+    phi = np.zeros((4, 5))
+    with pytest.raises(ValueError, match="dx must be of length"):
+        computeDistanceFunction(phi, dx=[1.0, 1.0, 1.0])
+    with pytest.raises(ValueError, match="greater than zero"):
+        computeDistanceFunction(phi, dx=[1.0, 0.0])
+    with pytest.raises(ValueError, match="order must be 1 or 2"):
+        computeDistanceFunction(phi, dx=1.0, order=3)
+    with pytest.raises(ValueError, match="mask"):
+        computeDistanceFunction(phi, dx=1.0, mask=np.ones((5, 4)))

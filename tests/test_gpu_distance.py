@@ -1,0 +1,118 @@
+"""The GPU distance function (liblsmgpu.so computeDistanceFunction3d /
+lsmgpu_distance_function3d) against the reference's fast marching method:
+the committed golden outputs of the reference itself, and the C restatement
+of its heap march (oracle/fmm_oracle.c) on seeded inputs, bit for bit."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from test_fmm_golden import GOLDEN, NAMES, _case, seeded_mask, seeded_spheres
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from lsmlib_b200 import gpu
+    return gpu.load()
+
+
+def gpu_distance(lib, phi, order, dx, mask=None):
+    """lsmgpu_distance_function3d on host arrays (nz, ny, nx), dx in x, y, z."""
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    out = np.zeros_like(phi)
+    dims = (ctypes.c_int * 3)(*phi.shape[::-1])
+    h = (ctypes.c_double * 3)(*dx)
+    sweeps = ctypes.c_int(0)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
+    rc = lib.lsmgpu_distance_function3d(out.ctypes.data, phi.ctypes.data,
+                                        None if m is None else m.ctypes.data, order, dims, h,
+                                        ctypes.byref(sweeps))
+    assert rc == 0, lib.lsmgpu_get_last_error_string()
+    return out, sweeps.value
+
+
+def same_bits(a, b):
+    return np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_distance_reproduces_reference_golden(lib, name, order):
+    z = np.load(GOLDEN)
+    phi, dx, mask = _case(z, name)
+    got, _ = gpu_distance(lib, phi, order, dx, mask)
+    assert same_bits(got, z["%s|out%d" % (name, order)])
+
+
+@pytest.mark.parametrize("shape,seed", [((33, 41, 29), 1), ((20, 64, 48), 2), ((1, 80, 90), 3),
+                                        ((64, 64, 64), 4), ((40, 100, 70), 5)])
+@pytest.mark.parametrize("order", [1, 2])
+def test_distance_matches_oracle(lib, shape, seed, order):
+    phi, dx = seeded_spheres(shape, seed)
+    mask = seeded_mask(shape, seed)
+    want = oracle.oracle_fmm()(phi, order, dx, mask)
+    got, sweeps = gpu_distance(lib, phi, order, dx, mask)
+    assert same_bits(got, want), (np.mean(got == want), np.abs(got - want).max())
+    assert 0 < sweeps <= 16 * sum(shape) + 256
+
+
+def test_distance_c_abi_entry_point(lib):
+    """The reference's signature, host pointers, 0 on success and 2 for a bad
+    order (lsm_fast_marching_method.h:386-392)."""
+    z = np.load(GOLDEN)
+    phi, dx, _ = _case(z, "spheres3d")
+    fn = lib.computeDistanceFunction3d
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    phi = np.ascontiguousarray(phi)
+    out = np.zeros_like(phi)
+    dims = np.array(phi.shape[::-1], dtype=np.intc)
+    h = np.array(dx)
+    assert fn(out.ctypes.data, phi.ctypes.data, None, 2, dims.ctypes.data, h.ctypes.data) == 0
+    assert same_bits(out, z["spheres3d|out2"])
+    assert fn(out.ctypes.data, phi.ctypes.data, None, 3, dims.ctypes.data, h.ctypes.data) == 2
+
+
+def test_distance_device_arrays(lib):
+    """Device pointers are used in place (torch tensors on cuda:0)."""
+    import torch
+    phi, dx = seeded_spheres((24, 30, 36), 9)
+    want = oracle.oracle_fmm()(phi, 2, dx)
+    tp = torch.from_numpy(phi).cuda()
+    out = torch.empty_like(tp)
+    dims = (ctypes.c_int * 3)(*phi.shape[::-1])
+    h = (ctypes.c_double * 3)(*dx)
+    rc = lib.lsmgpu_distance_function3d(out.data_ptr(), tp.data_ptr(), None, 2, dims, h, None)
+    assert rc == 0
+    assert same_bits(out.cpu().numpy(), want)
+
+
+def test_distance_edge_cases(lib):
+    phi = np.ones((5, 6, 7))
+    got, _ = gpu_distance(lib, phi, 1, [1.0, 1.0, 1.0])
+    assert np.all(got == -1.0)                       # no interface: the default
+    phi[2, 3, 3] = -1.0
+    got, _ = gpu_distance(lib, phi, 2, [1.0, 1.0, 1.0], -np.ones_like(phi))
+    assert np.all(got == np.finfo(np.float64).max)   # all outside the domain
+    phi = np.linspace(-1, 1, 9)[None, None, :] * np.ones((3, 4, 9))
+    got, _ = gpu_distance(lib, phi, 1, [0.25, 1.0, 1.0])
+    assert same_bits(got, oracle.oracle_fmm()(phi, 1, [0.25, 1.0, 1.0]))
+    assert np.all(got[..., 4] == -1e-11)             # on the interface
+    one = np.array([[[0.3]]])                        # a single point
+    got, _ = gpu_distance(lib, one, 2, [1.0, 1.0, 1.0])
+    assert got[0, 0, 0] == -1.0
+
+
+def test_pylsmlib_compute_distance_function():
+    """The Python front door: C-ordered arrays, dx in shape order, 2D input."""
+    from pylsmlib import computeDistanceFunction
+    z = np.load(GOLDEN)
+    phi = z["spheres2d|phi"][0]
+    dx = z["spheres2d|dx"][1:]
+    got = computeDistanceFunction(phi, dx, order=2)
+    assert same_bits(got, z["spheres2d|out2"][0])
+    got1 = computeDistanceFunction(phi[5], dx[1], order=1)      # 1D
+    assert same_bits(got1, oracle.oracle_fmm()(phi[5][None, None, :], 1, [dx[1], 1.0, 1.0])[0, 0])
