@@ -399,8 +399,8 @@ void lsm3dcomputereinitializationeqnrhssubcellfixorder1_(
  * the values of the reference's first- (order 1) or second-order (order 2)
  * fast marching method: points on the interface hold +-1e-11, points no
  * front reaches -1, points with mask < 0 (mask may be NULL)
- * LSMLIB_REAL_MAX.  Computed on the GPU by sweeps to the march's fixed point
- * (no heap).  Arrays are host or device pointers (see above); the call
+ * LSMLIB_REAL_MAX.  Computed on the GPU as the march's fixed point, tile by
+ * tile (no heap).  Arrays are host or device pointers (see above); the call
  * returns after the work finishes.  Returns 0, 2 for an order other than 1
  * or 2 (LSM_FMM_ERR_INVALID_SPATIAL_DISCRETIZATION_ORDER), -1 for any other
  * failure (the error is recorded for lsmgpu_get_last_error). */
@@ -631,13 +631,14 @@ int lsmgpu_adjoint_phi_final(lsmgpu_adjoint *h, double *host);
 
 /* ---- signed distance function -------------------------------------------------
  * computeDistanceFunction3d with the lsmgpu error codes: LSMGPU_SUCCESS,
- * LSMGPU_ERR_INVALID_VALUE for an order other than 1 or 2 or a dx <= 0,
- * LSMGPU_ERR_INVALID_BOX for an empty grid; ``sweeps`` (may be NULL)
- * receives the number of sweeps the fixed point took. */
+ * LSMGPU_ERR_INVALID_VALUE for an order other than 1 or 2, a dx <= 0 or an
+ * input without a fixed point (NaN), LSMGPU_ERR_INVALID_BOX for an empty
+ * grid; ``passes`` (may be NULL) receives the number of passes over the
+ * active tiles of 16 x 8 x 8 points that the solve took. */
 int lsmgpu_distance_function3d(double *distance_function, const double *phi,
                                const double *mask, int order,
                                const int grid_dims[3], const double dx[3],
-                               int *sweeps);
+                               int *passes);
 
 /* ---- an entry point that allocates no memory --------------------------------
  * No counterpart in the reference.  For callers that must not allocate device

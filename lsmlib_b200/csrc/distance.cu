@@ -13,23 +13,16 @@
 //   - at second order, the next point along an axis when it is a front
 //     point or was accepted before the neighbour whose acceptance made the
 //     last update.
-// "Accepted before" is decided by acceptance time.  Mostly the heap accepts
-// in order of |d|, but an acceptance can lower a trial neighbour's value
-// below the key just popped (the second-order update is not monotone); the
-// heap then pops that neighbour next.  So a point's time is the pair
-// (e, s): e the largest key popped up to its acceptance, s = -1 when its
-// own key is e, else its |d|.
+// "Accepted before" is decided by acceptance time (Time3 below): mostly the
+// heap accepts in order of |d|, but an acceptance can lower a trial
+// neighbour's value below the key just popped (the second-order update is
+// not monotone), and the heap then pops that neighbour next.
 // The GPU computes the march's result as the fixed point of these rules,
 // without a heap:
 //   1. the front is initialised cell by cell exactly as the reference does
 //      (:397-668);
-//   2. every other point starts unreached and is swept in place: each thread
-//      walks a column in z (alternating up and down); a point takes its free
-//      neighbours in order of time, each while it comes before the point's
-//      own time given the ones taken so far, and stores its value and time
-//      when either changes.  The sweeps stop when a batch of them changes
-//      nothing.  A point depends only on points accepted before it, which
-//      settle first;
+//   2. every other point starts unreached; passes over a band of active
+//      points (below) evaluate the rules until nothing changes;
 //   3. points no front reaches keep the reference's default -1; points with
 //      mask < 0 are outside the domain and hold LSMLIB_REAL_MAX.
 // Built with --fmad=false so the update rounds as the reference's C does.
@@ -49,13 +42,40 @@ namespace {
 enum : unsigned char { kOutside = 0, kFront = 1, kFree = 2 };
 constexpr double kZeroTol = 1.0e-11;   // LSMLIB_ZERO_TOL of the FP64 build
 
-__device__ __forceinline__ long lin(int i, int j, int k, int nx, int ny) {
-  return (long)i + (long)nx * ((long)j + (long)ny * k);
+// Acceptance time of a free point, compared lexicographically.  A point the
+// heap pops with the largest key so far (a "root") has time (|d|, -1, -1).
+// A point an acceptance lowered below the keys already popped is popped
+// right after its trigger (the last neighbour accepted before it), ahead of
+// every larger key: its time extends the trigger's by its own |d| at the
+// first level where |d| exceeds the trigger's key -- (a, |d|, -1) under a
+// root trigger, (a, b, |d|) when it drops below a lowered trigger's key b.
+// A time therefore always follows its trigger's.  Deeper lowering (below a
+// third-level key) keeps the trigger's time; it has not been seen in
+// practice.
+struct Time3 {
+  double a, b, c;
+};
+
+__device__ __forceinline__ bool tless(const Time3& x, const Time3& y) {
+  return x.a < y.a || (x.a == y.a && (x.b < y.b || (x.b == y.b && x.c < y.c)));
+}
+
+__device__ __forceinline__ bool tequal(const Time3& x, const Time3& y) {
+  return x.a == y.a && x.b == y.b && x.c == y.c;
+}
+
+// the time of a point with key ``a`` whose trigger has time ``x`` (no free
+// trigger: a root)
+__device__ __forceinline__ Time3 tafter(const Time3& x, double a, bool has_trigger) {
+  if (!has_trigger || a > x.a) return Time3{a, -1.0, -1.0};
+  if (x.b < 0 || a > x.b) return Time3{x.a, a, -1.0};
+  if (x.c < 0 || a > x.c) return Time3{x.a, x.b, a};
+  return x;
 }
 
 // FMM_initializeFront_FieldExtension3d_Order1 (lsm_FMM_field_extension.c:
 // 397-668) for one point; the neighbours' phi is read whatever their mask
-__global__ void k_fmm_front(double* d, double* e, unsigned char* st, const double* phi,
+__global__ void k_fmm_front(double* d, Time3* tm, unsigned char* st, const double* phi,
                             const double* mask, int nx, int ny, int nz, double dx,
                             double dy, double dz) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -64,8 +84,8 @@ __global__ void k_fmm_front(double* d, double* e, unsigned char* st, const doubl
   const int n[3] = {nx, ny, nz};
   const double h[3] = {dx, dy, dz};
   for (int k = blockIdx.z; k < nz; k += gridDim.z) {
-    const long o = lin(i, j, k, nx, ny);
-    e[o] = INFINITY;
+    const long o = (long)i + (long)nx * ((long)j + (long)ny * k);
+    tm[o] = Time3{INFINITY, INFINITY, INFINITY};
     if (mask && mask[o] < 0) {
       st[o] = kOutside;
       d[o] = DBL_MAX;
@@ -118,42 +138,32 @@ __device__ __forceinline__ bool known(const double* d, const unsigned char* st, 
   return st[o] != kOutside && fabs(d[o]) <= DBL_MAX;
 }
 
-// Acceptance time of a free point in the reference's march, as the pair
-// (e, s): e is the largest key popped from the heap up to and including the
-// point's own acceptance, s is -1 for a point accepted with that key and |d|
-// for a point whose value an acceptance lowered below e (the heap pops it,
-// and the other lowered points in order of |d|, before any larger key).
-// Front points are KNOWN before every free point.
-__device__ __forceinline__ double time_s(double v, double e) {
-  const double a = fabs(v);
-  return a < e ? a : -1.0;
-}
-__device__ __forceinline__ bool before(double ea, double sa, double eb, double sb) {
-  return ea < eb || (ea == eb && sa < sb);
-}
-
 // The neighbours of one point, by slot 2*axis + (plus side): the immediate
-// neighbour (value v1, time e1) and, at second order, the next one in that
-// direction (v2, e2).
+// neighbour (value v1, time t1) and, at second order, the next one in that
+// direction (value v2; its time is read when needed).
 struct Stencil {
-  double v1[6], e1[6], v2[6], e2[6];
+  double v1[6], v2[6];
+  Time3 t1[6];
+  long o2[6];
   unsigned char has1, front1, has2, front2;  // bit per slot
 };
 
-// The reference's trial update (:1021-1119 first order, :1232-1381 second
-// order) over the immediate neighbours in ``incl`` (bit per slot).  Per axis
-// the minus neighbour is taken when included and replaced by the plus one
-// when its |d| is strictly smaller.  At second order the next point in the
-// chosen direction counts when it was KNOWN at the update -- a front point,
-// or a free point accepted before the neighbour whose acceptance made the
-// update (time (te, ts); -inf in the front phase) -- and its |d| is not
-// above the neighbour's.  Coefficients accumulate over x, y, z; returns
-// false when the discriminant is negative (the reference then keeps the
-// point's previous value).
+// The coefficients of the reference's trial update (:1021-1119 first order,
+// :1232-1381 second order) over the immediate neighbours in ``incl`` (bit
+// per slot), accumulated in its order and rounding.  Per axis the minus
+// neighbour is taken when included and replaced by the plus one when its
+// |d| is strictly smaller.  At second order the next point in the chosen
+// direction counts when it was KNOWN at the update -- a front point, or a
+// free point accepted before the trigger (time ``trig``; the front phase
+// comes before every free point) -- and its |d| is not above the
+// neighbour's.  Returns the discriminant B^2 - 4AC.
 template <int ORDER>
-__device__ __forceinline__ bool fmm_quad(const Stencil& n, int incl, double te, double ts,
-                                         const double i2[3], double& out) {
-  double A = 0, B = 0, C = 0;
+__device__ __forceinline__ double fmm_coeffs(const Stencil& n, const Time3* tm, int incl,
+                                             const Time3& trig, bool has_trigger,
+                                             const double i2[3], double& A, double& B) {
+  double C = 0;
+  A = 0;
+  B = 0;
 #pragma unroll
   for (int dir = 0; dir < 3; dir++) {
     double u1 = DBL_MAX, u2 = DBL_MAX;
@@ -166,9 +176,8 @@ __device__ __forceinline__ bool fmm_quad(const Stencil& n, int incl, double te, 
       u1 = n.v1[q];
       u2 = DBL_MAX;
       sw = 0;
-      if (ORDER == 2 && (n.has2 & (1 << q)) &&
-          ((n.front2 & (1 << q)) || before(n.e2[q], time_s(n.v2[q], n.e2[q]), te, ts)) &&
-          fabs(n.v2[q]) <= fabs(u1)) {
+      if (ORDER == 2 && (n.has2 & (1 << q)) && fabs(n.v2[q]) <= fabs(u1) &&
+          ((n.front2 & (1 << q)) || (has_trigger && tless(tm[n.o2[q]], trig)))) {
         u2 = n.v2[q];
         sw = 1;
       }
@@ -189,27 +198,52 @@ __device__ __forceinline__ bool fmm_quad(const Stencil& n, int incl, double te, 
   }
   B *= -2.0;
   C -= 1.0;
-  const double disc = B * B - 4.0 * A * C;
-  if (!(disc >= 0)) return false;
-  if (B == 0) out = 0;
-  else if (B < kZeroTol) out = 0.5 * (-B + sqrt(disc)) / A;
-  else out = 0.5 * (-B - sqrt(disc)) / A;
-  return true;
+  return B * B - 4.0 * A * C;
 }
+
+// The root the reference takes (disc >= 0), in its rounding.
+__device__ __forceinline__ double fmm_root(double A, double B, double disc) {
+  if (B == 0) return 0;
+  if (B < kZeroTol) return 0.5 * (-B + sqrt(disc)) / A;
+  return 0.5 * (-B - sqrt(disc)) / A;
+}
+
+// ---- the band solver ----------------------------------------------------------
+// The threshold T on acceptance time (its first level) advances in steps; a
+// point's value is stored only while its time is within T.  A point depends
+// only on points with earlier times, so the points within T settle exactly
+// and are never revised once T has moved past them: the work follows a thin
+// band, as the march does, instead of relaxing the whole grid.  Each pass
+// evaluates the points of the active list, one thread per point, from its
+// neighbours' current values; a point whose value or time changed queues
+// the points whose stencil reads it for the next pass.  A point whose time
+// is above T keeps its time as a candidate and waits in a pending list;
+// when a pass queues nothing, T moves to max(T + delta, smallest
+// candidate) and the pending points it reaches are queued.  Points
+// evaluated in the same pass may read one another mid-update; any change
+// queues the readers again, so the final pass reads settled values.
+
+// the threshold advances by this many of the smallest spacing per step
+constexpr double kDeltaCells = 2.0;
 
 // The value and acceptance time of free point o from its neighbours' current
 // values and times: the reference's last trial update.  Every front point is
 // KNOWN before the march starts (FMM_Core.c:203-243), so the front
 // neighbours are always in the update.  The free neighbours are taken in
-// order of acceptance time; each is in the update when the heap accepted it
-// while this point was still a trial point, i.e. before this point's time as
-// given by the neighbours taken so far.  A negative discriminant keeps the
-// previous value, -1 (the reference's default) when there is none.
+// order of time; each is in the update when the heap accepted it while this
+// point was still a trial point, i.e. before this point's time as given by
+// the neighbours taken so far.  The set must also be consistent with the
+// point's final time -- every neighbour in it accepted before the point --
+// as it always is in a real march; when it is not (a transient state of the
+// passes), the set is cut before the earliest offending neighbour and the
+// update is taken again.  A negative discriminant keeps the previous value,
+// -1 (the reference's default) when there is none.  Neighbours off the grid
+// are left out, as the reference's bounds checks do.
 template <int ORDER>
-__device__ __forceinline__ void fmm_point(const double* d, const double* e,
+__device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
                                           const unsigned char* st, long o, const int c[3],
                                           const int n[3], const long s[3], const double i2[3],
-                                          double& val, double& ev, bool& any_known) {
+                                          double& val, Time3& tv) {
   Stencil nb;
   nb.has1 = nb.front1 = nb.has2 = nb.front2 = 0;
 #pragma unroll
@@ -217,95 +251,242 @@ __device__ __forceinline__ void fmm_point(const double* d, const double* e,
     const int dir = q >> 1;
     const int sg = (q & 1) ? 1 : -1;
     nb.v1[q] = nb.v2[q] = DBL_MAX;
-    nb.e1[q] = nb.e2[q] = INFINITY;
+    nb.t1[q] = Time3{INFINITY, INFINITY, INFINITY};
+    nb.o2[q] = 0;
     const int c1 = c[dir] + sg;
     if (c1 < 0 || c1 >= n[dir]) continue;
     const long o1 = o + sg * s[dir];
     if (!known(d, st, o1)) continue;
     nb.v1[q] = d[o1];
-    nb.e1[q] = e[o1];
     nb.has1 |= 1 << q;
     if (st[o1] == kFront) nb.front1 |= 1 << q;
+    else nb.t1[q] = tm[o1];
     if (ORDER == 2) {
       const int c2 = c1 + sg;
       if (c2 < 0 || c2 >= n[dir]) continue;
       const long o2 = o1 + sg * s[dir];
       if (!known(d, st, o2)) continue;
       nb.v2[q] = d[o2];
-      nb.e2[q] = e[o2];
+      nb.o2[q] = o2;
       nb.has2 |= 1 << q;
       if (st[o2] == kFront) nb.front2 |= 1 << q;
     }
   }
-  any_known = nb.has1 != 0;
-  if (!any_known) return;
-  int incl = nb.front1;
-  bool have = incl != 0;
-  val = -1.0;
-  double elast = -INFINITY;             // e of the last free neighbour taken
-  double te = -INFINITY, ts = -1.0;     // its time (the front phase before all)
-  if (have) {
-    double t;
-    if (fmm_quad<ORDER>(nb, incl, te, ts, i2, t)) val = t;
-  }
-  for (int rem = nb.has1 & ~nb.front1; rem;) {
-    // the earliest remaining free neighbour (ties by slot)
-    int best = 0;
-    double be = INFINITY, bs = INFINITY;
-#pragma unroll
-    for (int q = 5; q >= 0; q--) {
-      if (!(rem & (1 << q))) continue;
-      const double eq = nb.e1[q], sq = time_s(nb.v1[q], nb.e1[q]);
-      if (!before(be, bs, eq, sq)) {
-        best = q;
-        be = eq;
-        bs = sq;
-      }
-    }
-    rem &= ~(1 << best);
+  if (!nb.has1) return false;
+  const int free1 = nb.has1 & ~nb.front1;
+  Time3 cap{INFINITY, INFINITY, INFINITY};   // only neighbours before this
+  for (;;) {
+    int incl = nb.front1;
+    bool have = incl != 0, trig_free = false;
+    Time3 trig{-INFINITY, -1.0, -1.0};
+    double cur = -1.0;
     if (have) {
-      const double a = fabs(val);
-      if (!before(be, bs, a > elast ? a : elast, a < elast ? a : -1.0)) break;
+      double A, B;
+      const double disc = fmm_coeffs<ORDER>(nb, tm, incl, trig, false, i2, A, B);
+      if (disc >= 0) cur = fmm_root(A, B, disc);
     }
-    incl |= 1 << best;
-    elast = te = be;
-    ts = bs;
-    double t;
-    if (fmm_quad<ORDER>(nb, incl, te, ts, i2, t)) val = t;
-    have = true;
+    for (int rem = free1; rem;) {
+      // the earliest remaining free neighbour (ties by slot)
+      int best = 0;
+      Time3 bt{INFINITY, INFINITY, INFINITY};
+#pragma unroll
+      for (int q = 5; q >= 0; q--) {
+        if (!(rem & (1 << q))) continue;
+        if (!tless(bt, nb.t1[q])) {
+          best = q;
+          bt = nb.t1[q];
+        }
+      }
+      rem &= ~(1 << best);
+      if (!tless(bt, cap)) break;
+      if (have && !tless(bt, tafter(trig, fabs(cur), trig_free))) break;
+      incl |= 1 << best;
+      trig = bt;
+      trig_free = true;
+      double A, B;
+      const double disc = fmm_coeffs<ORDER>(nb, tm, incl, trig, true, i2, A, B);
+      if (disc >= 0) cur = fmm_root(A, B, disc);
+      have = true;
+    }
+    const Time3 t = tafter(trig, fabs(cur), trig_free);
+    // the earliest neighbour in the set not accepted before the point
+    bool bad = false;
+    Time3 badt{INFINITY, INFINITY, INFINITY};
+#pragma unroll
+    for (int q = 0; q < 6; q++)
+      if ((incl & free1 & (1 << q)) && !tless(nb.t1[q], t) && tless(nb.t1[q], badt)) {
+        bad = true;
+        badt = nb.t1[q];
+      }
+    if (!bad) {
+      val = cur;
+      tv = t;
+      return true;
+    }
+    cap = badt;
   }
-  const double a = fabs(val);
-  ev = a > elast ? a : elast;
 }
 
-// One sweep over the free points, columns walked up (up != 0) or down in z;
-// a point's value and time are stored when either changes.
-template <int ORDER>
-__global__ void k_fmm_sweep(double* d, double* e, const unsigned char* st, int nx, int ny,
-                            int nz, double i2x, double i2y, double i2z, int up, int* changed) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= nx || j >= ny) return;
-  const double i2[3] = {i2x, i2y, i2z};
-  const int n[3] = {nx, ny, nz};
+// Device state of the solve, read and advanced by the kernels so that the
+// host only launches and, every few passes, looks at ``done``.
+struct Ctrl {
+  int pass;                  // passes run so far
+  int count[2];              // lengths of the two active lists (by pass parity)
+  int pend_count[2];         // lengths of the two pending lists (by epoch parity)
+  int epoch;                 // number of threshold advances
+  int done;
+  int advance;               // the last control step moved the threshold
+  int filter_count;          // length of the pending list being filtered
+  int pad;
+  double T;                  // threshold on the first level of the time
+  unsigned long long minrej; // bits of the smallest candidate queued since
+                             // the last advance (times are >= 0)
+  unsigned long long minkeep;// bits of the smallest candidate kept waiting
+};
+
+struct Lists {
+  int* active;               // two lists of n points (by pass parity)
+  int* stamp;                // pass that last queued a point
+  int* pending;              // two lists of n points (by epoch parity)
+  int* pend_stamp;           // epoch + 1 that last queued a point
+};
+
+__device__ __forceinline__ void push_once(long p, int stamp_val, int* stamp, int* list,
+                                          int* count) {
+  if (atomicExch(stamp + p, stamp_val) != stamp_val) list[atomicAdd(count, 1)] = (int)p;
+}
+
+// The first active list: the free points next to the front.
+__global__ void k_fmm_seed(const unsigned char* st, int nx, int ny, int nz, Lists L,
+                           Ctrl* ctrl) {
+  const long n = (long)nx * ny * nz;
   const long s[3] = {1L, (long)nx, (long)nx * ny};
-  bool any = false;
-  for (int kk = 0; kk < nz; kk++) {
-    const int k = up ? kk : nz - 1 - kk;
-    const long o = lin(i, j, k, nx, ny);
+  const int nn[3] = {nx, ny, nz};
+  for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n;
+       o += (long)gridDim.x * blockDim.x) {
     if (st[o] != kFree) continue;
-    const int c[3] = {i, j, k};
-    double val, ev;
-    bool known_nb;
-    fmm_point<ORDER>(d, e, st, o, c, n, s, i2, val, ev, known_nb);
-    if (!known_nb) continue;
-    if (val != d[o] || ev != e[o]) {
-      d[o] = val;
-      e[o] = ev;
-      any = true;
+    const int c[3] = {(int)(o % nx), (int)((o / nx) % ny), (int)(o / s[2])};
+    bool near = false;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const int dir = q >> 1, sg = (q & 1) ? 1 : -1;
+      const int c1 = c[dir] + sg;
+      if (c1 >= 0 && c1 < nn[dir] && st[o + sg * s[dir]] == kFront) near = true;
+    }
+    if (near) push_once(o, 1, L.stamp, L.active, &ctrl->count[0]);
+  }
+}
+
+// One pass over the active list (count[pass & 1]).
+template <int ORDER>
+__global__ void __launch_bounds__(128)
+k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz,
+           double i2x, double i2y, double i2z, Lists L, Ctrl* ctrl) {
+  const int it = ctrl->pass;
+  const int par = it & 1;
+  const int count = ctrl->count[par];
+  const long n = (long)nx * ny * nz;
+  const int* cur = L.active + par * n;
+  int* next = L.active + (par ^ 1) * n;
+  int* next_count = &ctrl->count[par ^ 1];
+  const int ep = ctrl->epoch;
+  int* pend = L.pending + (ep & 1) * n;
+  int* pend_count = &ctrl->pend_count[ep & 1];
+  const double T = ctrl->T;
+  const double i2[3] = {i2x, i2y, i2z};
+  const int nn[3] = {nx, ny, nz};
+  const long s[3] = {1L, (long)nx, (long)nx * ny};
+  unsigned long long minrej = ~0ULL;
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < count; w += gridDim.x * blockDim.x) {
+    const long o = cur[w];
+    if (st[o] != kFree) continue;
+    const int c[3] = {(int)(o % nx), (int)((o / nx) % ny), (int)(o / s[2])};
+    double val;
+    Time3 tv;
+    if (!fmm_point<ORDER>(d, tm, st, o, c, nn, s, i2, val, tv)) continue;
+    const double old = d[o];
+    if (!(tv.a <= T)) {
+      // accepted after the threshold: a candidate only, waiting for T
+      val = copysign(INFINITY, old);
+      push_once(o, ep + 1, L.pend_stamp, pend, pend_count);
+      const unsigned long long bits = __double_as_longlong(tv.a);
+      minrej = bits < minrej ? bits : minrej;
+    }
+    if (val == old && tequal(tv, tm[o])) continue;
+    d[o] = val;
+    tm[o] = tv;
+    if (!(fabs(old) <= DBL_MAX) && !(fabs(val) <= DBL_MAX)) continue;   // invisible
+    // queue the free points whose stencil reads this one
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const int dir = q >> 1, sg = (q & 1) ? 1 : -1;
+#pragma unroll
+      for (int r = 1; r <= ORDER; r++) {
+        const int cr = c[dir] + r * sg;
+        if (cr < 0 || cr >= nn[dir]) break;
+        const long on = o + r * sg * s[dir];
+        if (st[on] == kFree) push_once(on, it + 2, L.stamp, next, next_count);
+      }
     }
   }
-  if (any) *changed = 1;
+  if (minrej != ~0ULL) atomicMin(&ctrl->minrej, minrej);
+}
+
+// Between passes (one thread): with points queued, the next pass runs at the
+// same threshold; else the threshold moves to max(T + delta, smallest
+// waiting candidate) and the pending list is filtered (next kernel); with
+// nothing waiting either, the solve is done.
+__global__ void k_fmm_control(double delta, Ctrl* ctrl) {
+  if (threadIdx.x != 0 || ctrl->done) return;
+  const int par = ctrl->pass & 1;
+  ctrl->advance = 0;
+  if (ctrl->count[par ^ 1] == 0) {
+    const int ep = ctrl->epoch;
+    const int np = ctrl->pend_count[ep & 1];
+    if (np == 0) {
+      ctrl->done = 1;
+    } else {
+      const unsigned long long m = ctrl->minrej < ctrl->minkeep ? ctrl->minrej : ctrl->minkeep;
+      const double lo = __longlong_as_double((long long)m);
+      const double step = ctrl->T + delta;
+      ctrl->T = lo > step ? lo : step;
+      ctrl->advance = 1;
+      ctrl->filter_count = np;
+      ctrl->pend_count[(ep & 1) ^ 1] = 0;
+      ctrl->epoch = ep + 1;
+      ctrl->minrej = __double_as_longlong(INFINITY);
+      ctrl->minkeep = __double_as_longlong(INFINITY);
+    }
+  }
+  ctrl->count[par] = 0;
+  ctrl->pass += 1;
+}
+
+// After a threshold advance: the pending points the threshold reaches join
+// the active list, the others wait in the other pending list.
+__global__ void k_fmm_filter(const double* d, const Time3* tm, long n, Lists L, Ctrl* ctrl) {
+  if (!ctrl->advance) return;
+  const int ep = ctrl->epoch;              // already advanced
+  const int np = ctrl->filter_count;
+  const int* src = L.pending + ((ep - 1) & 1) * n;
+  int* keep = L.pending + (ep & 1) * n;
+  const int par = ctrl->pass & 1;          // the coming pass
+  int* next = L.active + par * n;
+  const double T = ctrl->T;
+  unsigned long long mk = ~0ULL;
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < np; w += gridDim.x * blockDim.x) {
+    const long o = src[w];
+    if (fabs(d[o]) <= DBL_MAX) continue;   // reached since
+    const double t = tm[o].a;
+    if (t <= T) {
+      push_once(o, ctrl->pass + 1, L.stamp, next, &ctrl->count[par]);
+    } else if (t < INFINITY) {
+      push_once(o, ep + 1, L.pend_stamp, keep, &ctrl->pend_count[ep & 1]);
+      const unsigned long long bits = __double_as_longlong(t);
+      mk = bits < mk ? bits : mk;
+    }
+  }
+  if (mk != ~0ULL) atomicMin(&ctrl->minkeep, mk);
 }
 
 // free points no front reached: the reference's default value -1
@@ -316,7 +497,7 @@ __global__ void k_fmm_unreached(double* d, const unsigned char* st, long n) {
 }
 
 int distance3d(double* distance, const double* phi, const double* mask, int order,
-               const int* grid_dims, const double* dx, int* sweeps_out, const char* R) {
+               const int* grid_dims, const double* dx, int* passes_out, const char* R) {
   clear_error();
   if (!distance || !phi || !grid_dims || !dx) {
     set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null argument");
@@ -331,32 +512,64 @@ int distance3d(double* distance, const double* phi, const double* mask, int orde
     set_error(LSMGPU_ERR_INVALID_BOX, std::string(R) + ": empty grid");
     return LSMGPU_ERR_INVALID_BOX;
   }
-  if (!(dx[0] > 0) || !(dx[1] > 0) || !(dx[2] > 0)) {
-    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": dx must be positive");
+  if (!(dx[0] > 0) || !(dx[1] > 0) || !(dx[2] > 0) || !(dx[0] < INFINITY) ||
+      !(dx[1] < INFINITY) || !(dx[2] < INFINITY)) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": dx must be positive and finite");
     return LSMGPU_ERR_INVALID_VALUE;
   }
   const long n = (long)nx * ny * nz;
+  if (n > 0x7fffffffL) {
+    set_error(LSMGPU_ERR_INVALID_BOX, std::string(R) + ": more than 2^31 - 1 points");
+    return LSMGPU_ERR_INVALID_BOX;
+  }
+  const double hmin = fmin(dx[0], fmin(dx[1], dx[2]));
+  const double delta = kDeltaCells * hmin;
+  // a bound on the passes for inputs without a fixed point (NaN): the
+  // threshold crosses the grid in at most (diagonal / delta) steps of a
+  // few passes each
+  const long max_passes = 4096 + 32L * (nx + ny + nz);
   cudaStream_t st = cur_stream();
-  Staging s(st);
+  Staging stg(st);
   const Box b{{0, 0, 0}, {nx, ny, nz}};
-  double* dd = (double*)s.add(distance, b, 8, kOut, "distance_function", R);
-  const double* dp = dd ? (const double*)s.add(phi, b, 8, kIn, "phi", R) : nullptr;
+  double* dd = (double*)stg.add(distance, b, 8, kOut, "distance_function", R);
+  const double* dp = dd ? (const double*)stg.add(phi, b, 8, kIn, "phi", R) : nullptr;
   const double* dm = nullptr;
-  if (dp && mask) dm = (const double*)s.add(mask, b, 8, kIn, "mask", R);
+  if (dp && mask) dm = (const double*)stg.add(mask, b, 8, kIn, "mask", R);
   if (!dd || !dp || (mask && !dm)) return lsmgpu_peek_last_error();
   unsigned char* status = nullptr;
-  double* etime = nullptr;
-  int* changed = nullptr;
-  int h_changed = 0;
-  bool ok = cuda_ok(cudaMallocAsync((void**)&status, (size_t)n, st), R) &&
-            cuda_ok(cudaMallocAsync((void**)&etime, (size_t)n * sizeof(double), st), R) &&
-            cuda_ok(cudaMallocAsync((void**)&changed, sizeof(int), st), R);
-  const dim3 blk(32, 4, 1);
-  const dim3 grid2((nx + 31) / 32, (ny + 3) / 4, 1);
-  const dim3 grid3((nx + 31) / 32, (ny + 3) / 4, nz < 65535 ? nz : 65535);
+  Time3* tm = nullptr;
+  Lists L{nullptr, nullptr, nullptr, nullptr};
+  Ctrl* ctrl = nullptr;
+  const size_t un = (size_t)n;
+  bool ok = cuda_ok(cudaMallocAsync((void**)&status, un, st), R) &&
+            cuda_ok(cudaMallocAsync((void**)&tm, un * sizeof(Time3), st), R) &&
+            cuda_ok(cudaMallocAsync((void**)&L.active, 2 * un * sizeof(int), st), R) &&
+            cuda_ok(cudaMallocAsync((void**)&L.pending, 2 * un * sizeof(int), st), R) &&
+            cuda_ok(cudaMallocAsync((void**)&L.stamp, un * sizeof(int), st), R) &&
+            cuda_ok(cudaMallocAsync((void**)&L.pend_stamp, un * sizeof(int), st), R) &&
+            cuda_ok(cudaMallocAsync((void**)&ctrl, sizeof(Ctrl), st), R);
+  Ctrl h_ctrl{};
+  h_ctrl.T = delta;
+  h_ctrl.minrej = 0x7ff0000000000000ULL;   // +infinity
+  h_ctrl.minkeep = 0x7ff0000000000000ULL;
+  int sms = 148;
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const int elem_blocks = (int)((n + 255) / 256 < 8 * sms ? (n + 255) / 256 : 8 * sms);
   if (ok) {
-    k_fmm_front<<<grid3, blk, 0, st>>>(dd, etime, status, dp, dm, nx, ny, nz, dx[0], dx[1], dx[2]);
-    ++launch_counter();
+    ok = cuda_ok(cudaMemsetAsync(L.stamp, 0, un * sizeof(int), st), R) &&
+         cuda_ok(cudaMemsetAsync(L.pend_stamp, 0, un * sizeof(int), st), R) &&
+         cuda_ok(cudaMemcpyAsync(ctrl, &h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, st), R);
+  }
+  if (ok) {
+    const dim3 blk(32, 4, 1);
+    const dim3 grid3((nx + 31) / 32, (ny + 3) / 4, nz < 65535 ? nz : 65535);
+    k_fmm_front<<<grid3, blk, 0, st>>>(dd, tm, status, dp, dm, nx, ny, nz, dx[0], dx[1], dx[2]);
+    k_fmm_seed<<<elem_blocks, 256, 0, st>>>(status, nx, ny, nz, L, ctrl);
+    launch_counter() += 2;
     ok = cuda_ok(cudaGetLastError(), R);
   }
   // 1/dx, squared (:1077-1078)
@@ -365,46 +578,41 @@ int distance3d(double* distance, const double* phi, const double* mask, int orde
     i2[q] = 1 / dx[q];
     i2[q] *= i2[q];
   }
-  const int batch = 8;
-  const long max_sweeps = 16L * (nx + ny + nz) + 256;
-  long sweeps = 0;
+  const int pass_blocks = 16 * sms;
+  const int batch = 32;
+  long launched = 0;
   while (ok) {
-    ok = cuda_ok(cudaMemsetAsync(changed, 0, sizeof(int), st), R);
-    for (int q = 0; ok && q < batch; q++, sweeps++) {
+    for (int q = 0; q < batch; q++, launched++) {
       if (order == 1)
-        k_fmm_sweep<1><<<grid2, blk, 0, st>>>(dd, etime, status, nx, ny, nz, i2[0], i2[1], i2[2],
-                                              (int)(sweeps & 1) ^ 1, changed);
+        k_fmm_pass<1><<<pass_blocks, 128, 0, st>>>(dd, tm, status, nx, ny, nz, i2[0], i2[1],
+                                                   i2[2], L, ctrl);
       else
-        k_fmm_sweep<2><<<grid2, blk, 0, st>>>(dd, etime, status, nx, ny, nz, i2[0], i2[1], i2[2],
-                                              (int)(sweeps & 1) ^ 1, changed);
-      ++launch_counter();
+        k_fmm_pass<2><<<pass_blocks, 128, 0, st>>>(dd, tm, status, nx, ny, nz, i2[0], i2[1],
+                                                   i2[2], L, ctrl);
+      k_fmm_control<<<1, 32, 0, st>>>(delta, ctrl);
+      k_fmm_filter<<<pass_blocks, 256, 0, st>>>(dd, tm, n, L, ctrl);
+      launch_counter() += 3;
     }
-    ok = ok && cuda_ok(cudaGetLastError(), R) &&
-         cuda_ok(cudaMemcpyAsync(&h_changed, changed, sizeof(int), cudaMemcpyDeviceToHost,
-                                 st), R) &&
+    ok = cuda_ok(cudaGetLastError(), R) &&
+         cuda_ok(cudaMemcpyAsync(&h_ctrl, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st), R) &&
          cuda_ok(cudaStreamSynchronize(st), R);
-    if (!ok || !h_changed) break;
-    if (sweeps >= max_sweeps) {
-      // the fixed point is reached well within this bound (about one sweep
-      // per cell of the longest upwind path); it guards against inputs
-      // without one
-      set_error(LSMGPU_ERR_INVALID_VALUE,
-                std::string(R) + ": no convergence (NaN in phi or dx?)");
+    if (!ok || h_ctrl.done) break;
+    if (launched >= max_passes) {
+      set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": no convergence (NaN in phi?)");
       ok = false;
     }
   }
   if (ok) {
-    const long nb = (n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096;
-    k_fmm_unreached<<<(int)nb, 256, 0, st>>>(dd, status, n);
+    k_fmm_unreached<<<elem_blocks, 256, 0, st>>>(dd, status, n);
     ++launch_counter();
     ok = cuda_ok(cudaGetLastError(), R);
   }
-  if (status) cudaFreeAsync(status, st);
-  if (etime) cudaFreeAsync(etime, st);
-  if (changed) cudaFreeAsync(changed, st);
-  if (sweeps_out) *sweeps_out = (int)sweeps;
+  for (void* q : {(void*)status, (void*)tm, (void*)L.active, (void*)L.pending,
+                  (void*)L.stamp, (void*)L.pend_stamp, (void*)ctrl})
+    if (q) cudaFreeAsync(q, st);
+  if (passes_out) *passes_out = h_ctrl.pass;
   if (!ok) return lsmgpu_peek_last_error() ? lsmgpu_peek_last_error() : LSMGPU_ERR_CUDA;
-  return s.finish(R) ? LSMGPU_SUCCESS : LSMGPU_ERR_CUDA;
+  return stg.finish(R) ? LSMGPU_SUCCESS : LSMGPU_ERR_CUDA;
 }
 
 }  // namespace
@@ -425,8 +633,8 @@ int computeDistanceFunction3d(double* distance_function, double* phi, double* ma
 
 int lsmgpu_distance_function3d(double* distance_function, const double* phi,
                                const double* mask, int order, const int* grid_dims,
-                               const double* dx, int* sweeps) {
-  return distance3d(distance_function, phi, mask, order, grid_dims, dx, sweeps,
+                               const double* dx, int* passes) {
+  return distance3d(distance_function, phi, mask, order, grid_dims, dx, passes,
                     "lsmgpu_distance_function3d");
 }
 
