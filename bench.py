@@ -16,7 +16,9 @@ fast arithmetic), the FP32 form beside it (with its error against the FP64
 run), e2e (the same steps through the C ABI with the level set and speed on
 pinned host memory, copied in and out every step), the roofline of the
 dominant kernel, the CFL-dt kernel count and the reference's CPU toolbox timed
-on this host.  Under torchrun every rank runs a replica on its own GPU
+on this host.  Beside it: the batched, adjoint, deformation and per-routine
+toolbox legs, and the signed-distance leg (fast marching values, 128^3 and
+256^3, against the CPU oracle of the reference's heap march).  Under torchrun every rank runs a replica on its own GPU
 (weak scaling, no data-path collective).
 
 ``--impl reference`` times the reference's own toolbox routines (translated
@@ -305,6 +307,10 @@ def run_ours(args, world, rank, local, pg):
     if not args.no_toolbox:
         toolbox_res = run_toolbox(peak)
 
+    distance_res = None
+    if not args.no_distance:
+        distance_res = run_distance()
+
     deformation_res = None
     if not args.no_deformation:
         deformation_res = run_config3(lib, pg, world,
@@ -326,7 +332,7 @@ def run_ours(args, world, rank, local, pg):
                    "l2": "inputs larger than L2 (144 MB per field, 6 fields live)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "fp32": fp32, "batched": batched_res, "adjoint": adjoint_res,
-        "deformation": deformation_res, "toolbox": toolbox_res,
+        "deformation": deformation_res, "toolbox": toolbox_res, "distance": distance_res,
         "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk,
     }
@@ -476,6 +482,69 @@ def run_toolbox(peak, n=256, reps=10):
                     "gb_s": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 3)}
     return {"grid": "256^3 fill box, 262^3 ghost boxes, FP64, device arrays, mean of "
                     "%d calls" % reps, "routines": res}
+
+
+def run_distance(n=256, n_cpu=128, reps=3):
+    """The signed distance function (computeDistanceFunction3d; fast
+    marching values) on workloads.distance_case at n^3 and n_cpu^3, orders 1
+    and 2: device arrays timed with CUDA events (mean of ``reps`` solves),
+    the drop-in entry point on host arrays (copies included), and at n_cpu^3
+    the CPU oracle (the reference's heap march restated in C, one core) with
+    a bit-for-bit comparison."""
+    import oracle
+    from lsmlib_b200 import gpu, workloads
+    lib = gpu.load()
+    fn = lib.computeDistanceFunction3d
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    timer = gpu.Timer()
+    out = {"workload": "config-2 union of 6 spheres on [-1,1]^3, scaled by "
+                       "1.2 + 0.5 sin(3 pi x) sin(2 pi y) cos(pi z) (same zero set)",
+           "unit": "grid points/s", "sizes": {}}
+    for size in (n_cpu, n):
+        phi, dx = workloads.distance_case(size)
+        pts = size ** 3
+        d_phi = gpu.DeviceArray.from_host(phi)
+        d_out = gpu.DeviceArray(phi.shape)
+        dims = (ctypes.c_int * 3)(size, size, size)
+        h = (ctypes.c_double * 3)(*dx)
+        hd = np.ascontiguousarray(np.array(dx))
+        hdims = np.array([size] * 3, dtype=np.intc)
+        entry = {}
+        for order in (1, 2):
+            passes = ctypes.c_int(0)
+            gpu.check_rc(lib.lsmgpu_distance_function3d(d_out.ptr, d_phi.ptr, None, order, dims,
+                                                        h, ctypes.byref(passes)), "distance")
+            timer.start()
+            for _ in range(reps):
+                lib.lsmgpu_distance_function3d(d_out.ptr, d_phi.ptr, None, order, dims, h, None)
+            timer.stop()
+            ms = timer.ms() / reps
+            host_out = np.zeros_like(phi)
+            t_e2e = float("inf")
+            for _ in range(2):      # best of two: the first may grow the memory pool
+                t0 = time.perf_counter()
+                rc = fn(host_out.ctypes.data, phi.ctypes.data, None, order, hdims.ctypes.data,
+                        hd.ctypes.data)
+                t_e2e = min(t_e2e, time.perf_counter() - t0)
+            r = {"ms": round(ms, 2), "value": pts / (ms / 1e3), "passes": passes.value,
+                 "e2e": {"ms": round(1e3 * t_e2e, 2), "value": pts / t_e2e, "rc": rc,
+                         "path": "computeDistanceFunction3d on host arrays (copies "
+                                 "included), best of 2 calls"}}
+            if size == n_cpu:
+                t0 = time.perf_counter()
+                want = oracle.oracle_fmm()(phi.T, order, dx)
+                t_cpu = time.perf_counter() - t0
+                got = d_out.download()
+                r["cpu_oracle"] = {"ms": round(1e3 * t_cpu, 1), "value": pts / t_cpu,
+                                   "cores": 1, "kind": "port"}
+                r["bitwise_vs_oracle"] = bool(np.array_equal(got.T.view(np.uint64),
+                                                              want.view(np.uint64)))
+            entry["order%d" % order] = r
+        out["sizes"]["%d^3" % size] = entry
+        d_phi.free()
+        d_out.free()
+    return out
 
 
 def deformation_run(ws, d_phi, fb, cfg, timer):
@@ -764,6 +833,8 @@ def main():
                     help="skip the batched uneven-grid leg (config 4)")
     ap.add_argument("--no-toolbox", action="store_true",
                     help="skip the per-routine drop-in timings")
+    ap.add_argument("--no-distance", action="store_true",
+                    help="skip the signed-distance (fast marching) leg")
     ap.add_argument("--no-deformation", action="store_true",
                     help="skip the deformation leg (config 3)")
     ap.add_argument("--config3-full", action="store_true",

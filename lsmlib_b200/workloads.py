@@ -12,6 +12,10 @@ recorded in each description.
   CFL 0.5, 200 steps, reinitialization every 10 steps (20 pseudo-steps).
 * ``config3`` -- 512^3 on [0,1]^3, sphere r = 0.15 at (0.35,0.35,0.35),
   LeVeque deformation field with period 3, run to t = 3.
+* ``distance_case`` -- n^3 grid points on [-1,1]^3 (no ghost cells), the
+  config-2 union of spheres scaled by 1.2 + 0.5 sin(3 pi x) sin(2 pi y)
+  cos(pi z): the same zero level set, no longer a distance function; the
+  input of the signed-distance (fast marching) benchmark.
 """
 import numpy as np
 
@@ -62,6 +66,18 @@ def config2(n=256, seed=SEED, dtype=np.float64):
     return {"n": (n, n, n), "dx": dx, "phi": phi, "F": F, "cfl": 0.5,
             "steps": 200, "reinit_interval": 10, "reinit_iters": 20,
             "use_phi0": 0, "seed": seed, "x_lo": (-1.0, -1.0, -1.0)}
+
+
+def distance_case(n=256, seed=SEED):
+    """(phi, dx): phi an (n, n, n) Fortran-ordered array (x fastest) of grid
+    points x_i = -1 + i dx, dx = 2/(n-1); dx in x, y, z order."""
+    a = np.linspace(-1.0, 1.0, n)
+    dx = [2.0 / (n - 1)] * 3
+    centres, radii = config2_spheres(seed)
+    phi = union_of_spheres([a, a, a], centres, radii)
+    scale = (1.2 + 0.5 * np.sin(3 * np.pi * a)[:, None, None] *
+             np.sin(2 * np.pi * a)[None, :, None] * np.cos(np.pi * a)[None, None, :])
+    return np.asfortranarray(phi * scale), dx
 
 
 def config3(n=512, dtype=np.float64):
