@@ -817,6 +817,23 @@ def profile_adjoint():
     p.close()
 
 
+def profile_distance(n=128):
+    """The distance function on workloads.distance_case(n), orders 1 and 2,
+    device arrays (for ncu captures of the band-solver pass kernel)."""
+    from lsmlib_b200 import gpu, workloads
+    lib = gpu.load()
+    phi, dx = workloads.distance_case(n)
+    d_phi = gpu.DeviceArray.from_host(phi)
+    d_out = gpu.DeviceArray(phi.shape)
+    dims = (ctypes.c_int * 3)(n, n, n)
+    h = (ctypes.c_double * 3)(*dx)
+    for order in (1, 2):
+        gpu.check_rc(lib.lsmgpu_distance_function3d(d_out.ptr, d_phi.ptr, None, order, dims, h,
+                                                    None), "distance")
+    d_phi.free()
+    d_out.free()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -843,6 +860,9 @@ def main():
     ap.add_argument("--profile-adjoint", action="store_true",
                     help="only run the config-5 forward and reverse sweep twice "
                          "(for ncu captures) and exit")
+    ap.add_argument("--profile-distance", action="store_true",
+                    help="only run the 128^3 distance function at orders 1 and 2 "
+                         "(for ncu captures) and exit")
     ap.add_argument("--profile", action="store_true",
                     help="only launch the two fused stage kernels twice each "
                          "(for ncu captures) and exit")
@@ -857,6 +877,9 @@ def main():
         return
     if args.profile_adjoint:
         profile_adjoint()
+        return
+    if args.profile_distance:
+        profile_distance()
         return
     if args.impl == "reference":
         line = run_reference(args, world, rank)
