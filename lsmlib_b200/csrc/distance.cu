@@ -578,21 +578,47 @@ int distance3d(double* distance, const double* phi, const double* mask, int orde
     i2[q] = 1 / dx[q];
     i2[q] *= i2[q];
   }
-  const int pass_blocks = 16 * sms;
+  // a pass touches only the band, so a few blocks per SM cover it; the
+  // grid-stride loops take any count
+  const int pass_blocks = 4 * sms, filter_blocks = 2 * sms;
   const int batch = 32;
+  auto launch_batch = [&](cudaStream_t s) {
+    for (int q = 0; q < batch; q++) {
+      if (order == 1)
+        k_fmm_pass<1><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0], i2[1],
+                                                  i2[2], L, ctrl);
+      else
+        k_fmm_pass<2><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0], i2[1],
+                                                  i2[2], L, ctrl);
+      k_fmm_control<<<1, 32, 0, s>>>(delta, ctrl);
+      k_fmm_filter<<<filter_blocks, 256, 0, s>>>(dd, tm, n, L, ctrl);
+    }
+  };
+  // The kernels read the pass number and lists from ``ctrl``, so every batch
+  // is the same sequence of launches: capture it once as a CUDA graph and
+  // replay it (direct launches if the graph cannot be built).
+  cudaGraphExec_t gexec = nullptr;
+  if (ok) {
+    cudaStream_t cs = nullptr;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess) {
+      if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        launch_batch(cs);
+        if (cudaStreamEndCapture(cs, &graph) == cudaSuccess && graph) {
+          if (cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess) gexec = nullptr;
+          cudaGraphDestroy(graph);
+        }
+      }
+      cudaStreamDestroy(cs);
+    }
+    cudaGetLastError();   // a failed capture leaves nothing behind but the error
+  }
   long launched = 0;
   while (ok) {
-    for (int q = 0; q < batch; q++, launched++) {
-      if (order == 1)
-        k_fmm_pass<1><<<pass_blocks, 128, 0, st>>>(dd, tm, status, nx, ny, nz, i2[0], i2[1],
-                                                   i2[2], L, ctrl);
-      else
-        k_fmm_pass<2><<<pass_blocks, 128, 0, st>>>(dd, tm, status, nx, ny, nz, i2[0], i2[1],
-                                                   i2[2], L, ctrl);
-      k_fmm_control<<<1, 32, 0, st>>>(delta, ctrl);
-      k_fmm_filter<<<pass_blocks, 256, 0, st>>>(dd, tm, n, L, ctrl);
-      launch_counter() += 3;
-    }
+    if (gexec) ok = cuda_ok(cudaGraphLaunch(gexec, st), R);
+    else launch_batch(st);
+    launched += batch;
+    launch_counter() += 3 * batch;
     ok = cuda_ok(cudaGetLastError(), R) &&
          cuda_ok(cudaMemcpyAsync(&h_ctrl, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st), R) &&
          cuda_ok(cudaStreamSynchronize(st), R);
@@ -607,6 +633,7 @@ int distance3d(double* distance, const double* phi, const double* mask, int orde
     ++launch_counter();
     ok = cuda_ok(cudaGetLastError(), R);
   }
+  if (gexec) cudaGraphExecDestroy(gexec);
   for (void* q : {(void*)status, (void*)tm, (void*)L.active, (void*)L.pending,
                   (void*)L.stamp, (void*)L.pend_stamp, (void*)ctrl})
     if (q) cudaFreeAsync(q, st);
