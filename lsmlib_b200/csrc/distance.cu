@@ -133,18 +133,12 @@ __global__ void k_fmm_front(double* d, Time3* tm, unsigned char* st, const doubl
   }
 }
 
-// a neighbour that has a value (front or reached, inside the domain)
-__device__ __forceinline__ bool known(const double* d, const unsigned char* st, long o) {
-  return st[o] != kOutside && fabs(d[o]) <= DBL_MAX;
-}
-
 // The neighbours of one point, by slot 2*axis + (plus side): the immediate
 // neighbour (value v1, time t1) and, at second order, the next one in that
-// direction (value v2; its time is read when needed).
+// direction (v2, t2).
 struct Stencil {
   double v1[6], v2[6];
-  Time3 t1[6];
-  long o2[6];
+  Time3 t1[6], t2[6];
   unsigned char has1, front1, has2, front2;  // bit per slot
 };
 
@@ -158,7 +152,7 @@ struct Stencil {
 // comes before every free point) -- and its |d| is not above the
 // neighbour's.  Returns the discriminant B^2 - 4AC.
 template <int ORDER>
-__device__ __forceinline__ double fmm_coeffs(const Stencil& n, const Time3* tm, int incl,
+__device__ __forceinline__ double fmm_coeffs(const Stencil& n, int incl,
                                              const Time3& trig, bool has_trigger,
                                              const double i2[3], double& A, double& B) {
   double C = 0;
@@ -177,7 +171,7 @@ __device__ __forceinline__ double fmm_coeffs(const Stencil& n, const Time3* tm, 
       u2 = DBL_MAX;
       sw = 0;
       if (ORDER == 2 && (n.has2 & (1 << q)) && fabs(n.v2[q]) <= fabs(u1) &&
-          ((n.front2 & (1 << q)) || (has_trigger && tless(tm[n.o2[q]], trig)))) {
+          ((n.front2 & (1 << q)) || (has_trigger && tless(n.t2[q], trig)))) {
         u2 = n.v2[q];
         sw = 1;
       }
@@ -244,32 +238,50 @@ __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
                                           const unsigned char* st, long o, const int c[3],
                                           const int n[3], const long s[3], const double i2[3],
                                           double& val, Time3& tv) {
+  // every load first, at in-range addresses (the point itself stands in
+  // for a neighbour off the grid), so that they are in flight together
   Stencil nb;
-  nb.has1 = nb.front1 = nb.has2 = nb.front2 = 0;
+  unsigned char s1[6], s2[6];
+  bool in1[6], in2[6];
 #pragma unroll
   for (int q = 0; q < 6; q++) {
     const int dir = q >> 1;
     const int sg = (q & 1) ? 1 : -1;
-    nb.v1[q] = nb.v2[q] = DBL_MAX;
-    nb.t1[q] = Time3{INFINITY, INFINITY, INFINITY};
-    nb.o2[q] = 0;
-    const int c1 = c[dir] + sg;
-    if (c1 < 0 || c1 >= n[dir]) continue;
-    const long o1 = o + sg * s[dir];
-    if (!known(d, st, o1)) continue;
+    in1[q] = c[dir] + sg >= 0 && c[dir] + sg < n[dir];
+    const long o1 = in1[q] ? o + sg * s[dir] : o;
+    s1[q] = st[o1];
     nb.v1[q] = d[o1];
-    nb.has1 |= 1 << q;
-    if (st[o1] == kFront) nb.front1 |= 1 << q;
-    else nb.t1[q] = tm[o1];
+    nb.t1[q] = tm[o1];
     if (ORDER == 2) {
-      const int c2 = c1 + sg;
-      if (c2 < 0 || c2 >= n[dir]) continue;
-      const long o2 = o1 + sg * s[dir];
-      if (!known(d, st, o2)) continue;
+      in2[q] = in1[q] && c[dir] + 2 * sg >= 0 && c[dir] + 2 * sg < n[dir];
+      const long o2 = in2[q] ? o + 2 * sg * s[dir] : o;
+      s2[q] = st[o2];
       nb.v2[q] = d[o2];
-      nb.o2[q] = o2;
+      nb.t2[q] = tm[o2];
+    }
+  }
+  nb.has1 = nb.front1 = nb.has2 = nb.front2 = 0;
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    const bool k1 = in1[q] && s1[q] != kOutside && fabs(nb.v1[q]) <= DBL_MAX;
+    if (!k1) {
+      nb.v1[q] = DBL_MAX;
+      nb.t1[q] = Time3{INFINITY, INFINITY, INFINITY};
+      continue;
+    }
+    nb.has1 |= 1 << q;
+    if (s1[q] == kFront) {
+      nb.front1 |= 1 << q;
+      nb.t1[q] = Time3{INFINITY, INFINITY, INFINITY};
+    }
+    if (ORDER == 2) {
+      const bool k2 = in2[q] && s2[q] != kOutside && fabs(nb.v2[q]) <= DBL_MAX;
+      if (!k2) {
+        nb.v2[q] = DBL_MAX;
+        continue;
+      }
       nb.has2 |= 1 << q;
-      if (st[o2] == kFront) nb.front2 |= 1 << q;
+      if (s2[q] == kFront) nb.front2 |= 1 << q;
     }
   }
   if (!nb.has1) return false;
@@ -282,7 +294,7 @@ __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
     double cur = -1.0;
     if (have) {
       double A, B;
-      const double disc = fmm_coeffs<ORDER>(nb, tm, incl, trig, false, i2, A, B);
+      const double disc = fmm_coeffs<ORDER>(nb, incl, trig, false, i2, A, B);
       if (disc >= 0) cur = fmm_root(A, B, disc);
     }
     for (int rem = free1; rem;) {
@@ -304,7 +316,7 @@ __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
       trig = bt;
       trig_free = true;
       double A, B;
-      const double disc = fmm_coeffs<ORDER>(nb, tm, incl, trig, true, i2, A, B);
+      const double disc = fmm_coeffs<ORDER>(nb, incl, trig, true, i2, A, B);
       if (disc >= 0) cur = fmm_root(A, B, disc);
       have = true;
     }
@@ -337,7 +349,7 @@ struct Ctrl {
   int done;
   int advance;               // the last control step moved the threshold
   int filter_count;          // length of the pending list being filtered
-  int pad;
+  int peak;                  // largest queue of the current threshold step
   double T;                  // threshold on the first level of the time
   unsigned long long minrej; // bits of the smallest candidate queued since
                              // the last advance (times are >= 0)
@@ -379,7 +391,7 @@ __global__ void k_fmm_seed(const unsigned char* st, int nx, int ny, int nz, List
 
 // One pass over the active list (count[pass & 1]).
 template <int ORDER>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, ORDER == 1 ? 4 : 3)
 k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz,
            double i2x, double i2y, double i2z, Lists L, Ctrl* ctrl) {
   const int it = ctrl->pass;
@@ -432,19 +444,27 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
   if (minrej != ~0ULL) atomicMin(&ctrl->minrej, minrej);
 }
 
-// Between passes (one thread): with points queued, the next pass runs at the
-// same threshold; else the threshold moves to max(T + delta, smallest
-// waiting candidate) and the pending list is filtered (next kernel); with
-// nothing waiting either, the solve is done.
+// Between passes (one thread).  Each threshold step has a burst of large
+// passes and then a long tail of small ones as the last revisions settle;
+// the threshold need not wait for that tail (the fixed point does not
+// depend on when T moves, only the amount of revision does).  So once the
+// queued points fall to 1/kTailFraction of the step's largest pass, the
+// threshold moves to max(T + delta, smallest waiting candidate) and the
+// pending list is filtered (next kernel) into the queue beside them.  With
+// nothing queued and nothing waiting, the solve is done.
+constexpr int kTailFraction = 8;
+
 __global__ void k_fmm_control(double delta, Ctrl* ctrl) {
   if (threadIdx.x != 0 || ctrl->done) return;
   const int par = ctrl->pass & 1;
+  const int queued = ctrl->count[par ^ 1];
   ctrl->advance = 0;
-  if (ctrl->count[par ^ 1] == 0) {
+  if (queued > ctrl->peak) ctrl->peak = queued;
+  if ((long)queued * kTailFraction <= ctrl->peak) {
     const int ep = ctrl->epoch;
     const int np = ctrl->pend_count[ep & 1];
     if (np == 0) {
-      ctrl->done = 1;
+      if (queued == 0) ctrl->done = 1;
     } else {
       const unsigned long long m = ctrl->minrej < ctrl->minkeep ? ctrl->minrej : ctrl->minkeep;
       const double lo = __longlong_as_double((long long)m);
@@ -454,6 +474,7 @@ __global__ void k_fmm_control(double delta, Ctrl* ctrl) {
       ctrl->filter_count = np;
       ctrl->pend_count[(ep & 1) ^ 1] = 0;
       ctrl->epoch = ep + 1;
+      ctrl->peak = queued;
       ctrl->minrej = __double_as_longlong(INFINITY);
       ctrl->minkeep = __double_as_longlong(INFINITY);
     }
