@@ -407,6 +407,22 @@ void lsm3dcomputereinitializationeqnrhssubcellfixorder1_(
 int computeDistanceFunction3d(LSMLIB_REAL *distance_function, LSMLIB_REAL *phi,
                               LSMLIB_REAL *mask, int spatial_discretization_order,
                               int *grid_dims, LSMLIB_REAL *dx);
+/* lsm_fast_marching_method.h:331-341: the distance function and, with it,
+ * num_extension_fields fields extended off the zero level set of phi
+ * (grad ext . grad distance = 0): extension_fields[k] takes the values of
+ * source_fields[k] at the interface (linearly interpolated to the crossing,
+ * or taken from one side where extension_mask < 0; extension_mask may be
+ * NULL) and carries them outward with the march, as the reference does
+ * (first-order weights at both orders).  Points no front reaches hold -1,
+ * points with mask < 0 LSMLIB_REAL_MAX, in every field.  The pointer arrays
+ * are host arrays; each field may be a host or a device array.  Same return
+ * codes as computeDistanceFunction3d. */
+int computeExtensionFields3d(LSMLIB_REAL *distance_function,
+                             LSMLIB_REAL **extension_fields, LSMLIB_REAL *phi,
+                             LSMLIB_REAL *mask, LSMLIB_REAL **source_fields,
+                             LSMLIB_REAL *extension_mask, int num_extension_fields,
+                             int spatial_discretization_order, int *grid_dims,
+                             LSMLIB_REAL *dx);
 
 /* ======================================================================== */
 /* Part 2 -- extension API                                                   */
@@ -639,6 +655,14 @@ int lsmgpu_distance_function3d(double *distance_function, const double *phi,
                                const double *mask, int order,
                                const int grid_dims[3], const double dx[3],
                                int *passes);
+/* computeExtensionFields3d with the lsmgpu error codes and the number of
+ * passes (the last solve's; fields are solved in groups of 8). */
+int lsmgpu_extension_fields3d(double *distance_function, double **extension_fields,
+                              const double *phi, const double *mask,
+                              double *const *source_fields,
+                              const double *extension_mask, int num_extension_fields,
+                              int order, const int grid_dims[3], const double dx[3],
+                              int *passes);
 
 /* ---- an entry point that allocates no memory --------------------------------
  * No counterpart in the reference.  For callers that must not allocate device

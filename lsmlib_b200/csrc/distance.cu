@@ -73,11 +73,26 @@ __device__ __forceinline__ Time3 tafter(const Time3& x, double a, bool has_trigg
   return x;
 }
 
+// Extension fields carried by one solve (computeExtensionFields3d): output
+// fields, their source fields, the optional extension mask.
+constexpr int kMaxFields = 8;
+struct ExtSet {
+  double* ext[kMaxFields];
+  const double* src[kMaxFields];
+  const double* emask;
+  int nf;
+};
+
 // FMM_initializeFront_FieldExtension3d_Order1 (lsm_FMM_field_extension.c:
-// 397-668) for one point; the neighbours' phi is read whatever their mask
+// 397-668) for one point; the neighbours' phi is read whatever their mask.
+// Extension fields: every value starts at -1 (LSMLIB_REAL_MAX outside the
+// mask); on the interface the source value; next to it the average over
+// the axes of the source interpolated linearly to the nearer crossing (or
+// taken from one side where the extension mask is < 0), weights
+// 1/d_axis^2 (:524-660).
 __global__ void k_fmm_front(double* d, Time3* tm, unsigned char* st, const double* phi,
                             const double* mask, int nx, int ny, int nz, double dx,
-                            double dy, double dz) {
+                            double dy, double dz, ExtSet X) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= nx || j >= ny) return;
@@ -89,24 +104,31 @@ __global__ void k_fmm_front(double* d, Time3* tm, unsigned char* st, const doubl
     if (mask && mask[o] < 0) {
       st[o] = kOutside;
       d[o] = DBL_MAX;
+      for (int k = 0; k < X.nf; k++) X.ext[k][o] = DBL_MAX;
       continue;
     }
     const double pc = phi[o];
     if (fabs(pc) < kZeroTol) {           // on the interface
       st[o] = kFront;
       d[o] = pc > 0 ? kZeroTol : -kZeroTol;
+      for (int k = 0; k < X.nf; k++) X.ext[k][o] = X.src[k][o];
       continue;
     }
     const int c[3] = {i, j, k};
     const long s[3] = {1L, (long)nx, (long)nx * ny};
     bool borders = false;
     double sum = 0;
+    double fsum[kMaxFields];
+#pragma unroll
+    for (int f = 0; f < kMaxFields; f++) fsum[f] = 0;
     for (int dir = 0; dir < 3; dir++) {
       double dist_plus = DBL_MAX, dist_minus = DBL_MAX;
+      double frac_plus = 0, frac_minus = 0;
       if (c[dir] - 1 >= 0) {
         const double pm = phi[o - s[dir]];
         if (pm * pc <= 0) {
           dist_minus = pc / (pc - pm);
+          frac_minus = dist_minus;
           dist_minus *= h[dir];
         }
       }
@@ -114,21 +136,40 @@ __global__ void k_fmm_front(double* d, Time3* tm, unsigned char* st, const doubl
         const double pp = phi[o + s[dir]];
         if (pp * pc <= 0) {
           dist_plus = pc / (pc - pp);
+          frac_plus = dist_plus;
           dist_plus *= h[dir];
         }
       }
       if (dist_plus < DBL_MAX || dist_minus < DBL_MAX) {
         borders = true;
-        const double dd = dist_plus < dist_minus ? dist_plus : dist_minus;
-        sum += 1 / dd / dd;
+        const bool use_plus = dist_plus < dist_minus;
+        const double dd = use_plus ? dist_plus : dist_minus;
+        const double w = 1 / dd / dd;
+        sum += w;
+        const long on = use_plus ? o + s[dir] : o - s[dir];
+        const double frac = use_plus ? frac_plus : frac_minus;
+#pragma unroll
+        for (int f = 0; f < kMaxFields; f++) {
+          if (f >= X.nf) break;
+          const double cur = X.src[f][o];
+          double v;
+          if (X.emask && X.emask[o] < 0) v = X.src[f][on];
+          else if (X.emask && X.emask[on] < 0) v = cur;
+          else v = cur + frac * (X.src[f][on] - cur);
+          fsum[f] += v * w;
+        }
       }
     }
     if (borders) {
       st[o] = kFront;
       d[o] = pc > 0 ? sqrt(1.0 / sum) : -sqrt(1.0 / sum);
+#pragma unroll
+      for (int f = 0; f < kMaxFields; f++)
+        if (f < X.nf) X.ext[f][o] = fsum[f] / sum;
     } else {
       st[o] = kFree;
       d[o] = pc > 0 ? INFINITY : -INFINITY;
+      for (int f = 0; f < X.nf; f++) X.ext[f][o] = -1.0;
     }
   }
 }
@@ -237,10 +278,10 @@ template <int ORDER>
 __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
                                           const unsigned char* st, long o, const int c[3],
                                           const int n[3], const long s[3], const double i2[3],
-                                          double& val, Time3& tv) {
+                                          Stencil& nb, double& val, Time3& tv, int& incl_out,
+                                          Time3& trig_out, bool& trig_free_out) {
   // every load first, at in-range addresses (the point itself stands in
   // for a neighbour off the grid), so that they are in flight together
-  Stencil nb;
   unsigned char s1[6], s2[6];
   bool in1[6], in2[6];
 #pragma unroll
@@ -333,10 +374,71 @@ __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
     if (!bad) {
       val = cur;
       tv = t;
+      incl_out = incl;
+      trig_out = trig;
+      trig_free_out = trig_free;
       return true;
     }
     cap = badt;
   }
+}
+
+// The extension fields of the point's last trial update: over the axes in
+// the update, the weighted average of the upwind neighbour's field with
+// weights (dist - phi_upwind)/dx^2, or (1.5 dist - 2 phi_upwind1 +
+// 0.5 phi_upwind2)/dx^2 where the second-order stencil is used
+// (lsm_FMM_field_extension.c:1135-1168, :1400-1460); ``val`` is the
+// update's distance (the previous one where the discriminant was
+// negative).  Each field whose value changes is stored; returns whether any
+// did.
+template <int ORDER>
+__device__ __forceinline__ bool fmm_ext(const Stencil& n, int incl, const Time3& trig,
+                                        bool has_trigger, double val, const double i2[3],
+                                        const ExtSet& X, long o, const long s[3]) {
+  double g[3];
+  long a[3];
+  bool used[3];
+#pragma unroll
+  for (int dir = 0; dir < 3; dir++) {
+    double u1 = DBL_MAX, u2 = DBL_MAX;
+    int sw = 0, side_used = -1;
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+      const int q = 2 * dir + side;
+      if (!(incl & (1 << q))) continue;
+      if (side == 1 && !(fabs(n.v1[q]) < fabs(u1))) continue;
+      u1 = n.v1[q];
+      u2 = DBL_MAX;
+      sw = 0;
+      side_used = side;
+      if (ORDER == 2 && (n.has2 & (1 << q)) && fabs(n.v2[q]) <= fabs(u1) &&
+          ((n.front2 & (1 << q)) || (has_trigger && tless(n.t2[q], trig)))) {
+        u2 = n.v2[q];
+        sw = 1;
+      }
+    }
+    used[dir] = side_used >= 0;
+    a[dir] = side_used == 1 ? o + s[dir] : o - s[dir];
+    g[dir] = (ORDER == 2 && sw == 1) ? 1.5 * val - 2.0 * u1 + 0.5 * u2 : val - u1;
+  }
+  bool changed = false;
+#pragma unroll
+  for (int f = 0; f < kMaxFields; f++) {
+    if (f >= X.nf) break;
+    double num = 0, den = 0;
+#pragma unroll
+    for (int dir = 0; dir < 3; dir++) {
+      if (!used[dir]) continue;
+      num += i2[dir] * g[dir] * X.ext[f][a[dir]];
+      den += i2[dir] * g[dir];
+    }
+    const double v = num / den;
+    if (__double_as_longlong(v) != __double_as_longlong(X.ext[f][o])) {
+      X.ext[f][o] = v;
+      changed = true;
+    }
+  }
+  return changed;
 }
 
 // Device state of the solve, read and advanced by the kernels so that the
@@ -393,7 +495,7 @@ __global__ void k_fmm_seed(const unsigned char* st, int nx, int ny, int nz, List
 template <int ORDER>
 __global__ void __launch_bounds__(128, ORDER == 1 ? 4 : 3)
 k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz,
-           double i2x, double i2y, double i2z, Lists L, Ctrl* ctrl) {
+           double i2x, double i2y, double i2z, Lists L, Ctrl* ctrl, ExtSet X) {
   const int it = ctrl->pass;
   const int par = it & 1;
   const int count = ctrl->count[par];
@@ -413,18 +515,25 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
     const long o = cur[w];
     if (st[o] != kFree) continue;
     const int c[3] = {(int)(o % nx), (int)((o / nx) % ny), (int)(o / s[2])};
+    Stencil nb;
     double val;
-    Time3 tv;
-    if (!fmm_point<ORDER>(d, tm, st, o, c, nn, s, i2, val, tv)) continue;
+    Time3 tv, trig;
+    int incl;
+    bool trig_free;
+    if (!fmm_point<ORDER>(d, tm, st, o, c, nn, s, i2, nb, val, tv, incl, trig, trig_free))
+      continue;
     const double old = d[o];
+    bool ext_changed = false;
     if (!(tv.a <= T)) {
       // accepted after the threshold: a candidate only, waiting for T
       val = copysign(INFINITY, old);
       push_once(o, ep + 1, L.pend_stamp, pend, pend_count);
       const unsigned long long bits = __double_as_longlong(tv.a);
       minrej = bits < minrej ? bits : minrej;
+    } else if (X.nf) {
+      ext_changed = fmm_ext<ORDER>(nb, incl, trig, trig_free, val, i2, X, o, s);
     }
-    if (val == old && tequal(tv, tm[o])) continue;
+    if (val == old && tequal(tv, tm[o]) && !ext_changed) continue;
     d[o] = val;
     tm[o] = tv;
     if (!(fabs(old) <= DBL_MAX) && !(fabs(val) <= DBL_MAX)) continue;   // invisible
@@ -510,53 +619,30 @@ __global__ void k_fmm_filter(const double* d, const Time3* tm, long n, Lists L, 
   if (mk != ~0ULL) atomicMin(&ctrl->minkeep, mk);
 }
 
-// free points no front reached: the reference's default value -1
-__global__ void k_fmm_unreached(double* d, const unsigned char* st, long n) {
+// free points no front reached: the reference's default value -1 (distance
+// and extension fields)
+__global__ void k_fmm_unreached(double* d, const unsigned char* st, long n, ExtSet X) {
   for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n;
        o += (long)gridDim.x * blockDim.x)
-    if (st[o] == kFree && !(fabs(d[o]) <= DBL_MAX)) d[o] = -1.0;
+    if (st[o] == kFree && !(fabs(d[o]) <= DBL_MAX)) {
+      d[o] = -1.0;
+      for (int f = 0; f < X.nf; f++) X.ext[f][o] = -1.0;
+    }
 }
 
-int distance3d(double* distance, const double* phi, const double* mask, int order,
-               const int* grid_dims, const double* dx, int* passes_out, const char* R) {
-  clear_error();
-  if (!distance || !phi || !grid_dims || !dx) {
-    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null argument");
-    return LSMGPU_ERR_NULL_POINTER;
-  }
-  if (order != 1 && order != 2) {
-    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": order is 1 or 2");
-    return LSMGPU_ERR_INVALID_VALUE;
-  }
+// One solve on device arrays: the distance function and up to kMaxFields
+// extension fields (X.nf may be 0).
+bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& X, int order,
+                  const int* grid_dims, const double* dx, int* passes_out, const char* R,
+                  cudaStream_t st) {
   const int nx = grid_dims[0], ny = grid_dims[1], nz = grid_dims[2];
-  if (nx < 1 || ny < 1 || nz < 1) {
-    set_error(LSMGPU_ERR_INVALID_BOX, std::string(R) + ": empty grid");
-    return LSMGPU_ERR_INVALID_BOX;
-  }
-  if (!(dx[0] > 0) || !(dx[1] > 0) || !(dx[2] > 0) || !(dx[0] < INFINITY) ||
-      !(dx[1] < INFINITY) || !(dx[2] < INFINITY)) {
-    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": dx must be positive and finite");
-    return LSMGPU_ERR_INVALID_VALUE;
-  }
   const long n = (long)nx * ny * nz;
-  if (n > 0x7fffffffL) {
-    set_error(LSMGPU_ERR_INVALID_BOX, std::string(R) + ": more than 2^31 - 1 points");
-    return LSMGPU_ERR_INVALID_BOX;
-  }
   const double hmin = fmin(dx[0], fmin(dx[1], dx[2]));
   const double delta = kDeltaCells * hmin;
   // a bound on the passes for inputs without a fixed point (NaN): the
   // threshold crosses the grid in at most (diagonal / delta) steps of a
   // few passes each
   const long max_passes = 4096 + 32L * (nx + ny + nz);
-  cudaStream_t st = cur_stream();
-  Staging stg(st);
-  const Box b{{0, 0, 0}, {nx, ny, nz}};
-  double* dd = (double*)stg.add(distance, b, 8, kOut, "distance_function", R);
-  const double* dp = dd ? (const double*)stg.add(phi, b, 8, kIn, "phi", R) : nullptr;
-  const double* dm = nullptr;
-  if (dp && mask) dm = (const double*)stg.add(mask, b, 8, kIn, "mask", R);
-  if (!dd || !dp || (mask && !dm)) return lsmgpu_peek_last_error();
   unsigned char* status = nullptr;
   Time3* tm = nullptr;
   Lists L{nullptr, nullptr, nullptr, nullptr};
@@ -588,7 +674,8 @@ int distance3d(double* distance, const double* phi, const double* mask, int orde
   if (ok) {
     const dim3 blk(32, 4, 1);
     const dim3 grid3((nx + 31) / 32, (ny + 3) / 4, nz < 65535 ? nz : 65535);
-    k_fmm_front<<<grid3, blk, 0, st>>>(dd, tm, status, dp, dm, nx, ny, nz, dx[0], dx[1], dx[2]);
+    k_fmm_front<<<grid3, blk, 0, st>>>(dd, tm, status, dp, dm, nx, ny, nz, dx[0], dx[1], dx[2],
+                                       X);
     k_fmm_seed<<<elem_blocks, 256, 0, st>>>(status, nx, ny, nz, L, ctrl);
     launch_counter() += 2;
     ok = cuda_ok(cudaGetLastError(), R);
@@ -607,10 +694,10 @@ int distance3d(double* distance, const double* phi, const double* mask, int orde
     for (int q = 0; q < batch; q++) {
       if (order == 1)
         k_fmm_pass<1><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0], i2[1],
-                                                  i2[2], L, ctrl);
+                                                  i2[2], L, ctrl, X);
       else
         k_fmm_pass<2><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0], i2[1],
-                                                  i2[2], L, ctrl);
+                                                  i2[2], L, ctrl, X);
       k_fmm_control<<<1, 32, 0, s>>>(delta, ctrl);
       k_fmm_filter<<<filter_blocks, 256, 0, s>>>(dd, tm, n, L, ctrl);
     }
@@ -640,7 +727,7 @@ int distance3d(double* distance, const double* phi, const double* mask, int orde
     else launch_batch(st);
     launched += batch;
     launch_counter() += 3 * batch;
-    ok = cuda_ok(cudaGetLastError(), R) &&
+    ok = ok && cuda_ok(cudaGetLastError(), R) &&
          cuda_ok(cudaMemcpyAsync(&h_ctrl, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st), R) &&
          cuda_ok(cudaStreamSynchronize(st), R);
     if (!ok || h_ctrl.done) break;
@@ -650,7 +737,7 @@ int distance3d(double* distance, const double* phi, const double* mask, int orde
     }
   }
   if (ok) {
-    k_fmm_unreached<<<elem_blocks, 256, 0, st>>>(dd, status, n);
+    k_fmm_unreached<<<elem_blocks, 256, 0, st>>>(dd, status, n, X);
     ++launch_counter();
     ok = cuda_ok(cudaGetLastError(), R);
   }
@@ -659,7 +746,73 @@ int distance3d(double* distance, const double* phi, const double* mask, int orde
                   (void*)L.stamp, (void*)L.pend_stamp, (void*)ctrl})
     if (q) cudaFreeAsync(q, st);
   if (passes_out) *passes_out = h_ctrl.pass;
-  if (!ok) return lsmgpu_peek_last_error() ? lsmgpu_peek_last_error() : LSMGPU_ERR_CUDA;
+  return ok;
+}
+
+// computeExtensionFields3d / computeDistanceFunction3d on host or device
+// arrays: argument checks, staging, and one solve per group of kMaxFields
+// fields (each solve recomputes the same distance function).
+int extension3d(double* distance, double** ext, const double* phi, const double* mask,
+                double* const* src, const double* emask, int nf, int order,
+                const int* grid_dims, const double* dx, int* passes_out, const char* R) {
+  clear_error();
+  if (!distance || !phi || !grid_dims || !dx || (nf > 0 && (!ext || !src))) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null argument");
+    return LSMGPU_ERR_NULL_POINTER;
+  }
+  for (int k = 0; k < nf; k++)
+    if (!ext[k] || !src[k]) {
+      set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null field pointer");
+      return LSMGPU_ERR_NULL_POINTER;
+    }
+  if (nf < 0) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": negative field count");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  if (order != 1 && order != 2) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": order is 1 or 2");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  const int nx = grid_dims[0], ny = grid_dims[1], nz = grid_dims[2];
+  if (nx < 1 || ny < 1 || nz < 1) {
+    set_error(LSMGPU_ERR_INVALID_BOX, std::string(R) + ": empty grid");
+    return LSMGPU_ERR_INVALID_BOX;
+  }
+  if (!(dx[0] > 0) || !(dx[1] > 0) || !(dx[2] > 0) || !(dx[0] < INFINITY) ||
+      !(dx[1] < INFINITY) || !(dx[2] < INFINITY)) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": dx must be positive and finite");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  if ((long)nx * ny * nz > 0x7fffffffL) {
+    set_error(LSMGPU_ERR_INVALID_BOX, std::string(R) + ": more than 2^31 - 1 points");
+    return LSMGPU_ERR_INVALID_BOX;
+  }
+  cudaStream_t st = cur_stream();
+  Staging stg(st);
+  const Box b{{0, 0, 0}, {nx, ny, nz}};
+  double* dd = (double*)stg.add(distance, b, 8, kOut, "distance_function", R);
+  const double* dp = dd ? (const double*)stg.add(phi, b, 8, kIn, "phi", R) : nullptr;
+  const double* dm = nullptr;
+  if (dp && mask) dm = (const double*)stg.add(mask, b, 8, kIn, "mask", R);
+  const double* dem = nullptr;
+  if (dp && emask) dem = (const double*)stg.add(emask, b, 8, kIn, "extension_mask", R);
+  if (!dd || !dp || (mask && !dm) || (emask && !dem)) return lsmgpu_peek_last_error();
+  int group = 0;
+  do {
+    ExtSet X{};
+    X.emask = dem;
+    X.nf = nf - group < kMaxFields ? nf - group : kMaxFields;
+    for (int k = 0; k < X.nf; k++) {
+      X.ext[k] = (double*)stg.add(ext[group + k], b, 8, kOut, "extension_field", R);
+      X.src[k] = X.ext[k] ? (const double*)stg.add(src[group + k], b, 8, kIn, "source_field",
+                                                   R)
+                          : nullptr;
+      if (!X.ext[k] || !X.src[k]) return lsmgpu_peek_last_error();
+    }
+    if (!solve_device(dd, dp, dm, X, order, grid_dims, dx, passes_out, R, st))
+      return lsmgpu_peek_last_error() ? lsmgpu_peek_last_error() : LSMGPU_ERR_CUDA;
+    group += X.nf;
+  } while (group < nf);
   return stg.finish(R) ? LSMGPU_SUCCESS : LSMGPU_ERR_CUDA;
 }
 
@@ -674,16 +827,40 @@ int computeDistanceFunction3d(double* distance_function, double* phi, double* ma
                               int spatial_discretization_order, int* grid_dims,
                               double* dx) {
   if (spatial_discretization_order != 1 && spatial_discretization_order != 2) return 2;
-  const int rc = distance3d(distance_function, phi, mask, spatial_discretization_order,
-                            grid_dims, dx, nullptr, "computeDistanceFunction3d");
+  const int rc = extension3d(distance_function, nullptr, phi, mask, nullptr, nullptr, 0,
+                             spatial_discretization_order, grid_dims, dx, nullptr,
+                             "computeDistanceFunction3d");
+  return rc == LSMGPU_SUCCESS ? 0 : -1;
+}
+
+// lsm_fast_marching_method.h:331-341, the same return codes
+int computeExtensionFields3d(double* distance_function, double** extension_fields,
+                             double* phi, double* mask, double** source_fields,
+                             double* extension_mask, int num_extension_fields,
+                             int spatial_discretization_order, int* grid_dims, double* dx) {
+  if (spatial_discretization_order != 1 && spatial_discretization_order != 2) return 2;
+  const int rc = extension3d(distance_function, extension_fields, phi, mask, source_fields,
+                             extension_mask, num_extension_fields,
+                             spatial_discretization_order, grid_dims, dx, nullptr,
+                             "computeExtensionFields3d");
   return rc == LSMGPU_SUCCESS ? 0 : -1;
 }
 
 int lsmgpu_distance_function3d(double* distance_function, const double* phi,
                                const double* mask, int order, const int* grid_dims,
                                const double* dx, int* passes) {
-  return distance3d(distance_function, phi, mask, order, grid_dims, dx, passes,
-                    "lsmgpu_distance_function3d");
+  return extension3d(distance_function, nullptr, phi, mask, nullptr, nullptr, 0, order,
+                     grid_dims, dx, passes, "lsmgpu_distance_function3d");
+}
+
+int lsmgpu_extension_fields3d(double* distance_function, double** extension_fields,
+                              const double* phi, const double* mask,
+                              double* const* source_fields, const double* extension_mask,
+                              int num_extension_fields, int order, const int* grid_dims,
+                              const double* dx, int* passes) {
+  return extension3d(distance_function, extension_fields, phi, mask, source_fields,
+                     extension_mask, num_extension_fields, order, grid_dims, dx, passes,
+                     "lsmgpu_extension_fields3d");
 }
 
 }  // extern "C"

@@ -83,6 +83,48 @@ def oracle_fmm():
                         "orc_computeDistanceFunction3d")
 
 
+def _extension_fn(fn, name):
+    import numpy as np
+    P = ctypes.c_void_p
+    fn.restype = ctypes.c_int
+    fn.argtypes = [P, P, P, P, P, P, ctypes.c_int, ctypes.c_int, P, P]
+
+    def run(phi, sources, order, dx, mask=None, ext_mask=None):
+        """(distance, [extension fields]) for C-ordered (nz, ny, nx) arrays."""
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        srcs = [np.ascontiguousarray(s, dtype=np.float64) for s in sources]
+        outs = [np.zeros_like(phi) for _ in srcs]
+        dist = np.zeros_like(phi)
+        nf = len(srcs)
+        src_p = (ctypes.c_void_p * max(nf, 1))(*[s.ctypes.data for s in srcs])
+        out_p = (ctypes.c_void_p * max(nf, 1))(*[o.ctypes.data for o in outs])
+        dims = np.array(phi.shape[::-1], dtype=np.intc)
+        h = np.array(dx, dtype=np.float64)
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
+        em = None if ext_mask is None else np.ascontiguousarray(ext_mask, dtype=np.float64)
+        rc = fn(dist.ctypes.data, ctypes.cast(out_p, P), phi.ctypes.data,
+                None if m is None else m.ctypes.data, ctypes.cast(src_p, P),
+                None if em is None else em.ctypes.data, nf, int(order), dims.ctypes.data,
+                h.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("%s returned %d" % (name, rc))
+        return dist, outs
+    return run
+
+
+def reference_extension():
+    """The reference's computeExtensionFields3d (lsm_fast_marching_method.h:
+    331-341) as ``f(phi, sources, order, dx, mask=None, ext_mask=None) ->
+    (distance, [fields])``, C-ordered arrays, dx in x, y, z order."""
+    return _extension_fn(_load(FMM_SO).computeExtensionFields3d, "computeExtensionFields3d")
+
+
+def oracle_extension():
+    """The C restatement of the same march with extension fields, same call."""
+    return _extension_fn(oracle_lib().orc_computeExtensionFields3d,
+                         "orc_computeExtensionFields3d")
+
+
 def heaviside(x, eps):
     """LSM_HEAVISIDE of lsm_calculus_toolbox.h:41-45, elementwise (numpy)."""
     import numpy as np

@@ -24,6 +24,14 @@
  *     next point in that direction when KNOWN and not larger in |d|; the
  *     upwind quadratic with coefficients accumulated over x, y, z; a
  *     negative discriminant keeps the current value;
+ *   - extension fields (computeExtensionFields3d, :203-370): at the front
+ *     the source fields interpolated linearly to the crossing along each
+ *     axis (or taken from one side where extension_mask < 0) and averaged
+ *     with weights 1/d_axis^2 (:524-660); at every trial update the weighted
+ *     average over the axes in the update of the upwind neighbour's field,
+ *     weights (dist - phi_upwind)/dx^2 (first order, :1135-1168) or
+ *     (1.5 dist - 2 phi_upwind1 + 0.5 phi_upwind2)/dx^2 where the
+ *     second-order stencil is used (:1400-1460);
  *   - the binary heap of FMM_Heap.c:118-470 (insert with sift-up, extract
  *     moving the last node into the root's slot and sifting down, update
  *     sifting up when below the parent and down otherwise), with the same
@@ -170,14 +178,22 @@ typedef struct {
   long s[3];
   real dx[3];
   int order;
+  int nf;            /* extension fields */
+  real **ext;
+  real **src;
+  const real *emask;
   fheap trial;
 } march_t;
 
 static real trial_update(march_t *m, long o, const int c[3]) {
   real A = 0, B = 0, C = 0;
+  int used[3], plus[3], sws[3];
+  real up1[3], up2[3];
   for (int dir = 0; dir < 3; dir++) {
     real u1 = REAL_MAX, u2 = REAL_MAX;
     int sw = 0;
+    used[dir] = 0;
+    plus[dir] = 0;
     for (int sg = -1; sg <= 1; sg += 2) {
       int c1 = c[dir] + sg;
       if (c1 < 0 || c1 >= m->n[dir]) continue;
@@ -187,6 +203,8 @@ static real trial_update(march_t *m, long o, const int c[3]) {
       u1 = m->d[o1];
       u2 = REAL_MAX;
       sw = 0;
+      used[dir] = 1;
+      plus[dir] = sg == 1;
       if (m->order == 2) {
         int c2 = c1 + sg;
         if (c2 >= 0 && c2 < m->n[dir]) {
@@ -198,6 +216,9 @@ static real trial_update(march_t *m, long o, const int c[3]) {
         }
       }
     }
+    up1[dir] = u1;
+    up2[dir] = u2;
+    sws[dir] = sw;
     if (u1 < REAL_MAX) {
       real inv = 1 / m->dx[dir];
       inv *= inv;
@@ -229,6 +250,22 @@ static real trial_update(march_t *m, long o, const int c[3]) {
   } else {
     out = m->d[o];
   }
+  /* extension fields: weighted average over the axes in the update */
+  for (int k = 0; k < m->nf; k++) {
+    real num = 0, den = 0;
+    for (int dir = 0; dir < 3; dir++) {
+      if (!used[dir]) continue;
+      long o1 = o + (plus[dir] ? 1 : -1) * m->s[dir];
+      real inv = 1 / m->dx[dir];
+      inv *= inv;
+      real g = (m->order == 2 && sws[dir] == 1)
+                   ? 1.5 * out - 2.0 * up1[dir] + 0.5 * up2[dir]
+                   : out - up1[dir];
+      num += inv * g * m->ext[k][o1];
+      den += inv * g;
+    }
+    m->ext[k][o] = num / den;
+  }
   m->d[o] = out;
   return out;
 }
@@ -257,15 +294,22 @@ static void update_neighbors(march_t *m, long o) {
   }
 }
 
-/* orc_computeDistanceFunction3d: arrays x fastest, grid_dims and dx in
- * x, y, z order.  Returns 0, or 2 for an order other than 1 and 2. */
-int orc_computeDistanceFunction3d(real *distance, const real *phi, const real *mask,
-                                  int order, const int *grid_dims, const real *dx) {
+/* orc_computeExtensionFields3d: the reference's computeExtensionFields3d
+ * (distance function and extension fields together); arrays x fastest,
+ * grid_dims and dx in x, y, z order.  Returns 0, or 2 for an order other
+ * than 1 and 2. */
+int orc_computeExtensionFields3d(real *distance, real **ext, const real *phi, const real *mask,
+                                 real **src, const real *emask, int nf, int order,
+                                 const int *grid_dims, const real *dx) {
   if (order != 1 && order != 2) return 2;
   march_t m;
   m.d = distance;
   m.phi = phi;
   m.order = order;
+  m.nf = nf;
+  m.ext = ext;
+  m.src = src;
+  m.emask = emask;
   for (int q = 0; q < 3; q++) {
     m.n[q] = grid_dims[q];
     m.dx[q] = dx[q];
@@ -278,10 +322,12 @@ int orc_computeDistanceFunction3d(real *distance, const real *phi, const real *m
   m.handle = (int *)malloc(sizeof(int) * (size_t)np);
   for (long o = 0; o < np; o++) {
     distance[o] = -1;
+    for (int k = 0; k < nf; k++) ext[k][o] = -1;
     m.handle[o] = -1;
     if (mask && mask[o] < 0) {
       m.st[o] = OUTSIDE;
       distance[o] = REAL_MAX;
+      for (int k = 0; k < nf; k++) ext[k][o] = REAL_MAX;
     }
   }
   fheap known;
@@ -289,6 +335,8 @@ int orc_computeDistanceFunction3d(real *distance, const real *phi, const real *m
   h_init(&m.trial, m.n[0] + m.n[1] + m.n[2]);
 
   /* the front (first-order initialisation at both orders) */
+  real *fsum = nf ? (real *)malloc(sizeof(real) * nf) : NULL;
+  real *fdir = nf ? (real *)malloc(sizeof(real) * 2 * nf) : NULL;
   for (long o = 0; o < np; o++) {
     if (m.st[o] == OUTSIDE) continue;
     int c[3] = {(int)(o % m.n[0]), (int)((o / m.n[0]) % m.n[1]),
@@ -296,40 +344,54 @@ int orc_computeDistanceFunction3d(real *distance, const real *phi, const real *m
     real pc = phi[o];
     if (fabs(pc) < ZERO_TOL) {
       distance[o] = pc > 0 ? ZERO_TOL : -ZERO_TOL;
+      for (int k = 0; k < nf; k++) ext[k][o] = src[k][o];
       m.st[o] = KNOWN;
       h_insert(&known, o, distance[o]);
       continue;
     }
     int borders = 0;
     real sum = 0;
+    for (int k = 0; k < nf; k++) fsum[k] = 0;
     for (int dir = 0; dir < 3; dir++) {
       real dp = REAL_MAX, dm = REAL_MAX;
-      if (c[dir] - 1 >= 0) {
-        real p = phi[o - m.s[dir]];
-        if (p * pc <= 0) {
-          dm = pc / (pc - p);
-          dm *= m.dx[dir];
+      for (int k = 0; k < 2 * nf; k++) fdir[k] = 0;   /* [minus k, plus k] */
+      for (int sg = -1; sg <= 1; sg += 2) {
+        if (c[dir] + sg < 0 || c[dir] + sg >= m.n[dir]) continue;
+        long on = o + sg * m.s[dir];
+        real p = phi[on];
+        if (!(p * pc <= 0)) continue;
+        real frac = pc / (pc - p);
+        for (int k = 0; k < nf; k++) {
+          real v;
+          if (emask && emask[o] < 0)
+            v = src[k][on];
+          else if (emask && emask[on] < 0)
+            v = src[k][o];
+          else
+            v = src[k][o] + frac * (src[k][on] - src[k][o]);
+          fdir[(sg == 1 ? nf : 0) + k] = v;
         }
-      }
-      if (c[dir] + 1 < m.n[dir]) {
-        real p = phi[o + m.s[dir]];
-        if (p * pc <= 0) {
-          dp = pc / (pc - p);
-          dp *= m.dx[dir];
-        }
+        frac *= m.dx[dir];
+        if (sg == 1) dp = frac; else dm = frac;
       }
       if (dp < REAL_MAX || dm < REAL_MAX) {
         borders = 1;
-        real dd = dp < dm ? dp : dm;
-        sum += 1 / dd / dd;
+        int use_plus = dp < dm;
+        real dd = use_plus ? dp : dm;
+        real w = 1 / dd / dd;
+        sum += w;
+        for (int k = 0; k < nf; k++) fsum[k] += fdir[(use_plus ? nf : 0) + k] * w;
       }
     }
     if (borders) {
       distance[o] = pc > 0 ? sqrt(1.0 / sum) : -sqrt(1.0 / sum);
+      for (int k = 0; k < nf; k++) ext[k][o] = fsum[k] / sum;
       m.st[o] = KNOWN;
       h_insert(&known, o, distance[o]);
     }
   }
+  free(fsum);
+  free(fdir);
   /* the front's neighbours become trial points */
   while (known.size > 0) {
     long mi;
@@ -351,4 +413,11 @@ int orc_computeDistanceFunction3d(real *distance, const real *phi, const real *m
   free(m.st);
   free(m.handle);
   return 0;
+}
+
+/* orc_computeDistanceFunction3d: the distance function alone. */
+int orc_computeDistanceFunction3d(real *distance, const real *phi, const real *mask, int order,
+                                  const int *grid_dims, const real *dx) {
+  return orc_computeExtensionFields3d(distance, NULL, phi, mask, NULL, NULL, 0, order,
+                                      grid_dims, dx);
 }

@@ -1,5 +1,6 @@
-"""Signed distance functions on the GPU (the reference pylsmlib's
-``computeDistanceFunction``, pylsmlib/pylsmlib/__init__.py:27-84).
+"""Signed distance functions and extension fields on the GPU (the reference
+pylsmlib's ``computeDistanceFunction`` and ``computeExtensionFields``,
+pylsmlib/pylsmlib/__init__.py:27-146).
 
 ``computeDistanceFunction(phi0, dx, order)`` returns the distance function of
 the zero level set of ``phi0`` with the values of the reference's fast
@@ -55,3 +56,50 @@ def computeDistanceFunction(phi0, dx=1.0, order=2, mask=None):
                                         gd, h, None)
     gpu.check_rc(rc, "distance_function3d")
     return out
+
+
+def computeExtensionFields(phi0, speed, dx=1.0, order=2, mask=None, ext_mask=None):
+    """(distance function, extension fields): ``speed`` of phi0's shape or
+    (N,) + phi0.shape, extended off the zero level set of phi0 as the
+    reference does (computeExtensionFields3d).  ``ext_mask`` is boolean:
+    True marks the points whose own source value is used at the interface
+    (the reference passes it on as -ext_mask * 2 + 1)."""
+    phi = np.ascontiguousarray(np.asarray(phi0, dtype=np.float64))
+    if phi.ndim not in (1, 2, 3):
+        raise ValueError("phi0 must be 1D, 2D or 3D")
+    dims, spacing = _dims_dx(phi.shape, dx)
+    if order not in (1, 2):
+        raise ValueError("order must be 1 or 2")
+    u0 = np.asarray(speed, dtype=np.float64)
+    u0shape = u0.shape
+    if u0shape == phi.shape:
+        u0 = u0.reshape((1,) + u0shape)
+    if u0.shape[1:] != phi.shape:
+        raise ValueError("phi and speed must have the same shape")
+    m = None
+    if mask is not None:
+        m = np.ascontiguousarray(np.asarray(mask, dtype=np.float64))
+        if m.shape != phi.shape:
+            raise ValueError("phi and mask have incompatible shapes")
+    em = None
+    if ext_mask is not None:
+        em = np.asarray(ext_mask, dtype=np.float64)
+        if em.shape != phi.shape:
+            raise ValueError("phi and extensionMask have incompatible shapes")
+        em = np.ascontiguousarray(-em * 2.0 + 1.0)
+    nf = u0.shape[0]
+    src = [np.ascontiguousarray(u0[k]) for k in range(nf)]
+    ext = [np.empty_like(phi) for _ in range(nf)]
+    dist = np.empty_like(phi)
+    lib = gpu.load()
+    gd = (ctypes.c_int * 3)(*dims)
+    h = (ctypes.c_double * 3)(*spacing)
+    src_p = (ctypes.c_void_p * max(nf, 1))(*[a.ctypes.data for a in src])
+    ext_p = (ctypes.c_void_p * max(nf, 1))(*[a.ctypes.data for a in ext])
+    rc = lib.lsmgpu_extension_fields3d(dist.ctypes.data, ctypes.cast(ext_p, ctypes.c_void_p),
+                                       phi.ctypes.data, None if m is None else m.ctypes.data,
+                                       ctypes.cast(src_p, ctypes.c_void_p),
+                                       None if em is None else em.ctypes.data, nf, int(order),
+                                       gd, h, None)
+    gpu.check_rc(rc, "extension_fields3d")
+    return dist, np.stack(ext).reshape(u0shape)

@@ -1,7 +1,9 @@
 """Regenerate tests/golden/fmm_golden.npz from the reference's own fast
 marching method (its C sources built by ``make -C oracle ref`` into
 oracle/_ref/libfmm.so): computeDistanceFunction3d on seeded unions of spheres
-(anisotropic spacing, with and without a mask, 3D and 2D), orders 1 and 2.
+(anisotropic spacing, with and without a mask, 3D and 2D), orders 1 and 2,
+and computeExtensionFields3d on the same cases with two seeded source fields
+(and an extension mask in the masked case).
 
     make -C oracle ref && python tests/golden/gen_fmm_golden.py
 """
@@ -42,16 +44,41 @@ def cases():
     return out
 
 
+def sources(name, phi, mask):
+    """Two source fields (quantised to 1/64, so they compress) and, with a
+    mask, an extension mask."""
+    rng = np.random.default_rng(len(name) * 7919)
+    src = [np.round(64 * rng.standard_normal(phi.shape)) / 64,
+           np.round(64 * np.cos(0.37 * np.arange(phi.size, dtype=np.float64))).reshape(
+               phi.shape) / 64]
+    emask = None
+    if mask is not None:
+        emask = np.where(rng.random(phi.shape) < 0.3, -1.0, 1.0)
+    return src, emask
+
+
 def main():
     fmm = oracle.reference_fmm()
+    ext = oracle.reference_extension()
     blobs = {}
     for name, phi, h, mask in cases():
         blobs[name + "|phi"] = phi
         blobs[name + "|dx"] = np.array(h)
         if mask is not None:
             blobs[name + "|mask"] = mask
+        src, emask = sources(name, phi, mask)
+        for k, a in enumerate(src):
+            blobs["%s|src%d" % (name, k)] = a
+        if emask is not None:
+            blobs[name + "|emask"] = emask
         for order in (1, 2):
             blobs["%s|out%d" % (name, order)] = fmm(phi, order, h[::-1], mask)
+            dist, fields = ext(phi, src, order, h[::-1], mask, emask)
+            # the distance of the extension call is the distance function's
+            assert np.array_equal(dist.view(np.uint64),
+                                  blobs["%s|out%d" % (name, order)].view(np.uint64))
+            for k, f in enumerate(fields):
+                blobs["%s|ext%d_%d" % (name, order, k)] = f
     np.savez_compressed(OUT, **blobs)
     print("wrote %s (%.1f KB)" % (OUT, os.path.getsize(OUT) / 1024))
 

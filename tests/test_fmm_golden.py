@@ -6,6 +6,7 @@
 * The C restatement of the heap march (oracle/fmm_oracle.c) reproduces the
   same golden outputs, and the reference's results on seeded noisy unions of
   spheres, bit for bit (these pin the restatement).
+* The same for the extension fields (computeExtensionFields3d).
 """
 import os
 
@@ -97,6 +98,62 @@ def test_oracle_fmm_edge_cases():
     # an order other than 1 or 2 is refused with the reference's code 2
     with pytest.raises(RuntimeError, match="returned 2"):
         fmm(phi, 3, [1.0, 1.0, 1.0])
+
+
+def ext_case(z, name):
+    """Source fields and extension mask (or None) of a golden case."""
+    src = [z["%s|src%d" % (name, k)] for k in range(2)]
+    emask = z[name + "|emask"] if name + "|emask" in z.files else None
+    return src, emask
+
+
+def seeded_sources(shape, seed, n=2):
+    rng = np.random.default_rng(seed + 100)
+    out = [rng.standard_normal(shape)]
+    x = np.arange(np.prod(shape), dtype=np.float64).reshape(shape)
+    out += [np.cos(0.01 * (k + 1) * x) for k in range(n - 1)]
+    return out
+
+
+@pytest.mark.skipif(not oracle.fmm_available(), reason="oracle/_ref/libfmm.so not built")
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_reference_extension_reproduces_golden(name, order):
+    z = np.load(GOLDEN)
+    phi, dx, mask = _case(z, name)
+    src, emask = ext_case(z, name)
+    dist, fields = oracle.reference_extension()(phi, src, order, dx, mask, emask)
+    assert np.array_equal(dist.view(np.uint64), z["%s|out%d" % (name, order)].view(np.uint64))
+    for k, f in enumerate(fields):
+        assert np.array_equal(f.view(np.uint64), z["%s|ext%d_%d" % (name, order, k)].view(np.uint64))
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_oracle_extension_reproduces_golden(name, order):
+    z = np.load(GOLDEN)
+    phi, dx, mask = _case(z, name)
+    src, emask = ext_case(z, name)
+    dist, fields = oracle.oracle_extension()(phi, src, order, dx, mask, emask)
+    assert np.array_equal(dist.view(np.uint64), z["%s|out%d" % (name, order)].view(np.uint64))
+    for k, f in enumerate(fields):
+        assert np.array_equal(f.view(np.uint64), z["%s|ext%d_%d" % (name, order, k)].view(np.uint64))
+
+
+@pytest.mark.skipif(not oracle.fmm_available(), reason="oracle/_ref/libfmm.so not built")
+@pytest.mark.parametrize("shape,seed", [((33, 41, 29), 1), ((20, 64, 48), 2), ((1, 50, 60), 3)])
+@pytest.mark.parametrize("order", [1, 2])
+def test_oracle_extension_matches_reference(shape, seed, order):
+    phi, dx = seeded_spheres(shape, seed)
+    mask = seeded_mask(shape, seed)
+    emask = None
+    if mask is not None:
+        emask = np.where(np.random.default_rng(seed).random(shape) < 0.3, -1.0, 1.0)
+    src = seeded_sources(shape, seed)
+    a = oracle.reference_extension()(phi, src, order, dx, mask, emask)
+    b = oracle.oracle_extension()(phi, src, order, dx, mask, emask)
+    for x, y in zip([a[0]] + a[1], [b[0]] + b[1]):
+        assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
 
 
 @pytest.mark.parametrize("name", NAMES)

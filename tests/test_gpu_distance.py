@@ -116,3 +116,113 @@ def test_pylsmlib_compute_distance_function():
     assert same_bits(got, z["spheres2d|out2"][0])
     got1 = computeDistanceFunction(phi[5], dx[1], order=1)      # 1D
     assert same_bits(got1, oracle.oracle_fmm()(phi[5][None, None, :], 1, [dx[1], 1.0, 1.0])[0, 0])
+
+
+# ---- extension fields -------------------------------------------------------
+from test_fmm_golden import ext_case, seeded_sources  # noqa: E402
+
+
+def gpu_extension(lib, phi, sources, order, dx, mask=None, emask=None):
+    """lsmgpu_extension_fields3d on host arrays: (distance, [fields])."""
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    src = [np.ascontiguousarray(a, dtype=np.float64) for a in sources]
+    ext = [np.zeros_like(phi) for _ in src]
+    dist = np.zeros_like(phi)
+    nf = len(src)
+    src_p = (ctypes.c_void_p * max(nf, 1))(*[a.ctypes.data for a in src])
+    ext_p = (ctypes.c_void_p * max(nf, 1))(*[a.ctypes.data for a in ext])
+    dims = (ctypes.c_int * 3)(*phi.shape[::-1])
+    h = (ctypes.c_double * 3)(*dx)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
+    em = None if emask is None else np.ascontiguousarray(emask, dtype=np.float64)
+    rc = lib.lsmgpu_extension_fields3d(dist.ctypes.data, ctypes.cast(ext_p, ctypes.c_void_p),
+                                       phi.ctypes.data, None if m is None else m.ctypes.data,
+                                       ctypes.cast(src_p, ctypes.c_void_p),
+                                       None if em is None else em.ctypes.data, nf, order, dims,
+                                       h, None)
+    assert rc == 0, lib.lsmgpu_get_last_error_string()
+    return dist, ext
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_extension_reproduces_reference_golden(lib, name, order):
+    z = np.load(GOLDEN)
+    phi, dx, mask = _case(z, name)
+    src, emask = ext_case(z, name)
+    dist, fields = gpu_extension(lib, phi, src, order, dx, mask, emask)
+    assert same_bits(dist, z["%s|out%d" % (name, order)])
+    for k, f in enumerate(fields):
+        assert same_bits(f, z["%s|ext%d_%d" % (name, order, k)])
+
+
+@pytest.mark.parametrize("shape,seed", [((33, 41, 29), 1), ((20, 64, 48), 2), ((1, 80, 90), 3),
+                                        ((64, 64, 64), 4)])
+@pytest.mark.parametrize("order", [1, 2])
+def test_extension_matches_oracle(lib, shape, seed, order):
+    phi, dx = seeded_spheres(shape, seed)
+    mask = seeded_mask(shape, seed)
+    emask = None
+    if mask is not None:
+        emask = np.where(np.random.default_rng(seed).random(shape) < 0.3, -1.0, 1.0)
+    src = seeded_sources(shape, seed, n=3)
+    want = oracle.oracle_extension()(phi, src, order, dx, mask, emask)
+    got = gpu_extension(lib, phi, src, order, dx, mask, emask)
+    assert same_bits(got[0], want[0])
+    for a, b in zip(got[1], want[1]):
+        assert same_bits(a, b), (np.mean(a == b), np.nanmax(np.abs(a - b)))
+
+
+def test_extension_more_fields_than_one_solve(lib):
+    """Nine fields: two groups of solves, each field as the oracle has it."""
+    phi, dx = seeded_spheres((24, 28, 20), 6)
+    src = seeded_sources((24, 28, 20), 6, n=9)
+    want = oracle.oracle_extension()(phi, src, 2, dx)
+    got = gpu_extension(lib, phi, src, 2, dx)
+    assert same_bits(got[0], want[0])
+    for a, b in zip(got[1], want[1]):
+        assert same_bits(a, b)
+
+
+def test_extension_c_abi_entry_point(lib):
+    """computeExtensionFields3d with the reference's arguments (host arrays)
+    and its return code 2 for a bad order."""
+    z = np.load(GOLDEN)
+    phi, dx, mask = _case(z, "masked3d")
+    src, emask = ext_case(z, "masked3d")
+    fn = lib.computeExtensionFields3d
+    P = ctypes.c_void_p
+    fn.restype = ctypes.c_int
+    fn.argtypes = [P, P, P, P, P, P, ctypes.c_int, ctypes.c_int, P, P]
+    phi = np.ascontiguousarray(phi)
+    dist = np.zeros_like(phi)
+    ext = [np.zeros_like(phi) for _ in src]
+    src = [np.ascontiguousarray(a) for a in src]
+    ext_p = (ctypes.c_void_p * 2)(*[a.ctypes.data for a in ext])
+    src_p = (ctypes.c_void_p * 2)(*[a.ctypes.data for a in src])
+    dims = np.array(phi.shape[::-1], dtype=np.intc)
+    h = np.array(dx)
+    m, em = np.ascontiguousarray(mask), np.ascontiguousarray(emask)
+    args = [dist.ctypes.data, ctypes.cast(ext_p, P), phi.ctypes.data, m.ctypes.data,
+            ctypes.cast(src_p, P), em.ctypes.data, 2]
+    assert fn(*args, 1, dims.ctypes.data, h.ctypes.data) == 0
+    assert same_bits(dist, z["masked3d|out1"])
+    assert same_bits(ext[0], z["masked3d|ext1_0"]) and same_bits(ext[1], z["masked3d|ext1_1"])
+    assert fn(*args, 3, dims.ctypes.data, h.ctypes.data) == 2
+
+
+def test_pylsmlib_compute_extension_fields():
+    """The Python front door: (N,) + shape speeds, boolean ext_mask."""
+    from pylsmlib import computeExtensionFields
+    phi, dx = seeded_spheres((1, 40, 50), 8)
+    phi2 = phi[0]
+    src = seeded_sources((1, 40, 50), 8, n=2)
+    speed = np.stack([a[0] for a in src])
+    em = np.random.default_rng(3).random(phi2.shape) < 0.2
+    dist, ext = computeExtensionFields(phi2, speed, dx=[dx[1], dx[0]], order=1, ext_mask=em)
+    want = oracle.oracle_extension()(phi, src, 1, dx, None,
+                                     (-em.astype(float) * 2.0 + 1.0)[None])
+    assert same_bits(dist, want[0][0])
+    assert ext.shape == speed.shape
+    for k in range(2):
+        assert same_bits(ext[k], want[1][k][0])
