@@ -423,6 +423,15 @@ int computeExtensionFields3d(LSMLIB_REAL *distance_function,
                              LSMLIB_REAL *extension_mask, int num_extension_fields,
                              int spatial_discretization_order, int *grid_dims,
                              LSMLIB_REAL *dx);
+/* lsm_fast_marching_method.h:463-469: solves |grad phi| speed = 1.  phi
+ * holds the boundary data on input -- the points with phi > -1e-11 keep
+ * their values -- and the solution on output, with the reference's march
+ * values (first or second order).  Points with mask < 0 (mask may be NULL)
+ * or speed < 1e-11 get LSMLIB_REAL_MAX; points no boundary value reaches
+ * keep their input.  Same return codes as computeDistanceFunction3d. */
+int solveEikonalEquation3d(LSMLIB_REAL *phi, LSMLIB_REAL *speed, LSMLIB_REAL *mask,
+                           int spatial_discretization_order, int *grid_dims,
+                           LSMLIB_REAL *dx);
 
 /* ======================================================================== */
 /* Part 2 -- extension API                                                   */
@@ -663,6 +672,10 @@ int lsmgpu_extension_fields3d(double *distance_function, double **extension_fiel
                               const double *extension_mask, int num_extension_fields,
                               int order, const int grid_dims[3], const double dx[3],
                               int *passes);
+/* solveEikonalEquation3d with the lsmgpu error codes and the number of
+ * passes. */
+int lsmgpu_eikonal3d(double *phi, const double *speed, const double *mask, int order,
+                     const int grid_dims[3], const double dx[3], int *passes);
 
 /* ---- an entry point that allocates no memory --------------------------------
  * No counterpart in the reference.  For callers that must not allocate device

@@ -174,6 +174,36 @@ __global__ void k_fmm_front(double* d, Time3* tm, unsigned char* st, const doubl
   }
 }
 
+// The Eikonal solver's data (solveEikonalEquation3d): the speed F and the
+// input phi, whose values the points never updated keep.  speed == nullptr
+// for the distance function.
+struct Eik {
+  const double* speed;
+  const double* phi0;
+};
+
+// FMM_initializeFront_Eikonal3d (lsm_FMM_eikonal.c:259-312) and the domain
+// marking before it (:214-246): points with mask < 0 or speed < 1e-11 are
+// outside the domain and get LSMLIB_REAL_MAX; points with phi > -1e-11 are
+// the front, KNOWN with their own values; the others start unreached.
+__global__ void k_eik_front(double* d, Time3* tm, unsigned char* st, const double* phi0,
+                            const double* speed, const double* mask, long n) {
+  for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n;
+       o += (long)gridDim.x * blockDim.x) {
+    tm[o] = Time3{INFINITY, INFINITY, INFINITY};
+    if ((mask && mask[o] < 0) || speed[o] < kZeroTol) {
+      st[o] = kOutside;
+      d[o] = DBL_MAX;
+    } else if (phi0[o] > -kZeroTol) {
+      st[o] = kFront;
+      d[o] = phi0[o];
+    } else {
+      st[o] = kFree;
+      d[o] = INFINITY;
+    }
+  }
+}
+
 // The neighbours of one point, by slot 2*axis + (plus side): the immediate
 // neighbour (value v1, time t1) and, at second order, the next one in that
 // direction (v2, t2).
@@ -191,11 +221,14 @@ struct Stencil {
 // direction counts when it was KNOWN at the update -- a front point, or a
 // free point accepted before the trigger (time ``trig``; the front phase
 // comes before every free point) -- and its |d| is not above the
-// neighbour's.  Returns the discriminant B^2 - 4AC.
+// neighbour's.  ``cterm`` is what the constant term loses: 1 for the
+// distance function, 1/F^2 for the Eikonal solver (lsm_FMM_eikonal.c:427,
+// :621).  Returns the discriminant B^2 - 4AC.
 template <int ORDER>
 __device__ __forceinline__ double fmm_coeffs(const Stencil& n, int incl,
                                              const Time3& trig, bool has_trigger,
-                                             const double i2[3], double& A, double& B) {
+                                             const double i2[3], double cterm, double& A,
+                                             double& B) {
   double C = 0;
   A = 0;
   B = 0;
@@ -232,12 +265,16 @@ __device__ __forceinline__ double fmm_coeffs(const Stencil& n, int incl,
     }
   }
   B *= -2.0;
-  C -= 1.0;
+  C -= cterm;
   return B * B - 4.0 * A * C;
 }
 
-// The root the reference takes (disc >= 0), in its rounding.
+// The root the reference takes (disc >= 0), in its rounding: by the sign
+// of B for the distance function (lsm_FMM_field_extension.c:1106-1117), the
+// larger root for the Eikonal solver (lsm_FMM_eikonal.c:433-436).
+template <bool EIK>
 __device__ __forceinline__ double fmm_root(double A, double B, double disc) {
+  if (EIK) return 0.5 * (-B + sqrt(disc)) / A;
   if (B == 0) return 0;
   if (B < kZeroTol) return 0.5 * (-B + sqrt(disc)) / A;
   return 0.5 * (-B - sqrt(disc)) / A;
@@ -271,15 +308,17 @@ constexpr double kDeltaCells = 2.0;
 // point's final time -- every neighbour in it accepted before the point --
 // as it always is in a real march; when it is not (a transient state of the
 // passes), the set is cut before the earliest offending neighbour and the
-// update is taken again.  A negative discriminant keeps the previous value,
-// -1 (the reference's default) when there is none.  Neighbours off the grid
+// update is taken again.  A negative discriminant keeps the previous value:
+// -1 (the reference's default) when there is none, or for the Eikonal
+// solver the point's input.  Neighbours off the grid
 // are left out, as the reference's bounds checks do.
-template <int ORDER>
+template <int ORDER, bool EIK>
 __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
                                           const unsigned char* st, long o, const int c[3],
                                           const int n[3], const long s[3], const double i2[3],
-                                          Stencil& nb, double& val, Time3& tv, int& incl_out,
-                                          Time3& trig_out, bool& trig_free_out) {
+                                          const Eik& E, Stencil& nb, double& val, Time3& tv,
+                                          int& incl_out, Time3& trig_out,
+                                          bool& trig_free_out) {
   // every load first, at in-range addresses (the point itself stands in
   // for a neighbour off the grid), so that they are in flight together
   unsigned char s1[6], s2[6];
@@ -327,16 +366,18 @@ __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
   }
   if (!nb.has1) return false;
   const int free1 = nb.has1 & ~nb.front1;
+  const double cterm = EIK ? 1 / E.speed[o] / E.speed[o] : 1.0;
+  const double none = EIK ? E.phi0[o] : -1.0;   // the value without an update
   Time3 cap{INFINITY, INFINITY, INFINITY};   // only neighbours before this
   for (;;) {
     int incl = nb.front1;
     bool have = incl != 0, trig_free = false;
     Time3 trig{-INFINITY, -1.0, -1.0};
-    double cur = -1.0;
+    double cur = none;
     if (have) {
       double A, B;
-      const double disc = fmm_coeffs<ORDER>(nb, incl, trig, false, i2, A, B);
-      if (disc >= 0) cur = fmm_root(A, B, disc);
+      const double disc = fmm_coeffs<ORDER>(nb, incl, trig, false, i2, cterm, A, B);
+      if (disc >= 0) cur = fmm_root<EIK>(A, B, disc);
     }
     for (int rem = free1; rem;) {
       // the earliest remaining free neighbour (ties by slot)
@@ -357,8 +398,8 @@ __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
       trig = bt;
       trig_free = true;
       double A, B;
-      const double disc = fmm_coeffs<ORDER>(nb, incl, trig, true, i2, A, B);
-      if (disc >= 0) cur = fmm_root(A, B, disc);
+      const double disc = fmm_coeffs<ORDER>(nb, incl, trig, true, i2, cterm, A, B);
+      if (disc >= 0) cur = fmm_root<EIK>(A, B, disc);
       have = true;
     }
     const Time3 t = tafter(trig, fabs(cur), trig_free);
@@ -492,10 +533,10 @@ __global__ void k_fmm_seed(const unsigned char* st, int nx, int ny, int nz, List
 }
 
 // One pass over the active list (count[pass & 1]).
-template <int ORDER>
+template <int ORDER, bool EIK>
 __global__ void __launch_bounds__(128, ORDER == 1 ? 4 : 3)
 k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz,
-           double i2x, double i2y, double i2z, Lists L, Ctrl* ctrl, ExtSet X) {
+           double i2x, double i2y, double i2z, Lists L, Ctrl* ctrl, ExtSet X, Eik E) {
   const int it = ctrl->pass;
   const int par = it & 1;
   const int count = ctrl->count[par];
@@ -520,7 +561,8 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
     Time3 tv, trig;
     int incl;
     bool trig_free;
-    if (!fmm_point<ORDER>(d, tm, st, o, c, nn, s, i2, nb, val, tv, incl, trig, trig_free))
+    if (!fmm_point<ORDER, EIK>(d, tm, st, o, c, nn, s, i2, E, nb, val, tv, incl, trig,
+                               trig_free))
       continue;
     const double old = d[o];
     bool ext_changed = false;
@@ -530,7 +572,7 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
       push_once(o, ep + 1, L.pend_stamp, pend, pend_count);
       const unsigned long long bits = __double_as_longlong(tv.a);
       minrej = bits < minrej ? bits : minrej;
-    } else if (X.nf) {
+    } else if (!EIK && X.nf) {
       ext_changed = fmm_ext<ORDER>(nb, incl, trig, trig_free, val, i2, X, o, s);
     }
     if (val == old && tequal(tv, tm[o]) && !ext_changed) continue;
@@ -620,21 +662,23 @@ __global__ void k_fmm_filter(const double* d, const Time3* tm, long n, Lists L, 
 }
 
 // free points no front reached: the reference's default value -1 (distance
-// and extension fields)
-__global__ void k_fmm_unreached(double* d, const unsigned char* st, long n, ExtSet X) {
+// and extension fields), or the Eikonal solver's input
+__global__ void k_fmm_unreached(double* d, const unsigned char* st, long n, ExtSet X,
+                                const double* phi0) {
   for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n;
        o += (long)gridDim.x * blockDim.x)
     if (st[o] == kFree && !(fabs(d[o]) <= DBL_MAX)) {
-      d[o] = -1.0;
+      d[o] = phi0 ? phi0[o] : -1.0;
       for (int f = 0; f < X.nf; f++) X.ext[f][o] = -1.0;
     }
 }
 
 // One solve on device arrays: the distance function and up to kMaxFields
-// extension fields (X.nf may be 0).
-bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& X, int order,
-                  const int* grid_dims, const double* dx, int* passes_out, const char* R,
-                  cudaStream_t st) {
+// extension fields (X.nf may be 0), or with E.speed the Eikonal solution
+// for the boundary data E.phi0 (dp unused).
+bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& X,
+                  const Eik& E, int order, const int* grid_dims, const double* dx,
+                  int* passes_out, const char* R, cudaStream_t st) {
   const int nx = grid_dims[0], ny = grid_dims[1], nz = grid_dims[2];
   const long n = (long)nx * ny * nz;
   const double hmin = fmin(dx[0], fmin(dx[1], dx[2]));
@@ -674,8 +718,11 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
   if (ok) {
     const dim3 blk(32, 4, 1);
     const dim3 grid3((nx + 31) / 32, (ny + 3) / 4, nz < 65535 ? nz : 65535);
-    k_fmm_front<<<grid3, blk, 0, st>>>(dd, tm, status, dp, dm, nx, ny, nz, dx[0], dx[1], dx[2],
-                                       X);
+    if (E.speed)
+      k_eik_front<<<elem_blocks, 256, 0, st>>>(dd, tm, status, E.phi0, E.speed, dm, n);
+    else
+      k_fmm_front<<<grid3, blk, 0, st>>>(dd, tm, status, dp, dm, nx, ny, nz, dx[0], dx[1],
+                                         dx[2], X);
     k_fmm_seed<<<elem_blocks, 256, 0, st>>>(status, nx, ny, nz, L, ctrl);
     launch_counter() += 2;
     ok = cuda_ok(cudaGetLastError(), R);
@@ -692,12 +739,18 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
   const int batch = 32;
   auto launch_batch = [&](cudaStream_t s) {
     for (int q = 0; q < batch; q++) {
-      if (order == 1)
-        k_fmm_pass<1><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0], i2[1],
-                                                  i2[2], L, ctrl, X);
+      if (order == 1 && !E.speed)
+        k_fmm_pass<1, false><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0],
+                                                         i2[1], i2[2], L, ctrl, X, E);
+      else if (!E.speed)
+        k_fmm_pass<2, false><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0],
+                                                         i2[1], i2[2], L, ctrl, X, E);
+      else if (order == 1)
+        k_fmm_pass<1, true><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0],
+                                                        i2[1], i2[2], L, ctrl, X, E);
       else
-        k_fmm_pass<2><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0], i2[1],
-                                                  i2[2], L, ctrl, X);
+        k_fmm_pass<2, true><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0],
+                                                        i2[1], i2[2], L, ctrl, X, E);
       k_fmm_control<<<1, 32, 0, s>>>(delta, ctrl);
       k_fmm_filter<<<filter_blocks, 256, 0, s>>>(dd, tm, n, L, ctrl);
     }
@@ -737,7 +790,7 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
     }
   }
   if (ok) {
-    k_fmm_unreached<<<elem_blocks, 256, 0, st>>>(dd, status, n, X);
+    k_fmm_unreached<<<elem_blocks, 256, 0, st>>>(dd, status, n, X, E.phi0);
     ++launch_counter();
     ok = cuda_ok(cudaGetLastError(), R);
   }
@@ -809,10 +862,58 @@ int extension3d(double* distance, double** ext, const double* phi, const double*
                           : nullptr;
       if (!X.ext[k] || !X.src[k]) return lsmgpu_peek_last_error();
     }
-    if (!solve_device(dd, dp, dm, X, order, grid_dims, dx, passes_out, R, st))
+    if (!solve_device(dd, dp, dm, X, Eik{nullptr, nullptr}, order, grid_dims, dx, passes_out,
+                      R, st))
       return lsmgpu_peek_last_error() ? lsmgpu_peek_last_error() : LSMGPU_ERR_CUDA;
     group += X.nf;
   } while (group < nf);
+  return stg.finish(R) ? LSMGPU_SUCCESS : LSMGPU_ERR_CUDA;
+}
+
+// solveEikonalEquation3d on host or device arrays: phi holds the boundary
+// data on input and the solution on output.
+int eikonal3d(double* phi, const double* speed, const double* mask, int order,
+              const int* grid_dims, const double* dx, int* passes_out, const char* R) {
+  clear_error();
+  if (!phi || !speed || !grid_dims || !dx) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null argument");
+    return LSMGPU_ERR_NULL_POINTER;
+  }
+  if (order != 1 && order != 2) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": order is 1 or 2");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  const int nx = grid_dims[0], ny = grid_dims[1], nz = grid_dims[2];
+  if (nx < 1 || ny < 1 || nz < 1) {
+    set_error(LSMGPU_ERR_INVALID_BOX, std::string(R) + ": empty grid");
+    return LSMGPU_ERR_INVALID_BOX;
+  }
+  if (!(dx[0] > 0) || !(dx[1] > 0) || !(dx[2] > 0) || !(dx[0] < INFINITY) ||
+      !(dx[1] < INFINITY) || !(dx[2] < INFINITY)) {
+    set_error(LSMGPU_ERR_INVALID_VALUE, std::string(R) + ": dx must be positive and finite");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  const long n = (long)nx * ny * nz;
+  if (n > 0x7fffffffL) {
+    set_error(LSMGPU_ERR_INVALID_BOX, std::string(R) + ": more than 2^31 - 1 points");
+    return LSMGPU_ERR_INVALID_BOX;
+  }
+  cudaStream_t st = cur_stream();
+  Staging stg(st);
+  const Box b{{0, 0, 0}, {nx, ny, nz}};
+  double* dd = (double*)stg.add(phi, b, 8, kInOut, "phi", R);
+  const double* df = dd ? (const double*)stg.add(speed, b, 8, kIn, "speed", R) : nullptr;
+  const double* dm = nullptr;
+  if (df && mask) dm = (const double*)stg.add(mask, b, 8, kIn, "mask", R);
+  if (!dd || !df || (mask && !dm)) return lsmgpu_peek_last_error();
+  double* phi0 = nullptr;
+  bool ok = cuda_ok(cudaMallocAsync((void**)&phi0, (size_t)n * sizeof(double), st), R) &&
+            cuda_ok(cudaMemcpyAsync(phi0, dd, (size_t)n * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, st), R);
+  ok = ok && solve_device(dd, nullptr, dm, ExtSet{}, Eik{df, phi0}, order, grid_dims, dx,
+                          passes_out, R, st);
+  if (phi0) cudaFreeAsync(phi0, st);
+  if (!ok) return lsmgpu_peek_last_error() ? lsmgpu_peek_last_error() : LSMGPU_ERR_CUDA;
   return stg.finish(R) ? LSMGPU_SUCCESS : LSMGPU_ERR_CUDA;
 }
 
@@ -861,6 +962,20 @@ int lsmgpu_extension_fields3d(double* distance_function, double** extension_fiel
   return extension3d(distance_function, extension_fields, phi, mask, source_fields,
                      extension_mask, num_extension_fields, order, grid_dims, dx, passes,
                      "lsmgpu_extension_fields3d");
+}
+
+// lsm_fast_marching_method.h:463-469, the same return codes
+int solveEikonalEquation3d(double* phi, double* speed, double* mask,
+                           int spatial_discretization_order, int* grid_dims, double* dx) {
+  if (spatial_discretization_order != 1 && spatial_discretization_order != 2) return 2;
+  const int rc = eikonal3d(phi, speed, mask, spatial_discretization_order, grid_dims, dx,
+                           nullptr, "solveEikonalEquation3d");
+  return rc == LSMGPU_SUCCESS ? 0 : -1;
+}
+
+int lsmgpu_eikonal3d(double* phi, const double* speed, const double* mask, int order,
+                     const int* grid_dims, const double* dx, int* passes) {
+  return eikonal3d(phi, speed, mask, order, grid_dims, dx, passes, "lsmgpu_eikonal3d");
 }
 
 }  // extern "C"

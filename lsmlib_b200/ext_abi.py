@@ -26,6 +26,7 @@ SIGNATURES = {
     "lsmgpu_normal_rhs_dt_noalloc": (I, [P, P, P, P, IA, IA, DA, D]),
     "lsmgpu_distance_function3d": (I, [P, P, P, I, P, P, P]),
     "lsmgpu_extension_fields3d": (I, [P, P, P, P, P, P, I, I, P, P, P]),
+    "lsmgpu_eikonal3d": (I, [P, P, P, I, P, P, P]),
     "lsmgpu_batch_create": (I, [ctypes.POINTER(P), I, IA, DA, I]),
     "lsmgpu_batch_destroy": (I, [P]),
     "lsmgpu_batch_grid": (I, [P, I, ctypes.POINTER(ctypes.c_longlong), IA]),

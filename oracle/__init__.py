@@ -125,6 +125,39 @@ def oracle_extension():
                          "orc_computeExtensionFields3d")
 
 
+def _eikonal_fn(fn, name):
+    import numpy as np
+    P = ctypes.c_void_p
+    fn.restype = ctypes.c_int
+    fn.argtypes = [P, P, P, ctypes.c_int, P, P]
+
+    def run(phi, speed, order, dx, mask=None):
+        """The solution for boundary data ``phi`` (C-ordered (nz, ny, nx),
+        front where phi > -1e-11); a new array."""
+        out = np.array(phi, dtype=np.float64, order="C", copy=True)
+        f = np.ascontiguousarray(speed, dtype=np.float64)
+        dims = np.array(out.shape[::-1], dtype=np.intc)
+        h = np.array(dx, dtype=np.float64)
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
+        rc = fn(out.ctypes.data, f.ctypes.data, None if m is None else m.ctypes.data,
+                int(order), dims.ctypes.data, h.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("%s returned %d" % (name, rc))
+        return out
+    return run
+
+
+def reference_eikonal():
+    """The reference's solveEikonalEquation3d (lsm_fast_marching_method.h:
+    463-469) as ``f(phi, speed, order, dx, mask=None) -> phi``."""
+    return _eikonal_fn(_load(FMM_SO).solveEikonalEquation3d, "solveEikonalEquation3d")
+
+
+def oracle_eikonal():
+    """The C restatement of the same march (fmm_oracle.c), same call."""
+    return _eikonal_fn(oracle_lib().orc_solveEikonalEquation3d, "orc_solveEikonalEquation3d")
+
+
 def heaviside(x, eps):
     """LSM_HEAVISIDE of lsm_calculus_toolbox.h:41-45, elementwise (numpy)."""
     import numpy as np

@@ -32,6 +32,11 @@
  *     weights (dist - phi_upwind)/dx^2 (first order, :1135-1168) or
  *     (1.5 dist - 2 phi_upwind1 + 0.5 phi_upwind2)/dx^2 where the
  *     second-order stencil is used (:1400-1460);
+ *   - the Eikonal solver (solveEikonalEquation3d, lsm_FMM_eikonal.c:140-652):
+ *     points with mask < 0 or speed < 1e-11 are outside (LSMLIB_REAL_MAX),
+ *     points with phi > -1e-11 are the KNOWN front with their own values,
+ *     the update's constant term is 1/speed^2 and its root always
+ *     0.5 (-B + sqrt(disc)) / A; points never updated keep their input;
  *   - the binary heap of FMM_Heap.c:118-470 (insert with sift-up, extract
  *     moving the last node into the root's slot and sifting down, update
  *     sifting up when below the parent and down otherwise), with the same
@@ -182,6 +187,7 @@ typedef struct {
   real **ext;
   real **src;
   const real *emask;
+  const real *speed; /* the Eikonal solver's speed (NULL: distance function) */
   fheap trial;
 } march_t;
 
@@ -237,11 +243,16 @@ static real trial_update(march_t *m, long o, const int c[3]) {
   }
   if (fabs(A) == 0) return REAL_MAX;
   B *= -2.0;
-  C -= 1.0;
+  if (m->speed)
+    C -= 1 / m->speed[o] / m->speed[o];
+  else
+    C -= 1.0;
   real disc = B * B - 4.0 * A * C;
   real out;
   if (disc >= 0) {
-    if (B == 0)
+    if (m->speed)
+      out = 0.5 * (-B + sqrt(disc)) / A;
+    else if (B == 0)
       out = 0;
     else if (B < ZERO_TOL)
       out = 0.5 * (-B + sqrt(disc)) / A;
@@ -310,6 +321,7 @@ int orc_computeExtensionFields3d(real *distance, real **ext, const real *phi, co
   m.ext = ext;
   m.src = src;
   m.emask = emask;
+  m.speed = NULL;
   for (int q = 0; q < 3; q++) {
     m.n[q] = grid_dims[q];
     m.dx[q] = dx[q];
@@ -420,4 +432,65 @@ int orc_computeDistanceFunction3d(real *distance, const real *phi, const real *m
                                   const int *grid_dims, const real *dx) {
   return orc_computeExtensionFields3d(distance, NULL, phi, mask, NULL, NULL, 0, order,
                                       grid_dims, dx);
+}
+
+/* orc_solveEikonalEquation3d: the reference's solveEikonalEquation3d; phi is
+ * the boundary data on input (the front: phi > -1e-11) and the solution on
+ * output.  Returns 0, or 2 for an order other than 1 and 2. */
+int orc_solveEikonalEquation3d(real *phi, const real *speed, const real *mask, int order,
+                               const int *grid_dims, const real *dx) {
+  if (order != 1 && order != 2) return 2;
+  march_t m;
+  m.d = phi;
+  m.phi = phi;
+  m.order = order;
+  m.nf = 0;
+  m.ext = NULL;
+  m.src = NULL;
+  m.emask = NULL;
+  m.speed = speed;
+  for (int q = 0; q < 3; q++) {
+    m.n[q] = grid_dims[q];
+    m.dx[q] = dx[q];
+  }
+  m.s[0] = 1;
+  m.s[1] = m.n[0];
+  m.s[2] = (long)m.n[0] * m.n[1];
+  long np = m.s[2] * m.n[2];
+  m.st = (unsigned char *)calloc((size_t)np, 1);
+  m.handle = (int *)malloc(sizeof(int) * (size_t)np);
+  for (long o = 0; o < np; o++) {
+    m.handle[o] = -1;
+    if ((mask && mask[o] < 0) || speed[o] < ZERO_TOL) {
+      m.st[o] = OUTSIDE;
+      phi[o] = REAL_MAX;
+    }
+  }
+  fheap known;
+  h_init(&known, m.n[0] + m.n[1] + m.n[2]);
+  h_init(&m.trial, m.n[0] + m.n[1] + m.n[2]);
+  for (long o = 0; o < np; o++)
+    if (phi[o] > -ZERO_TOL && m.st[o] != OUTSIDE) {
+      m.st[o] = KNOWN;
+      h_insert(&known, o, phi[o]);
+    }
+  while (known.size > 0) {
+    long mi;
+    int mh;
+    hnode nd = h_extract(&known, &mi, &mh);
+    if (nd.value < REAL_MAX) update_neighbors(&m, nd.idx);
+  }
+  while (m.trial.size > 0) {
+    long mi;
+    int mh;
+    hnode nd = h_extract(&m.trial, &mi, &mh);
+    if (mh != -1) m.handle[mi] = mh;
+    m.st[nd.idx] = KNOWN;
+    update_neighbors(&m, nd.idx);
+  }
+  h_free(&known);
+  h_free(&m.trial);
+  free(m.st);
+  free(m.handle);
+  return 0;
 }

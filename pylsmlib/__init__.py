@@ -8,9 +8,10 @@ the torch-facing front door of the GPU library:
 * :class:`LevelSetIntegrator` -- fused TVD-RK3 time stepping of CUDA tensors
   (normal speed with reinitialization, external velocity, the deformation
   field, reinitialization alone), on torch's current stream;
-* :func:`computeDistanceFunction` / :func:`computeExtensionFields` -- the
-  reference pylsmlib's signed distance function and extension fields (fast
-  marching values, computed on the GPU), 1D to 3D;
+* :func:`computeDistanceFunction` / :func:`computeExtensionFields` /
+  :func:`solveEikonalEquation` / :func:`travel_time` -- the reference
+  pylsmlib's fast marching routines (its values, computed on the GPU), 1D
+  to 3D;
 * :func:`write_data_array` / :func:`read_data_array` -- the serial
   package's data-array files (dims header, x-fastest values, gzip/bzip2);
 * :class:`LevelSetAdvectionLoss` / :func:`advection_loss` -- a
@@ -21,6 +22,7 @@ PyTorch is used only in this package.
 """
 from .adjoint import LevelSetAdvectionLoss, advection_loss  # noqa: F401
 from .levelset import Grid, LevelSetIntegrator  # noqa: F401
-from .distance import computeDistanceFunction, computeExtensionFields  # noqa: F401
+from .distance import (computeDistanceFunction, computeExtensionFields,  # noqa: F401
+                       solveEikonalEquation, travel_time)
 from .data_arrays import (BZIP2, GZIP, NO_ZIP, read_data_array,  # noqa: F401
                           write_data_array)

@@ -1,6 +1,7 @@
-"""Signed distance functions and extension fields on the GPU (the reference
-pylsmlib's ``computeDistanceFunction`` and ``computeExtensionFields``,
-pylsmlib/pylsmlib/__init__.py:27-146).
+"""Signed distance functions, extension fields and Eikonal solutions on the
+GPU (the reference pylsmlib's ``computeDistanceFunction``,
+``computeExtensionFields``, ``solveEikonalEquation`` and ``travel_time``,
+pylsmlib/pylsmlib/__init__.py:27-183, lsmlib.pyx:10-120).
 
 ``computeDistanceFunction(phi0, dx, order)`` returns the distance function of
 the zero level set of ``phi0`` with the values of the reference's fast
@@ -103,3 +104,34 @@ def computeExtensionFields(phi0, speed, dx=1.0, order=2, mask=None, ext_mask=Non
                                        gd, h, None)
     gpu.check_rc(rc, "extension_fields3d")
     return dist, np.stack(ext).reshape(u0shape)
+
+
+def solveEikonalEquation(phi0, speed, dx=1.0, order=2):
+    """phi with |grad phi| speed = 1 and phi = 0 where phi0 = 0, as the
+    reference's Python wrapper computes it: the region phi0 <= 0 (shifted
+    by -min(phi0)) is the boundary data, the rest is solved for
+    (solveEikonalEquation3d), and the shift is undone (lsmlib.pyx:98-120)."""
+    phi = np.array(np.asarray(phi0, dtype=np.float64), order="C", copy=True)
+    if phi.ndim not in (1, 2, 3):
+        raise ValueError("phi0 must be 1D, 2D or 3D")
+    dims, spacing = _dims_dx(phi.shape, dx)
+    if order not in (1, 2):
+        raise ValueError("order must be 1 or 2")
+    f = np.ascontiguousarray(np.asarray(speed, dtype=np.float64))
+    if f.shape != phi.shape:
+        raise ValueError("phi and speed must have the same shape")
+    minphi = phi.min()
+    phi[phi > 0] = minphi - 1.0
+    phi -= minphi
+    lib = gpu.load()
+    gd = (ctypes.c_int * 3)(*dims)
+    h = (ctypes.c_double * 3)(*spacing)
+    rc = lib.lsmgpu_eikonal3d(phi.ctypes.data, f.ctypes.data, None, int(order), gd, h, None)
+    gpu.check_rc(rc, "eikonal3d")
+    phi += minphi
+    return phi
+
+
+def travel_time(phi0, speed, dx=1.0, order=2):
+    """|solveEikonalEquation(phi0, speed, dx, order)|."""
+    return abs(solveEikonalEquation(phi0, speed, dx, order))

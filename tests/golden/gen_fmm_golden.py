@@ -2,8 +2,10 @@
 marching method (its C sources built by ``make -C oracle ref`` into
 oracle/_ref/libfmm.so): computeDistanceFunction3d on seeded unions of spheres
 (anisotropic spacing, with and without a mask, 3D and 2D), orders 1 and 2,
-and computeExtensionFields3d on the same cases with two seeded source fields
-(and an extension mask in the masked case).
+computeExtensionFields3d on the same cases with two seeded source fields
+(and an extension mask in the masked case), and solveEikonalEquation3d with
+the region phi <= 0 as boundary data (shifted as the reference's Python
+wrapper does) and a seeded speed (a zero-speed wall in the masked case).
 
     make -C oracle ref && python tests/golden/gen_fmm_golden.py
 """
@@ -57,9 +59,21 @@ def sources(name, phi, mask):
     return src, emask
 
 
+def eikonal_case(name, phi, mask):
+    """Boundary data (the reference Python wrapper's shift of phi) and speed."""
+    minphi = phi.min()
+    data = np.where(phi > 0, minphi - 1.0, phi) - minphi
+    x = np.linspace(0.0, 1.0, phi.size).reshape(phi.shape)
+    speed = np.round(64 * (1.0 + 0.5 * np.sin(40 * x))) / 64   # compresses
+    if mask is not None:
+        speed[:, 12:14, :] = 0.0          # a wall the front cannot cross
+    return data, speed
+
+
 def main():
     fmm = oracle.reference_fmm()
     ext = oracle.reference_extension()
+    eik = oracle.reference_eikonal()
     blobs = {}
     for name, phi, h, mask in cases():
         blobs[name + "|phi"] = phi
@@ -79,6 +93,9 @@ def main():
                                   blobs["%s|out%d" % (name, order)].view(np.uint64))
             for k, f in enumerate(fields):
                 blobs["%s|ext%d_%d" % (name, order, k)] = f
+        data, speed = eikonal_case(name, phi, mask)    # recomputed by the tests
+        for order in (1, 2):
+            blobs["%s|eik%d" % (name, order)] = eik(data, speed, order, h[::-1], mask)
     np.savez_compressed(OUT, **blobs)
     print("wrote %s (%.1f KB)" % (OUT, os.path.getsize(OUT) / 1024))
 

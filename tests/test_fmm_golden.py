@@ -6,7 +6,8 @@
 * The C restatement of the heap march (oracle/fmm_oracle.c) reproduces the
   same golden outputs, and the reference's results on seeded noisy unions of
   spheres, bit for bit (these pin the restatement).
-* The same for the extension fields (computeExtensionFields3d).
+* The same for the extension fields (computeExtensionFields3d) and the
+  Eikonal solver (solveEikonalEquation3d).
 """
 import os
 
@@ -154,6 +155,57 @@ def test_oracle_extension_matches_reference(shape, seed, order):
     b = oracle.oracle_extension()(phi, src, order, dx, mask, emask)
     for x, y in zip([a[0]] + a[1], [b[0]] + b[1]):
         assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
+
+
+def eik_case(z, name):
+    """Boundary data, speed and mask of a golden Eikonal case."""
+    from gen_fmm_golden import eikonal_case
+    phi, _, mask = _case(z, name)
+    data, speed = eikonal_case(name, phi, mask)
+    return data, speed, mask
+
+
+def seeded_eikonal(shape, seed):
+    """Boundary data (phi <= 0 of seeded spheres, shifted as the reference's
+    Python wrapper does), a speed with a zero-speed slab, dx."""
+    sdf, dx = seeded_spheres(shape, seed, noise=0.0)
+    minphi = sdf.min()
+    data = np.where(sdf > 0, minphi - 1.0, sdf) - minphi
+    x = np.linspace(0.0, 1.0, sdf.size).reshape(shape)
+    speed = 1.0 + 0.5 * np.sin(40 * x)
+    if shape[1] > 44:
+        speed[:, 40:44, :] = 0.0
+    return data, speed, dx
+
+
+@pytest.mark.skipif(not oracle.fmm_available(), reason="oracle/_ref/libfmm.so not built")
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_reference_eikonal_reproduces_golden(name, order):
+    z = np.load(GOLDEN)
+    data, speed, mask = eik_case(z, name)
+    got = oracle.reference_eikonal()(data, speed, order, z[name + "|dx"][::-1], mask)
+    assert np.array_equal(got.view(np.uint64), z["%s|eik%d" % (name, order)].view(np.uint64))
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_oracle_eikonal_reproduces_golden(name, order):
+    z = np.load(GOLDEN)
+    data, speed, mask = eik_case(z, name)
+    got = oracle.oracle_eikonal()(data, speed, order, z[name + "|dx"][::-1], mask)
+    assert np.array_equal(got.view(np.uint64), z["%s|eik%d" % (name, order)].view(np.uint64))
+
+
+@pytest.mark.skipif(not oracle.fmm_available(), reason="oracle/_ref/libfmm.so not built")
+@pytest.mark.parametrize("shape,seed", [((33, 41, 29), 1), ((20, 64, 48), 2), ((1, 50, 60), 3)])
+@pytest.mark.parametrize("order", [1, 2])
+def test_oracle_eikonal_matches_reference(shape, seed, order):
+    data, speed, dx = seeded_eikonal(shape, seed)
+    mask = seeded_mask(shape, seed)
+    a = oracle.reference_eikonal()(data, speed, order, dx, mask)
+    b = oracle.oracle_eikonal()(data, speed, order, dx, mask)
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
 
 
 @pytest.mark.parametrize("name", NAMES)

@@ -226,3 +226,72 @@ def test_pylsmlib_compute_extension_fields():
     assert ext.shape == speed.shape
     for k in range(2):
         assert same_bits(ext[k], want[1][k][0])
+
+
+# ---- Eikonal solver -------------------------------------------------------------
+from test_fmm_golden import eik_case, seeded_eikonal  # noqa: E402
+
+
+def gpu_eikonal(lib, data, speed, order, dx, mask=None):
+    """lsmgpu_eikonal3d on host arrays: the solution (a new array)."""
+    phi = np.array(data, dtype=np.float64, order="C", copy=True)
+    f = np.ascontiguousarray(speed, dtype=np.float64)
+    dims = (ctypes.c_int * 3)(*phi.shape[::-1])
+    h = (ctypes.c_double * 3)(*dx)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float64)
+    rc = lib.lsmgpu_eikonal3d(phi.ctypes.data, f.ctypes.data,
+                              None if m is None else m.ctypes.data, order, dims, h, None)
+    assert rc == 0, lib.lsmgpu_get_last_error_string()
+    return phi
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("order", [1, 2])
+def test_eikonal_reproduces_reference_golden(lib, name, order):
+    z = np.load(GOLDEN)
+    data, speed, mask = eik_case(z, name)
+    got = gpu_eikonal(lib, data, speed, order, z[name + "|dx"][::-1], mask)
+    assert same_bits(got, z["%s|eik%d" % (name, order)])
+
+
+@pytest.mark.parametrize("shape,seed", [((33, 41, 29), 1), ((20, 64, 48), 2), ((1, 80, 90), 3),
+                                        ((64, 64, 64), 4), ((40, 100, 70), 5)])
+@pytest.mark.parametrize("order", [1, 2])
+def test_eikonal_matches_oracle(lib, shape, seed, order):
+    data, speed, dx = seeded_eikonal(shape, seed)
+    mask = seeded_mask(shape, seed)
+    want = oracle.oracle_eikonal()(data, speed, order, dx, mask)
+    got = gpu_eikonal(lib, data, speed, order, dx, mask)
+    assert same_bits(got, want), (np.mean(got == want), np.abs(got - want).max())
+
+
+def test_eikonal_c_abi_entry_point(lib):
+    """solveEikonalEquation3d with the reference's arguments: phi in/out on
+    the device, 2 for a bad order."""
+    import torch
+    data, speed, dx = seeded_eikonal((24, 30, 36), 9)
+    want = oracle.oracle_eikonal()(data, speed, 2, dx)
+    fn = lib.solveEikonalEquation3d
+    P = ctypes.c_void_p
+    fn.restype = ctypes.c_int
+    fn.argtypes = [P, P, P, ctypes.c_int, P, P]
+    tp = torch.from_numpy(np.ascontiguousarray(data)).cuda()
+    tf = torch.from_numpy(np.ascontiguousarray(speed)).cuda()
+    dims = np.array(data.shape[::-1], dtype=np.intc)
+    h = np.array(dx)
+    assert fn(tp.data_ptr(), tf.data_ptr(), None, 2, dims.ctypes.data, h.ctypes.data) == 0
+    assert same_bits(tp.cpu().numpy(), want)
+    assert fn(tp.data_ptr(), tf.data_ptr(), None, 0, dims.ctypes.data, h.ctypes.data) == 2
+
+
+def test_pylsmlib_solve_eikonal_equation():
+    """The Python front door shifts phi as the reference's wrapper does."""
+    from pylsmlib import solveEikonalEquation, travel_time
+    sdf, dx = seeded_spheres((1, 40, 50), 12, noise=0.0)
+    speed = 1.0 + 0.25 * np.cos(np.linspace(0, 7, sdf.size)).reshape(sdf.shape)
+    minphi = sdf.min()
+    data = np.where(sdf > 0, minphi - 1.0, sdf) - minphi
+    want = oracle.oracle_eikonal()(data, speed, 2, dx) + minphi
+    got = solveEikonalEquation(sdf[0], speed[0], dx=[dx[1], dx[0]], order=2)
+    assert same_bits(got, want[0])
+    assert same_bits(travel_time(sdf[0], speed[0], dx=[dx[1], dx[0]]), np.abs(want[0]))
