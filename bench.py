@@ -17,8 +17,9 @@ run), e2e (the same steps through the C ABI with the level set and speed on
 pinned host memory, copied in and out every step), the roofline of the
 dominant kernel, the CFL-dt kernel count and the reference's CPU toolbox timed
 on this host.  Beside it: the batched, adjoint, deformation and per-routine
-toolbox legs, and the signed-distance leg (fast marching values, 128^3 and
-256^3, against the CPU oracle of the reference's heap march).  Under torchrun every rank runs a replica on its own GPU
+toolbox legs, and the fast marching leg (distance function, extension
+fields and Eikonal solver with the reference's march values, 128^3 and 256^3,
+against the CPU oracle of the reference's heap march).  Under torchrun every rank runs a replica on its own GPU
 (weak scaling, no data-path collective).
 
 ``--impl reference`` times the reference's own toolbox routines (translated
@@ -485,65 +486,130 @@ def run_toolbox(peak, n=256, reps=10):
 
 
 def run_distance(n=256, n_cpu=128, reps=3):
-    """The signed distance function (computeDistanceFunction3d; fast
-    marching values) on workloads.distance_case at n^3 and n_cpu^3, orders 1
-    and 2: device arrays timed with CUDA events (mean of ``reps`` solves),
-    the drop-in entry point on host arrays (copies included), and at n_cpu^3
-    the CPU oracle (the reference's heap march restated in C, one core) with
-    a bit-for-bit comparison."""
+    """The fast marching routines on workloads.distance_case at n^3 and
+    n_cpu^3, orders 1 and 2: the signed distance function
+    (computeDistanceFunction3d), three extension fields
+    (computeExtensionFields3d) and the Eikonal solution
+    (solveEikonalEquation3d, the region phi <= 0 as boundary data).  Device
+    arrays timed with CUDA events (mean of ``reps`` solves), the drop-in entry
+    point on host arrays (copies included), and at n_cpu^3 the CPU oracle
+    (the reference's heap march restated in C, one core) with a bit-for-bit
+    comparison."""
     import oracle
     from lsmlib_b200 import gpu, workloads
     lib = gpu.load()
-    fn = lib.computeDistanceFunction3d
-    fn.restype = ctypes.c_int
-    fn.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    P = ctypes.c_void_p
+    drop_in = {"distance": lib.computeDistanceFunction3d,
+               "extension": lib.computeExtensionFields3d,
+               "eikonal": lib.solveEikonalEquation3d}
+    drop_in["distance"].argtypes = [P] * 3 + [ctypes.c_int, P, P]
+    drop_in["extension"].argtypes = [P] * 6 + [ctypes.c_int, ctypes.c_int, P, P]
+    drop_in["eikonal"].argtypes = [P] * 3 + [ctypes.c_int, P, P]
+    for f in drop_in.values():
+        f.restype = ctypes.c_int
     timer = gpu.Timer()
     out = {"workload": "config-2 union of 6 spheres on [-1,1]^3, scaled by "
-                       "1.2 + 0.5 sin(3 pi x) sin(2 pi y) cos(pi z) (same zero set)",
+                       "1.2 + 0.5 sin(3 pi x) sin(2 pi y) cos(pi z) (same zero set); "
+                       "extension: 3 source fields; eikonal: phi <= 0 (shifted by "
+                       "-min phi) as boundary data, speed 1 + 0.5 sin(6x) cos(4y)",
            "unit": "grid points/s", "sizes": {}}
     for size in (n_cpu, n):
         phi, dx = workloads.distance_case(size)
+        a = np.linspace(-1.0, 1.0, size)
+        srcs = [np.asfortranarray(np.broadcast_to(v, phi.shape)) for v in
+                (a[:, None, None] + 0 * a[None, :, None],
+                 np.sin(3 * a)[None, :, None] + 0 * a[:, None, None],
+                 np.cos(2 * a)[None, None, :] + 0 * a[:, None, None])]
+        speed = np.asfortranarray(1.0 + 0.5 * np.sin(6 * a)[:, None, None] *
+                                  np.cos(4 * a)[None, :, None] + 0 * a[None, None, :])
+        minphi = phi.min()
+        eik_data = np.asfortranarray(np.where(phi > 0, minphi - 1.0, phi) - minphi)
         pts = size ** 3
         d_phi = gpu.DeviceArray.from_host(phi)
         d_out = gpu.DeviceArray(phi.shape)
+        d_src = [gpu.DeviceArray.from_host(x) for x in srcs]
+        d_ext = [gpu.DeviceArray(phi.shape) for _ in srcs]
+        d_speed = gpu.DeviceArray.from_host(speed)
+        d_eik0 = gpu.DeviceArray.from_host(eik_data)
         dims = (ctypes.c_int * 3)(size, size, size)
         h = (ctypes.c_double * 3)(*dx)
         hd = np.ascontiguousarray(np.array(dx))
         hdims = np.array([size] * 3, dtype=np.intc)
+        ext_p = (ctypes.c_void_p * 3)(*[x.ptr for x in d_ext])
+        src_p = (ctypes.c_void_p * 3)(*[x.ptr for x in d_src])
         entry = {}
-        for order in (1, 2):
-            passes = ctypes.c_int(0)
-            gpu.check_rc(lib.lsmgpu_distance_function3d(d_out.ptr, d_phi.ptr, None, order, dims,
-                                                        h, ctypes.byref(passes)), "distance")
-            timer.start()
-            for _ in range(reps):
-                lib.lsmgpu_distance_function3d(d_out.ptr, d_phi.ptr, None, order, dims, h, None)
-            timer.stop()
-            ms = timer.ms() / reps
-            host_out = np.zeros_like(phi)
-            t_e2e = float("inf")
-            for _ in range(2):      # best of two: the first may grow the memory pool
-                t0 = time.perf_counter()
-                rc = fn(host_out.ctypes.data, phi.ctypes.data, None, order, hdims.ctypes.data,
-                        hd.ctypes.data)
-                t_e2e = min(t_e2e, time.perf_counter() - t0)
-            r = {"ms": round(ms, 2), "value": pts / (ms / 1e3), "passes": passes.value,
-                 "e2e": {"ms": round(1e3 * t_e2e, 2), "value": pts / t_e2e, "rc": rc,
-                         "path": "computeDistanceFunction3d on host arrays (copies "
-                                 "included), best of 2 calls"}}
-            if size == n_cpu:
-                t0 = time.perf_counter()
-                want = oracle.oracle_fmm()(phi.T, order, dx)
-                t_cpu = time.perf_counter() - t0
-                got = d_out.download()
-                r["cpu_oracle"] = {"ms": round(1e3 * t_cpu, 1), "value": pts / t_cpu,
-                                   "cores": 1, "kind": "port"}
-                r["bitwise_vs_oracle"] = bool(np.array_equal(got.T.view(np.uint64),
-                                                              want.view(np.uint64)))
-            entry["order%d" % order] = r
+        for solver in ("distance", "extension", "eikonal"):
+            for order in (1, 2):
+                passes = ctypes.c_int(0)
+
+                def device_solve(pp=None):
+                    # the Eikonal solver overwrites its boundary data: restore it
+                    # (outside the timed region)
+                    if solver == "eikonal":
+                        lib.lsmgpu_memcpy_dtod(d_out.ptr, d_eik0.ptr, d_out.nbytes)
+                    timer.start()
+                    if solver == "distance":
+                        rc = lib.lsmgpu_distance_function3d(d_out.ptr, d_phi.ptr, None, order,
+                                                            dims, h, pp)
+                    elif solver == "extension":
+                        rc = lib.lsmgpu_extension_fields3d(d_out.ptr, ctypes.cast(ext_p, P),
+                                                           d_phi.ptr, None,
+                                                           ctypes.cast(src_p, P), None, 3,
+                                                           order, dims, h, pp)
+                    else:
+                        rc = lib.lsmgpu_eikonal3d(d_out.ptr, d_speed.ptr, None, order, dims, h,
+                                                  pp)
+                    timer.stop()
+                    return rc, timer.ms()
+                gpu.check_rc(device_solve(ctypes.byref(passes))[0], solver)
+                ms = sum(device_solve()[1] for _ in range(reps)) / reps
+                # the drop-in entry point on host arrays
+                host = np.zeros_like(phi)
+                hext = [np.zeros_like(phi) for _ in srcs]
+                hext_p = (ctypes.c_void_p * 3)(*[x.ctypes.data for x in hext])
+                hsrc_p = (ctypes.c_void_p * 3)(*[x.ctypes.data for x in srcs])
+                t_e2e = float("inf")
+                for _ in range(2):      # best of two: the first may grow the memory pool
+                    if solver == "eikonal":
+                        host[...] = eik_data
+                    t0 = time.perf_counter()
+                    if solver == "distance":
+                        rc = drop_in[solver](host.ctypes.data, phi.ctypes.data, None, order,
+                                             hdims.ctypes.data, hd.ctypes.data)
+                    elif solver == "extension":
+                        rc = drop_in[solver](host.ctypes.data, ctypes.cast(hext_p, P),
+                                             phi.ctypes.data, None, ctypes.cast(hsrc_p, P),
+                                             None, 3, order, hdims.ctypes.data, hd.ctypes.data)
+                    else:
+                        rc = drop_in[solver](host.ctypes.data, speed.ctypes.data, None, order,
+                                             hdims.ctypes.data, hd.ctypes.data)
+                    t_e2e = min(t_e2e, time.perf_counter() - t0)
+                r = {"ms": round(ms, 2), "value": pts / (ms / 1e3), "passes": passes.value,
+                     "e2e": {"ms": round(1e3 * t_e2e, 2), "value": pts / t_e2e, "rc": rc,
+                             "path": "the reference's entry point on host arrays (copies "
+                                     "included), best of 2 calls"}}
+                if size == n_cpu:
+                    t0 = time.perf_counter()
+                    if solver == "distance":
+                        want = [oracle.oracle_fmm()(phi.T, order, dx)]
+                    elif solver == "extension":
+                        dist, fields = oracle.oracle_extension()(phi.T, [x.T for x in srcs],
+                                                                 order, dx)
+                        want = [dist] + fields
+                    else:
+                        want = [oracle.oracle_eikonal()(eik_data.T, speed.T, order, dx)]
+                    t_cpu = time.perf_counter() - t0
+                    got = [host.T] + ([x.T for x in hext] if solver == "extension" else [])
+                    r["cpu_oracle"] = {"ms": round(1e3 * t_cpu, 1), "value": pts / t_cpu,
+                                       "cores": 1, "kind": "port"}
+                    r["bitwise_vs_oracle"] = all(
+                        np.array_equal(np.ascontiguousarray(x).view(np.uint64),
+                                       np.ascontiguousarray(y).view(np.uint64))
+                        for x, y in zip(got, want))
+                entry["%s_order%d" % (solver, order)] = r
         out["sizes"]["%d^3" % size] = entry
-        d_phi.free()
-        d_out.free()
+        for x in [d_phi, d_out, d_speed, d_eik0] + d_src + d_ext:
+            x.free()
     return out
 
 
@@ -851,7 +917,7 @@ def main():
     ap.add_argument("--no-toolbox", action="store_true",
                     help="skip the per-routine drop-in timings")
     ap.add_argument("--no-distance", action="store_true",
-                    help="skip the signed-distance (fast marching) leg")
+                    help="skip the fast marching leg (distance, extension fields, Eikonal)")
     ap.add_argument("--no-deformation", action="store_true",
                     help="skip the deformation leg (config 3)")
     ap.add_argument("--config3-full", action="store_true",

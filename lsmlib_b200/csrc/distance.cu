@@ -291,9 +291,9 @@ __device__ __forceinline__ double fmm_root(double A, double B, double disc) {
 // the points whose stencil reads it for the next pass.  A point whose time
 // is above T keeps its time as a candidate and waits in a pending list;
 // when a pass queues nothing, T moves to max(T + delta, smallest
-// candidate) and the pending points it reaches are queued.  Points
-// evaluated in the same pass may read one another mid-update; any change
-// queues the readers again, so the final pass reads settled values.
+// candidate) and the pending points it reaches are queued.  A pass is two
+// kernels: k_fmm_pass evaluates every queued point from the values before
+// the pass, k_fmm_apply stores the changes and queues their readers.
 
 // the threshold advances by this many of the smallest spacing per step
 constexpr double kDeltaCells = 2.0;
@@ -504,6 +504,9 @@ struct Lists {
   int* stamp;                // pass that last queued a point
   int* pending;              // two lists of n points (by epoch parity)
   int* pend_stamp;           // epoch + 1 that last queued a point
+  double* new_d;             // per slot of the active list: the evaluated value,
+  Time3* new_t;              //   time and what to apply (bit 0: evaluated,
+  unsigned char* new_f;      //   bit 1: an extension field changed)
 };
 
 __device__ __forceinline__ void push_once(long p, int stamp_val, int* stamp, int* list,
@@ -532,7 +535,9 @@ __global__ void k_fmm_seed(const unsigned char* st, int nx, int ny, int nz, List
   }
 }
 
-// One pass over the active list (count[pass & 1]).
+// The first half of a pass over the active list (count[pass & 1]): each
+// point's value and time from the values before the pass, into the list's
+// side arrays; rejected points join the pending list.
 template <int ORDER, bool EIK>
 __global__ void __launch_bounds__(128, ORDER == 1 ? 4 : 3)
 k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz,
@@ -542,8 +547,6 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
   const int count = ctrl->count[par];
   const long n = (long)nx * ny * nz;
   const int* cur = L.active + par * n;
-  int* next = L.active + (par ^ 1) * n;
-  int* next_count = &ctrl->count[par ^ 1];
   const int ep = ctrl->epoch;
   int* pend = L.pending + (ep & 1) * n;
   int* pend_count = &ctrl->pend_count[ep & 1];
@@ -554,6 +557,7 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
   unsigned long long minrej = ~0ULL;
   for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < count; w += gridDim.x * blockDim.x) {
     const long o = cur[w];
+    L.new_f[w] = 0;
     if (st[o] != kFree) continue;
     const int c[3] = {(int)(o % nx), (int)((o / nx) % ny), (int)(o / s[2])};
     Stencil nb;
@@ -561,12 +565,14 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
     Time3 tv, trig;
     int incl;
     bool trig_free;
-    if (!fmm_point<ORDER, EIK>(d, tm, st, o, c, nn, s, i2, E, nb, val, tv, incl, trig,
-                               trig_free))
-      continue;
     const double old = d[o];
     bool ext_changed = false;
-    if (!(tv.a <= T)) {
+    if (!fmm_point<ORDER, EIK>(d, tm, st, o, c, nn, s, i2, E, nb, val, tv, incl, trig,
+                               trig_free)) {
+      // no neighbour is reached (any more): no update, the point is unreached
+      val = copysign(INFINITY, old);
+      tv = Time3{INFINITY, INFINITY, INFINITY};
+    } else if (!(tv.a <= T)) {
       // accepted after the threshold: a candidate only, waiting for T
       val = copysign(INFINITY, old);
       push_once(o, ep + 1, L.pend_stamp, pend, pend_count);
@@ -575,11 +581,45 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
     } else if (!EIK && X.nf) {
       ext_changed = fmm_ext<ORDER>(nb, incl, trig, trig_free, val, i2, X, o, s);
     }
-    if (val == old && tequal(tv, tm[o]) && !ext_changed) continue;
+    L.new_d[w] = val;
+    L.new_t[w] = tv;
+    L.new_f[w] = ext_changed ? 3 : 1;
+  }
+  if (minrej != ~0ULL) atomicMin(&ctrl->minrej, minrej);
+}
+
+// The second half of a pass: the values and times evaluated by k_fmm_pass are
+// stored, and the points whose stencil reads a changed point are queued.
+// Evaluating every point of a pass from the values before it (rather than
+// in place, while others change) keeps the passes from cycling: read in
+// place, a half-written neighbour can sustain an oscillation that sequential
+// or synchronous sweeps never enter.
+template <int ORDER>
+__global__ void __launch_bounds__(256)
+k_fmm_apply(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz, Lists L,
+            Ctrl* ctrl) {
+  const int it = ctrl->pass;
+  const int par = it & 1;
+  const int count = ctrl->count[par];
+  const long n = (long)nx * ny * nz;
+  const int* cur = L.active + par * n;
+  int* next = L.active + (par ^ 1) * n;
+  int* next_count = &ctrl->count[par ^ 1];
+  const int nn[3] = {nx, ny, nz};
+  const long s[3] = {1L, (long)nx, (long)nx * ny};
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < count; w += gridDim.x * blockDim.x) {
+    const unsigned char f = L.new_f[w];
+    if (!f) continue;
+    const long o = cur[w];
+    const double val = L.new_d[w];
+    const Time3 tv = L.new_t[w];
+    const double old = d[o];
+    if (val == old && tequal(tv, tm[o]) && !(f & 2)) continue;
     d[o] = val;
     tm[o] = tv;
     if (!(fabs(old) <= DBL_MAX) && !(fabs(val) <= DBL_MAX)) continue;   // invisible
     // queue the free points whose stencil reads this one
+    const int c[3] = {(int)(o % nx), (int)((o / nx) % ny), (int)(o / s[2])};
 #pragma unroll
     for (int q = 0; q < 6; q++) {
       const int dir = q >> 1, sg = (q & 1) ? 1 : -1;
@@ -592,7 +632,6 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
       }
     }
   }
-  if (minrej != ~0ULL) atomicMin(&ctrl->minrej, minrej);
 }
 
 // Between passes (one thread).  Each threshold step has a burst of large
@@ -689,7 +728,7 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
   const long max_passes = 4096 + 32L * (nx + ny + nz);
   unsigned char* status = nullptr;
   Time3* tm = nullptr;
-  Lists L{nullptr, nullptr, nullptr, nullptr};
+  Lists L{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   Ctrl* ctrl = nullptr;
   const size_t un = (size_t)n;
   bool ok = cuda_ok(cudaMallocAsync((void**)&status, un, st), R) &&
@@ -698,6 +737,9 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
             cuda_ok(cudaMallocAsync((void**)&L.pending, 2 * un * sizeof(int), st), R) &&
             cuda_ok(cudaMallocAsync((void**)&L.stamp, un * sizeof(int), st), R) &&
             cuda_ok(cudaMallocAsync((void**)&L.pend_stamp, un * sizeof(int), st), R) &&
+            cuda_ok(cudaMallocAsync((void**)&L.new_d, un * sizeof(double), st), R) &&
+            cuda_ok(cudaMallocAsync((void**)&L.new_t, un * sizeof(Time3), st), R) &&
+            cuda_ok(cudaMallocAsync((void**)&L.new_f, un, st), R) &&
             cuda_ok(cudaMallocAsync((void**)&ctrl, sizeof(Ctrl), st), R);
   Ctrl h_ctrl{};
   h_ctrl.T = delta;
@@ -735,7 +777,7 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
   }
   // a pass touches only the band, so a few blocks per SM cover it; the
   // grid-stride loops take any count
-  const int pass_blocks = 4 * sms, filter_blocks = 2 * sms;
+  const int pass_blocks = 4 * sms, apply_blocks = 2 * sms, filter_blocks = 2 * sms;
   const int batch = 32;
   auto launch_batch = [&](cudaStream_t s) {
     for (int q = 0; q < batch; q++) {
@@ -751,6 +793,10 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
       else
         k_fmm_pass<2, true><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0],
                                                         i2[1], i2[2], L, ctrl, X, E);
+      if (order == 1)
+        k_fmm_apply<1><<<apply_blocks, 256, 0, s>>>(dd, tm, status, nx, ny, nz, L, ctrl);
+      else
+        k_fmm_apply<2><<<apply_blocks, 256, 0, s>>>(dd, tm, status, nx, ny, nz, L, ctrl);
       k_fmm_control<<<1, 32, 0, s>>>(delta, ctrl);
       k_fmm_filter<<<filter_blocks, 256, 0, s>>>(dd, tm, n, L, ctrl);
     }
@@ -779,7 +825,7 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
     if (gexec) ok = cuda_ok(cudaGraphLaunch(gexec, st), R);
     else launch_batch(st);
     launched += batch;
-    launch_counter() += 3 * batch;
+    launch_counter() += 4 * batch;
     ok = ok && cuda_ok(cudaGetLastError(), R) &&
          cuda_ok(cudaMemcpyAsync(&h_ctrl, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st), R) &&
          cuda_ok(cudaStreamSynchronize(st), R);
@@ -796,7 +842,8 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
   }
   if (gexec) cudaGraphExecDestroy(gexec);
   for (void* q : {(void*)status, (void*)tm, (void*)L.active, (void*)L.pending,
-                  (void*)L.stamp, (void*)L.pend_stamp, (void*)ctrl})
+                  (void*)L.stamp, (void*)L.pend_stamp, (void*)L.new_d, (void*)L.new_t,
+                  (void*)L.new_f, (void*)ctrl})
     if (q) cudaFreeAsync(q, st);
   if (passes_out) *passes_out = h_ctrl.pass;
   return ok;
