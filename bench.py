@@ -197,6 +197,23 @@ def run_ours(args, world, rank, local, pg):
     value = world * cells * K / (ms_max / 1e3)
     phi64 = d_phi.download()
 
+    # the two parts of a step separately: reinitialization pseudo-steps, and
+    # physical steps without reinitialization
+    timer.start()
+    ws.reinit(d_phi, fb, dx, cfl=cfg["cfl"], iters=iters, use_phi0=cfg["use_phi0"])
+    timer.stop()
+    ms_re = max_over_ranks(pg, timer.ms())
+    timer.start()
+    ws.normal(d_phi, d_F, fb, dx, cfl=cfg["cfl"], nsteps=interval, step0=1,
+              reinit_interval=10 ** 9, reinit_iters=0, use_phi0=cfg["use_phi0"])
+    timer.stop()
+    ms_no = max_over_ranks(pg, timer.ms())
+    parts = {"reinit_pseudo_step": {"value": world * cells * iters / (ms_re / 1e3),
+                                    "unit": "cell-updates/s",
+                                    "ms_per_pseudo_step": ms_re / iters},
+             "step_without_reinit": {"value": world * cells * interval / (ms_no / 1e3),
+                                     "unit": UNIT, "ms_per_step": ms_no / interval}}
+
     fp32 = None
     if not args.no_fp32:
         # ---- FP32 form beside it -----------------------------------------
@@ -299,6 +316,8 @@ def run_ours(args, world, rank, local, pg):
     batched_res = None
     if not args.no_batched:
         batched_res = run_batched(lib, pg, world)
+        if rank == 0 and world == 1 and not args.no_cpu:
+            batched_res["cpu_baseline"] = cpu_batched_sample()
 
     adjoint_res = None
     if not args.no_adjoint:
@@ -332,7 +351,7 @@ def run_ours(args, world, rank, local, pg):
                    "fp_mode": "fast (FMA, single-reciprocal WENO5 weights; <=1e-12 rel. vs reference)",
                    "l2": "inputs larger than L2 (144 MB per field, 6 fields live)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "fp32": fp32, "batched": batched_res, "adjoint": adjoint_res,
+        "parts": parts, "fp32": fp32, "batched": batched_res, "adjoint": adjoint_res,
         "deformation": deformation_res, "toolbox": toolbox_res, "distance": distance_res,
         "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clk,
@@ -802,6 +821,49 @@ def cpu_baseline_sample(cfg, nz=64):
     return {"value": cells / per_step, "unit": UNIT, "cores": 1, "kind": kind,
             "sample": "256x256x%d slab of the workload: 1 step + 2 reinit pseudo-steps "
                       "(= the reinit share of one step), %.1f s" % (nz, t2 - t0)}
+
+
+_C4_TOOLBOX = None
+
+
+def _c4_step(i):
+    """One external-velocity TVD-RK3 step of config-4 grid ``i`` with the
+    reference's routines (a process-pool task): (cells, seconds)."""
+    global _C4_TOOLBOX
+    from oracle.driver import Grid, Stepper
+    from lsmlib_b200 import workloads
+    if _C4_TOOLBOX is None:
+        _C4_TOOLBOX = reference_toolbox()[0]
+    cfg = workloads.config4()
+    n, dx, vel = cfg["sizes"][i], cfg["dx"][i], cfg["vel"][i]
+    ax, centres, radii = cfg["grids"][i]
+    g = Grid(n, dx=dx)
+    phi = g.field(workloads.union_of_spheres(ax, centres, radii))
+    v = [g.field(np.full(g.shape, c, order="F")) for c in vel]
+    st = Stepper(_C4_TOOLBOX, g, bc="periodic")
+    t0 = time.perf_counter()
+    dt = st.advect_dt(v, cfg["cfl"])
+    st.advect_step(phi, lambda c: v, dt)
+    return n[0] * n[1] * n[2], time.perf_counter() - t0
+
+
+def cpu_batched_sample():
+    """Config 4 on all host cores: independent grids, one process each, the
+    reference's routines; one step of each of the first 4 x cores grids."""
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    grids = list(range(min(256, 4 * cores)))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        pool.map(_c4_step, range(cores))          # start-up and first-touch
+        t0 = time.perf_counter()
+        res = pool.map(_c4_step, grids)
+        wall = time.perf_counter() - t0
+    cells = sum(c for c, _ in res)
+    return {"value": cells / wall, "unit": UNIT, "cores": cores,
+            "kind": reference_toolbox()[1],
+            "sample": "one TVD-RK3 step of each of the first %d config-4 grids (%.1f M "
+                      "cells), one process per core, %.1f s" % (len(grids), cells / 1e6, wall)}
 
 
 def run_reference(args, world, rank):
