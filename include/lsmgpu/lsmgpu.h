@@ -576,6 +576,17 @@ int lsmgpu_normal_tvdrk3(lsmgpu_workspace *ws, void *phi, const void *F,
                          const int fb[6], const double dx[3], double cfl,
                          int nsteps, int step0, int reinit_interval,
                          int reinit_iters, int use_phi0_for_sgn);
+/* lsmgpu_normal_tvdrk3 on phi and F in host memory (pinned or pageable,
+ * over the workspace's ghost box), phi updated in place.  The copies to
+ * the device run in z-slabs while the first step's RHS/CFL pass works on
+ * the slabs already there; the last step's final stage runs slab by slab
+ * with each slab copied back while the next is computed.  The same values
+ * as lsmgpu_normal_tvdrk3 on device copies of the arrays.  Returns when
+ * phi is back in host memory. */
+int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace *ws, void *phi, const void *F,
+                              const int fb[6], const double dx[3], double cfl,
+                              int nsteps, int step0, int reinit_interval,
+                              int reinit_iters, int use_phi0_for_sgn);
 /* iters TVD-RK3 reinitialization pseudo-steps of phi (in place) */
 int lsmgpu_reinit_tvdrk3(lsmgpu_workspace *ws, void *phi, const int fb[6],
                          const double dx[3], double cfl, int iters,

@@ -31,6 +31,13 @@ struct lsmgpu_workspace {
   void* phi2 = nullptr;
   void* rhs = nullptr;
   void* phi0 = nullptr;
+  // lsmgpu_normal_tvdrk3_host: device copies of the host level set and
+  // speed, the stream their slabs are copied on, one event per slab and
+  // direction (created on first use)
+  void* dphi = nullptr;
+  void* dF = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t slab_ev[8] = {};
   double* defo_tab = nullptr;   // deformation sine tables (see stage.cuh)
   size_t defo_len = 0;
   double* scal = nullptr;   // device scalars (kDt, kT, kDtLast, kG0..kG0+2)
@@ -371,9 +378,12 @@ int lsmgpu_workspace_create(lsmgpu_workspace** out, const int gb[6],
 int lsmgpu_workspace_destroy(lsmgpu_workspace* ws) {
   if (!ws) return LSMGPU_SUCCESS;
   void* ps[] = {ws->phi1, ws->phi2, ws->rhs, ws->phi0, ws->defo_tab, ws->scal,
-                ws->partials};
+                ws->partials, ws->dphi, ws->dF};
   for (void* p : ps)
     if (p) cudaFree(p);
+  for (cudaEvent_t e : ws->slab_ev)
+    if (e) cudaEventDestroy(e);
+  if (ws->copy_stream) cudaStreamDestroy(ws->copy_stream);
   delete ws;
   return LSMGPU_SUCCESS;
 }
@@ -677,6 +687,144 @@ int lsmgpu_normal_tvdrk3(lsmgpu_workspace* ws, void* phi, const void* F,
   }
   if (!cuda_ok(cudaGetLastError(), R)) return LSMGPU_ERR_CUDA;
   if (sync_mode() && !cuda_ok(cudaStreamSynchronize(st), R)) return LSMGPU_ERR_CUDA;
+  return LSMGPU_SUCCESS;
+}
+
+// lsmgpu_normal_tvdrk3 on a level set and speed in host memory: phi and F are
+// copied to the workspace's device buffers in kHostSlabs z-slabs while the
+// first step's RHS/CFL pass works through the slabs already there, and the
+// last step's final stage runs slab by slab, each slab copied back while the
+// next is computed.  Returns when phi is back in host memory.
+namespace {
+constexpr int kHostSlabs = 4;
+}
+
+int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
+                              const int fb[6], const double dx[3], double cfl, int nsteps,
+                              int step0, int reinit_interval, int reinit_iters,
+                              int use_phi0_for_sgn) {
+  const char* R = "lsmgpu_normal_tvdrk3_host";
+  FillBox f;
+  if (!common_checks(ws, phi, fb, dx, R, &f)) return lsmgpu_peek_last_error();
+  if (!F) {
+    set_error(LSMGPU_ERR_NULL_POINTER, std::string(R) + ": null speed");
+    return LSMGPU_ERR_NULL_POINTER;
+  }
+  if (nsteps < 1) return LSMGPU_SUCCESS;
+  cudaStream_t st = cur_stream();
+  if (!ws->dphi) {
+    if (!cuda_ok(cudaMalloc(&ws->dphi, ws->bytes), R) ||
+        !cuda_ok(cudaMalloc(&ws->dF, ws->bytes), R) ||
+        !cuda_ok(cudaStreamCreateWithFlags(&ws->copy_stream, cudaStreamNonBlocking), R))
+      return LSMGPU_ERR_CUDA;
+    for (cudaEvent_t& e : ws->slab_ev)
+      if (!cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), R))
+        return LSMGPU_ERR_CUDA;
+  }
+  cudaStream_t cs = ws->copy_stream;
+  const Box& gb = ws->gb;
+  const size_t esz = (size_t)ws->prec;
+  const size_t plane = (size_t)gb.sz() * esz;
+  // fill-box slabs on stage-tile boundaries in z, and the ghost-box planes
+  // each slab owns: [zb[s], zb[s+1]) with the ghost planes below the fill box
+  // in the first and those above it in the last
+  const int ntz = (f.n(2) + kStageTZ - 1) / kStageTZ;
+  const int ns = ntz < kHostSlabs ? ntz : kHostSlabs;
+  int zlo[kHostSlabs + 1];
+  for (int q = 0; q <= ns; q++) zlo[q] = f.lo[2] + (int)((long)q * ntz / ns) * kStageTZ;
+  zlo[ns] = f.hi[2] + 1;
+  int zb[kHostSlabs + 1];
+  for (int q = 0; q <= ns; q++) zb[q] = zlo[q];
+  zb[0] = gb.lo[2];
+  zb[ns] = gb.hi(2) + 1;
+  auto slab_fb = [&](int q) {
+    FillBox s = f;
+    s.lo[2] = zlo[q];
+    s.hi[2] = zlo[q + 1] - 1;
+    return s;
+  };
+  auto copy = [&](void* dst, const void* src, int q, cudaMemcpyKind kind) {
+    const size_t off = (size_t)(zb[q] - gb.lo[2]) * plane;
+    return cudaMemcpyAsync((char*)dst + off, (const char*)src + off,
+                           (size_t)(zb[q + 1] - zb[q]) * plane, kind, cs);
+  };
+  // host -> device, slab by slab, after the work already queued on st
+  if (!cuda_ok(cudaEventRecord(ws->slab_ev[0], st), R) ||
+      !cuda_ok(cudaStreamWaitEvent(cs, ws->slab_ev[0], 0), R))
+    return LSMGPU_ERR_CUDA;
+  for (int q = 0; q < ns; q++) {
+    if (!cuda_ok(copy(ws->dphi, phi, q, cudaMemcpyHostToDevice), R) ||
+        !cuda_ok(copy(ws->dF, F, q, cudaMemcpyHostToDevice), R) ||
+        !cuda_ok(cudaEventRecord(ws->slab_ev[q], cs), R))
+      return LSMGPU_ERR_CUDA;
+  }
+  const double tiny = ws->prec == 8 ? Consts<double>::tiny : (double)Consts<float>::tiny;
+  const int nblk = stage_blocks(f);
+  void* dphi = ws->dphi;
+  bool copied_back = false;
+  for (int s = 0; s < nsteps; s++) {
+    StageArgs a = base_args(ws, f, dx);
+    a.aux[0] = ws->dF;
+    a.rhs_out = ws->rhs;
+    a.phi_s = dphi;
+    if (s == 0) {
+      // RHS/CFL pass of slab q once its planes and the 3 above have arrived
+      int off = 0;
+      for (int q = 0; q < ns; q++) {
+        const int need = q + 1 < ns ? q + 1 : q;
+        if (!cuda_ok(cudaStreamWaitEvent(st, ws->slab_ev[need], 0), R)) return LSMGPU_ERR_CUDA;
+        StageArgs b = a;
+        b.fb = slab_fb(q);
+        b.partials = ws->partials + off;
+        off += stage_blocks(b.fb);
+        if (!cuda_ok(stage(kStageNormalRhs, ws->prec, b, st, ws), R)) return LSMGPU_ERR_CUDA;
+      }
+    } else {
+      a.partials = ws->partials;
+      if (!cuda_ok(stage(kStageNormalRhs, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
+    }
+    k_dt_finish<<<1, 256, 0, st>>>(ws->partials, nblk, cfl, tiny, ws->scal, 0.0);
+    ++launch_counter();
+    if (!cuda_ok(launch_rk(ws->prec, 1, ws->phi1, ws->gb, nullptr, ws->gb, dphi, ws->gb,
+                           ws->rhs, ws->gb, f, 0.0, ws->scal + kDt, st, next_sr_seed(ws)),
+                 R))
+      return LSMGPU_ERR_CUDA;
+    a.partials = ws->partials;
+    a.out = ws->phi2; a.phi_s = ws->phi1; a.phi_n = dphi; a.rk_kind = 32;
+    if (!cuda_ok(stage(kStageNormal, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
+    a.out = dphi; a.phi_s = ws->phi2; a.rk_kind = 33;
+    const bool reinit_now = reinit_interval > 0 && (step0 + s + 1) % reinit_interval == 0;
+    if (s == nsteps - 1 && !reinit_now) {
+      // the final stage slab by slab, each slab's planes copied back at once
+      for (int q = 0; q < ns; q++) {
+        StageArgs b = a;
+        b.fb = slab_fb(q);
+        if (!cuda_ok(stage(kStageNormal, ws->prec, b, st, ws), R) ||
+            !cuda_ok(cudaEventRecord(ws->slab_ev[kHostSlabs + q], st), R) ||
+            !cuda_ok(cudaStreamWaitEvent(cs, ws->slab_ev[kHostSlabs + q], 0), R) ||
+            !cuda_ok(copy(phi, dphi, q, cudaMemcpyDeviceToHost), R))
+          return LSMGPU_ERR_CUDA;
+      }
+      copied_back = true;
+    } else if (!cuda_ok(stage(kStageNormal, ws->prec, a, st, ws), R)) {
+      return LSMGPU_ERR_CUDA;
+    }
+    k_advance_t<<<1, 1, 0, st>>>(ws->scal);
+    ++launch_counter();
+    ws->steps++;
+    if (reinit_now && !reinit_run(ws, dphi, f, dx, cfl, reinit_iters, use_phi0_for_sgn, st, R))
+      return lsmgpu_peek_last_error();
+  }
+  if (!copied_back) {
+    if (!cuda_ok(cudaEventRecord(ws->slab_ev[kHostSlabs], st), R) ||
+        !cuda_ok(cudaStreamWaitEvent(cs, ws->slab_ev[kHostSlabs], 0), R))
+      return LSMGPU_ERR_CUDA;
+    for (int q = 0; q < ns; q++)
+      if (!cuda_ok(copy(phi, dphi, q, cudaMemcpyDeviceToHost), R)) return LSMGPU_ERR_CUDA;
+  }
+  if (!cuda_ok(cudaGetLastError(), R) || !cuda_ok(cudaStreamSynchronize(cs), R) ||
+      !cuda_ok(cudaStreamSynchronize(st), R))
+    return LSMGPU_ERR_CUDA;
   return LSMGPU_SUCCESS;
 }
 

@@ -22,6 +22,7 @@ SIGNATURES = {
     "lsmgpu_advect_tvdrk3": (I, [P, P, P, P, P, IA, DA, D, D, D, I]),
     "lsmgpu_deformation_tvdrk3": (I, [P, P, IA, DA, DA, D, D, D, I]),
     "lsmgpu_normal_tvdrk3": (I, [P, P, P, IA, DA, D, I, I, I, I, I]),
+    "lsmgpu_normal_tvdrk3_host": (I, [P, P, P, IA, DA, D, I, I, I, I, I]),
     "lsmgpu_reinit_tvdrk3": (I, [P, P, IA, DA, D, I, I]),
     "lsmgpu_normal_rhs_dt_noalloc": (I, [P, P, P, P, IA, IA, DA, D]),
     "lsmgpu_distance_function3d": (I, [P, P, P, I, P, P, P]),

@@ -94,6 +94,18 @@ class Workspace:
                                              int(use_phi0))
         gpu.check_rc(rc, "normal_tvdrk3")
 
+    def normal_host(self, phi, F, fb, dx, cfl=0.5, nsteps=1, step0=0,
+                    reinit_interval=0, reinit_iters=0, use_phi0=0):
+        """``normal`` on host arrays (numpy, Fortran order, the workspace's
+        ghost box, or raw host addresses); phi is updated in place."""
+        def addr(a):
+            return a.ctypes.data if hasattr(a, "ctypes") else int(a)
+        rc = gpu.load().lsmgpu_normal_tvdrk3_host(self.h, addr(phi), addr(F), ints(fb),
+                                                  dbls(dx), cfl, int(nsteps), int(step0),
+                                                  int(reinit_interval), int(reinit_iters),
+                                                  int(use_phi0))
+        gpu.check_rc(rc, "normal_tvdrk3_host")
+
     def reinit(self, phi, fb, dx, cfl=0.5, iters=1, use_phi0=0):
         rc = gpu.load().lsmgpu_reinit_tvdrk3(self.h, phi.ptr, ints(fb), dbls(dx), cfl,
                                              int(iters), int(use_phi0))

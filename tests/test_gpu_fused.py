@@ -298,3 +298,35 @@ def test_config1_full_run_strict_matches_oracle():
     finally:
         integrator.set_fp_mode(prev)
     assert same_bits(got, g.interior(ref))
+
+
+@pytest.mark.parametrize("n", [(37, 11, 70), (64, 40, 33), (20, 20, 17)])
+@pytest.mark.parametrize("steps,interval", [(1, 0), (3, 2), (2, 2)])
+def test_normal_host_buffers_match_device_driver(mode, n, steps, interval):
+    """lsmgpu_normal_tvdrk3_host (host phi and F, slab-pipelined copies) gives
+    the device driver's values bit for bit, with and without a
+    reinitialization after the last step."""
+    from lsmlib_b200 import gpu, integrator
+    g = Grid(n, dx=(2.0 / n[0],) * 3)
+    x_lo = (-1.0, -1.0, -1.0)
+    phi0 = np.asfortranarray(spheres(g, x_lo, seed=5))
+    x, y, z = g.centers(x_lo)
+    F = np.asfortranarray(1.0 + 0.2 * np.sin(4 * np.pi * x) * np.sin(4 * np.pi * y) *
+                          np.sin(4 * np.pi * z))
+    ws = integrator.Workspace(g.gb, 8)
+    d = gpu.DeviceArray.from_host(phi0)
+    dF = gpu.DeviceArray.from_host(F)
+    ws.normal(d, dF, g.fb, g.dx, cfl=0.5, nsteps=steps, reinit_interval=interval,
+              reinit_iters=3)
+    want = d.download()
+    ws2 = integrator.Workspace(g.gb, 8)
+    host = phi0.copy(order="F")
+    ws2.normal_host(host, F, g.fb, g.dx, cfl=0.5, nsteps=steps, reinit_interval=interval,
+                    reinit_iters=3)
+    assert same_bits(host, want)
+    # a second call continues from the host state, as two device calls would
+    ws.normal(d, dF, g.fb, g.dx, cfl=0.5, nsteps=1, step0=steps)
+    ws2.normal_host(host, F, g.fb, g.dx, cfl=0.5, nsteps=1, step0=steps)
+    assert same_bits(host, d.download())
+    ws.close()
+    ws2.close()
