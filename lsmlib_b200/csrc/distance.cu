@@ -497,6 +497,7 @@ struct Ctrl {
   unsigned long long minrej; // bits of the smallest candidate queued since
                              // the last advance (times are >= 0)
   unsigned long long minkeep;// bits of the smallest candidate kept waiting
+  int arrived;               // blocks of the current k_fmm_apply that finished
 };
 
 struct Lists {
@@ -542,33 +543,42 @@ template <int ORDER, bool EIK>
 __global__ void __launch_bounds__(128, ORDER == 1 ? 4 : 3)
 k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz,
            double i2x, double i2y, double i2z, Lists L, Ctrl* ctrl, ExtSet X, Eik E) {
+  // the control words are loaded together (no load waits on another)
   const int it = ctrl->pass;
+  const int count0 = ctrl->count[0], count1 = ctrl->count[1];
+  const int ep = ctrl->epoch;
+  const double T = ctrl->T;
   const int par = it & 1;
-  const int count = ctrl->count[par];
+  const int count = par ? count1 : count0;
   const long n = (long)nx * ny * nz;
   const int* cur = L.active + par * n;
-  const int ep = ctrl->epoch;
   int* pend = L.pending + (ep & 1) * n;
   int* pend_count = &ctrl->pend_count[ep & 1];
-  const double T = ctrl->T;
   const double i2[3] = {i2x, i2y, i2z};
   const int nn[3] = {nx, ny, nz};
   const long s[3] = {1L, (long)nx, (long)nx * ny};
   unsigned long long minrej = ~0ULL;
   for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < count; w += gridDim.x * blockDim.x) {
     const long o = cur[w];
-    L.new_f[w] = 0;
-    if (st[o] != kFree) continue;
+    // only free points are ever queued; the status, value and time of the
+    // point itself are loaded beside its stencil
+    const unsigned char self = st[o];
+    const double old = d[o];
+    const Time3 told = tm[o];
     const int c[3] = {(int)(o % nx), (int)((o / nx) % ny), (int)(o / s[2])};
     Stencil nb;
     double val;
     Time3 tv, trig;
     int incl;
     bool trig_free;
-    const double old = d[o];
     bool ext_changed = false;
-    if (!fmm_point<ORDER, EIK>(d, tm, st, o, c, nn, s, i2, E, nb, val, tv, incl, trig,
-                               trig_free)) {
+    const bool reached = fmm_point<ORDER, EIK>(d, tm, st, o, c, nn, s, i2, E, nb, val, tv,
+                                               incl, trig, trig_free);
+    if (self != kFree) {
+      L.new_f[w] = 0;
+      continue;
+    }
+    if (!reached) {
       // no neighbour is reached (any more): no update, the point is unreached
       val = copysign(INFINITY, old);
       tv = Time3{INFINITY, INFINITY, INFINITY};
@@ -581,71 +591,35 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
     } else if (!EIK && X.nf) {
       ext_changed = fmm_ext<ORDER>(nb, incl, trig, trig_free, val, i2, X, o, s);
     }
+    // what k_fmm_apply does with the slot: bit 0 store the value and time,
+    // bit 1 queue the readers (the change is visible: the value is finite
+    // before or after, or an extension field changed)
+    unsigned char f = 0;
+    if (ext_changed || !(val == old && tequal(tv, told))) {
+      f = 1;
+      if (ext_changed || fabs(old) <= DBL_MAX || fabs(val) <= DBL_MAX) f |= 2;
+    }
     L.new_d[w] = val;
     L.new_t[w] = tv;
-    L.new_f[w] = ext_changed ? 3 : 1;
+    L.new_f[w] = f;
   }
   if (minrej != ~0ULL) atomicMin(&ctrl->minrej, minrej);
 }
 
-// The second half of a pass: the values and times evaluated by k_fmm_pass are
-// stored, and the points whose stencil reads a changed point are queued.
-// Evaluating every point of a pass from the values before it (rather than
-// in place, while others change) keeps the passes from cycling: read in
-// place, a half-written neighbour can sustain an oscillation that sequential
-// or synchronous sweeps never enter.
-template <int ORDER>
-__global__ void __launch_bounds__(256)
-k_fmm_apply(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz, Lists L,
-            Ctrl* ctrl) {
-  const int it = ctrl->pass;
-  const int par = it & 1;
-  const int count = ctrl->count[par];
-  const long n = (long)nx * ny * nz;
-  const int* cur = L.active + par * n;
-  int* next = L.active + (par ^ 1) * n;
-  int* next_count = &ctrl->count[par ^ 1];
-  const int nn[3] = {nx, ny, nz};
-  const long s[3] = {1L, (long)nx, (long)nx * ny};
-  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < count; w += gridDim.x * blockDim.x) {
-    const unsigned char f = L.new_f[w];
-    if (!f) continue;
-    const long o = cur[w];
-    const double val = L.new_d[w];
-    const Time3 tv = L.new_t[w];
-    const double old = d[o];
-    if (val == old && tequal(tv, tm[o]) && !(f & 2)) continue;
-    d[o] = val;
-    tm[o] = tv;
-    if (!(fabs(old) <= DBL_MAX) && !(fabs(val) <= DBL_MAX)) continue;   // invisible
-    // queue the free points whose stencil reads this one
-    const int c[3] = {(int)(o % nx), (int)((o / nx) % ny), (int)(o / s[2])};
-#pragma unroll
-    for (int q = 0; q < 6; q++) {
-      const int dir = q >> 1, sg = (q & 1) ? 1 : -1;
-#pragma unroll
-      for (int r = 1; r <= ORDER; r++) {
-        const int cr = c[dir] + r * sg;
-        if (cr < 0 || cr >= nn[dir]) break;
-        const long on = o + r * sg * s[dir];
-        if (st[on] == kFree) push_once(on, it + 2, L.stamp, next, next_count);
-      }
-    }
-  }
-}
-
-// Between passes (one thread).  Each threshold step has a burst of large
-// passes and then a long tail of small ones as the last revisions settle;
-// the threshold need not wait for that tail (the fixed point does not
-// depend on when T moves, only the amount of revision does).  So once the
-// queued points fall to 1/kTailFraction of the step's largest pass, the
-// threshold moves to max(T + delta, smallest waiting candidate) and the
-// pending list is filtered (next kernel) into the queue beside them.  With
-// nothing queued and nothing waiting, the solve is done.
+// Between passes (the last block of k_fmm_apply, one thread).  Each
+// threshold step has a burst of large passes and then a long tail of small
+// ones as the last revisions settle; the threshold need not wait for that
+// tail (the fixed point does not depend on when T moves, only the amount of
+// revision does).  So once the queued points fall to 1/kTailFraction of the
+// step's largest pass, the threshold moves to max(T + delta, smallest
+// waiting candidate) and the pending list is filtered (next kernel) into the
+// queue beside them.  With nothing queued and nothing waiting, the solve is
+// done.  The words are read volatile: other blocks of the same launch wrote
+// the queue length.
 constexpr int kTailFraction = 8;
 
-__global__ void k_fmm_control(double delta, Ctrl* ctrl) {
-  if (threadIdx.x != 0 || ctrl->done) return;
+__device__ void fmm_control(double delta, volatile Ctrl* ctrl) {
+  if (ctrl->done) return;
   const int par = ctrl->pass & 1;
   const int queued = ctrl->count[par ^ 1];
   ctrl->advance = 0;
@@ -656,7 +630,8 @@ __global__ void k_fmm_control(double delta, Ctrl* ctrl) {
     if (np == 0) {
       if (queued == 0) ctrl->done = 1;
     } else {
-      const unsigned long long m = ctrl->minrej < ctrl->minkeep ? ctrl->minrej : ctrl->minkeep;
+      const unsigned long long rej = ctrl->minrej, keep = ctrl->minkeep;
+      const unsigned long long m = rej < keep ? rej : keep;
       const double lo = __longlong_as_double((long long)m);
       const double step = ctrl->T + delta;
       ctrl->T = lo > step ? lo : step;
@@ -670,7 +645,115 @@ __global__ void k_fmm_control(double delta, Ctrl* ctrl) {
     }
   }
   ctrl->count[par] = 0;
-  ctrl->pass += 1;
+  ctrl->pass = ctrl->pass + 1;
+}
+
+// The second half of a pass: the values and times evaluated by k_fmm_pass are
+// stored, and the points whose stencil reads a changed point are queued.
+// Evaluating every point of a pass from the values before it (rather than
+// in place, while others change) keeps the passes from cycling: read in
+// place, a half-written neighbour can sustain an oscillation that sequential
+// or synchronous sweeps never enter.
+//
+// The kernel is a short chain of memory round trips, so it is laid out to
+// keep each round in flight at once: a warp takes 32 consecutive slots; the
+// slot words load together; the readers' statuses load together; their
+// stamps are exchanged together; and the warp reserves its queue entries
+// with one atomic.  The block that finishes last runs the threshold control.
+template <int ORDER>
+__global__ void __launch_bounds__(256)
+k_fmm_apply(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz, Lists L,
+            Ctrl* ctrl, double delta) {
+  constexpr int kReaders = 6 * ORDER;
+  const int it = ctrl->pass;
+  const int count0 = ctrl->count[0], count1 = ctrl->count[1];
+  const int par = it & 1;
+  const int count = par ? count1 : count0;
+  const long n = (long)nx * ny * nz;
+  const int* cur = L.active + par * n;
+  int* next = L.active + (par ^ 1) * n;
+  int* next_count = &ctrl->count[par ^ 1];
+  const int nn[3] = {nx, ny, nz};
+  const long s[3] = {1L, (long)nx, (long)nx * ny};
+  const int lane = threadIdx.x & 31;
+  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  // the loop bound is the same for the 32 lanes of a warp
+  for (int w0 = warp * 32; w0 < count; w0 += nwarps * 32) {
+    const int w = w0 + lane;
+    unsigned char f = 0;
+    long o = 0;
+    double val = 0;
+    Time3 tv{0, 0, 0};
+    if (w < count) {
+      f = L.new_f[w];
+      o = cur[w];
+      val = L.new_d[w];
+      tv = L.new_t[w];
+    }
+    if (f & 1) {
+      d[o] = val;
+      tm[o] = tv;
+    }
+    // the free points whose stencil reads this one
+    long on[kReaders];
+    unsigned won = 0;
+    if (f & 2) {
+      const int c[3] = {(int)(o % nx), (int)((o / nx) % ny), (int)(o / s[2])};
+      unsigned char sn[kReaders];
+      unsigned cand = 0;
+#pragma unroll
+      for (int q = 0; q < 6; q++) {
+        const int dir = q >> 1, sg = (q & 1) ? 1 : -1;
+#pragma unroll
+        for (int r = 1; r <= ORDER; r++) {
+          const int k = q * ORDER + r - 1;
+          const int cr = c[dir] + r * sg;
+          const bool in = cr >= 0 && cr < nn[dir];
+          on[k] = in ? o + r * sg * s[dir] : o;
+          sn[k] = st[on[k]];
+          if (in) cand |= 1u << k;
+        }
+      }
+      int old[kReaders];
+#pragma unroll
+      for (int k = 0; k < kReaders; k++)
+        if ((cand >> k & 1) && sn[k] == kFree) {
+          old[k] = atomicExch(L.stamp + on[k], it + 2);
+          if (old[k] != it + 2) won |= 1u << k;
+        }
+    }
+    // one reservation for the warp's new queue entries
+    const int mine = __popc(won);
+    int upto = mine;
+#pragma unroll
+    for (int sh = 1; sh < 32; sh <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, upto, sh);
+      if (lane >= sh) upto += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, upto, 31);
+    if (total) {
+      int base = 0;
+      if (lane == 31) base = atomicAdd(next_count, total);
+      base = __shfl_sync(0xffffffffu, base, 31);
+      int pos = base + upto - mine;
+#pragma unroll
+      for (int k = 0; k < kReaders; k++)
+        if (won >> k & 1) next[pos++] = (int)on[k];
+    }
+  }
+  // the last block to finish runs the control step
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0)
+    last = atomicAdd(&ctrl->arrived, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    fmm_control(delta, ctrl);
+    ctrl->arrived = 0;
+  }
 }
 
 // After a threshold advance: the pending points the threshold reaches join
@@ -794,10 +877,11 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
         k_fmm_pass<2, true><<<pass_blocks, 128, 0, s>>>(dd, tm, status, nx, ny, nz, i2[0],
                                                         i2[1], i2[2], L, ctrl, X, E);
       if (order == 1)
-        k_fmm_apply<1><<<apply_blocks, 256, 0, s>>>(dd, tm, status, nx, ny, nz, L, ctrl);
+        k_fmm_apply<1><<<apply_blocks, 256, 0, s>>>(dd, tm, status, nx, ny, nz, L, ctrl,
+                                                     delta);
       else
-        k_fmm_apply<2><<<apply_blocks, 256, 0, s>>>(dd, tm, status, nx, ny, nz, L, ctrl);
-      k_fmm_control<<<1, 32, 0, s>>>(delta, ctrl);
+        k_fmm_apply<2><<<apply_blocks, 256, 0, s>>>(dd, tm, status, nx, ny, nz, L, ctrl,
+                                                     delta);
       k_fmm_filter<<<filter_blocks, 256, 0, s>>>(dd, tm, n, L, ctrl);
     }
   };
@@ -825,7 +909,7 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
     if (gexec) ok = cuda_ok(cudaGraphLaunch(gexec, st), R);
     else launch_batch(st);
     launched += batch;
-    launch_counter() += 4 * batch;
+    launch_counter() += 3 * batch;
     ok = ok && cuda_ok(cudaGetLastError(), R) &&
          cuda_ok(cudaMemcpyAsync(&h_ctrl, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st), R) &&
          cuda_ok(cudaStreamSynchronize(st), R);
