@@ -480,6 +480,9 @@ unsigned long long lsmgpu_kernel_launch_count(void);
 /* device memory and copies (on the calling thread's stream) */
 void *lsmgpu_malloc(size_t bytes);
 int lsmgpu_free(void *p);
+/* returns the scratch and staging memory the library keeps mapped between
+ * calls (up to 8 GiB per device) to the driver; waits for the device */
+int lsmgpu_release_scratch(void);
 void *lsmgpu_host_alloc(size_t bytes); /* page-locked host memory */
 int lsmgpu_host_free(void *p);
 int lsmgpu_memcpy_htod(void *dst, const void *src, size_t bytes);

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "capi_common.h"
@@ -97,6 +98,46 @@ bool covers(const Box& b, const FillBox& fb, int w, const char* what,
 }
 
 // ---------------------------------------------------------------------------
+// scratch pool
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kMaxDevices = 64;
+// freed memory the pool keeps mapped between calls (the distance function
+// of a 256^3 grid takes 1.4 GB of scratch)
+constexpr unsigned long long kRetainBytes = 8ULL << 30;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxDevices] = {};
+
+cudaMemPool_t device_pool(int dev) {
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    unsigned long long keep = kRetainBytes;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pool[dev] = pool;
+  }
+  return g_pool[dev];
+}
+}  // namespace
+
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t st) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  cudaMemPool_t pool = dev >= 0 && dev < kMaxDevices ? device_pool(dev) : nullptr;
+  // the device's default pool when no pool of our own can be made
+  return pool ? cudaMallocFromPoolAsync(p, bytes, pool, st) : cudaMallocAsync(p, bytes, st);
+}
+
+// ---------------------------------------------------------------------------
 // staging
 // ---------------------------------------------------------------------------
 bool is_device_pointer(const void* p) {
@@ -123,14 +164,16 @@ void* Staging::add(const void* p, const Box& b, int elem, Role role,
   } else {
     it.staged = true;
     staged_ = true;
-    if (!cuda_ok(cudaMallocAsync(&it.dev, it.bytes, st_), "cudaMallocAsync")) {
+    if (!cuda_ok(pool_alloc(&it.dev, it.bytes, st_), "cudaMallocFromPoolAsync")) {
       set_error(LSMGPU_ERR_ALLOC, std::string(routine) +
                                       ": cannot allocate staging buffer for " +
                                       what);
       return nullptr;
     }
-    // outputs are copied in too: cells outside the fill box keep their values
-    if (!cuda_ok(cudaMemcpyAsync(it.dev, it.host, it.bytes,
+    // outputs are copied in too (cells outside the fill box keep their
+    // values), unless the routine writes every cell
+    if (role != kOutFull &&
+        !cuda_ok(cudaMemcpyAsync(it.dev, it.host, it.bytes,
                                  cudaMemcpyHostToDevice, st_),
                  "cudaMemcpyAsync(H2D)")) {
       cudaFreeAsync(it.dev, st_);
@@ -165,8 +208,7 @@ Staging::~Staging() {
 }
 
 ReduceScratch::ReduceScratch(cudaStream_t st, int n) : st_(st), n_(n) {
-  if (cudaMallocAsync((void**)&p_, sizeof(double) * (size_t)(n + 1), st) !=
-      cudaSuccess) {
+  if (pool_alloc((void**)&p_, sizeof(double) * (size_t)(n + 1), st) != cudaSuccess) {
     cudaGetLastError();
     p_ = nullptr;
     set_error(LSMGPU_ERR_ALLOC, "cannot allocate reduction scratch");
@@ -907,6 +949,13 @@ void* lsmgpu_malloc(size_t bytes) {
 }
 int lsmgpu_free(void* p) {
   return cuda_ok(cudaFree(p), "cudaFree") ? LSMGPU_SUCCESS : LSMGPU_ERR_CUDA;
+}
+int lsmgpu_release_scratch(void) {
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  bool ok = cuda_ok(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+  for (int d = 0; d < kMaxDevices; d++)
+    if (g_pool[d]) ok = cuda_ok(cudaMemPoolTrimTo(g_pool[d], 0), "cudaMemPoolTrimTo") && ok;
+  return ok ? LSMGPU_SUCCESS : LSMGPU_ERR_CUDA;
 }
 void* lsmgpu_host_alloc(size_t bytes) {
   void* p = nullptr;

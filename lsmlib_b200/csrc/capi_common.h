@@ -35,8 +35,16 @@ bool covers(const Box& b, const FillBox& fb, int w, const char* what,
 bool covers3(const Box& b, const FillBox& fb, const int w[3], const char* what,
              const char* routine);
 
+// ---- device scratch -----------------------------------------------------------
+// Stream-ordered allocation from the library's own memory pool on the
+// current device.  Freed blocks stay mapped in the pool (up to a bound) for
+// the next call, so a call that is repeated does not map its scratch again;
+// lsmgpu_release_scratch() returns them to the driver.
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t st);
+
 // ---- staging ----------------------------------------------------------------
-enum Role { kIn = 1, kOut = 2, kInOut = 3 };
+// kOutFull: an output the routine writes completely (no copy in)
+enum Role { kIn = 1, kOut = 2, kInOut = 3, kOutFull = 6 };
 
 bool is_device_pointer(const void* p);
 

@@ -814,16 +814,16 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
   Lists L{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   Ctrl* ctrl = nullptr;
   const size_t un = (size_t)n;
-  bool ok = cuda_ok(cudaMallocAsync((void**)&status, un, st), R) &&
-            cuda_ok(cudaMallocAsync((void**)&tm, un * sizeof(Time3), st), R) &&
-            cuda_ok(cudaMallocAsync((void**)&L.active, 2 * un * sizeof(int), st), R) &&
-            cuda_ok(cudaMallocAsync((void**)&L.pending, 2 * un * sizeof(int), st), R) &&
-            cuda_ok(cudaMallocAsync((void**)&L.stamp, un * sizeof(int), st), R) &&
-            cuda_ok(cudaMallocAsync((void**)&L.pend_stamp, un * sizeof(int), st), R) &&
-            cuda_ok(cudaMallocAsync((void**)&L.new_d, un * sizeof(double), st), R) &&
-            cuda_ok(cudaMallocAsync((void**)&L.new_t, un * sizeof(Time3), st), R) &&
-            cuda_ok(cudaMallocAsync((void**)&L.new_f, un, st), R) &&
-            cuda_ok(cudaMallocAsync((void**)&ctrl, sizeof(Ctrl), st), R);
+  bool ok = cuda_ok(pool_alloc((void**)&status, un, st), R) &&
+            cuda_ok(pool_alloc((void**)&tm, un * sizeof(Time3), st), R) &&
+            cuda_ok(pool_alloc((void**)&L.active, 2 * un * sizeof(int), st), R) &&
+            cuda_ok(pool_alloc((void**)&L.pending, 2 * un * sizeof(int), st), R) &&
+            cuda_ok(pool_alloc((void**)&L.stamp, un * sizeof(int), st), R) &&
+            cuda_ok(pool_alloc((void**)&L.pend_stamp, un * sizeof(int), st), R) &&
+            cuda_ok(pool_alloc((void**)&L.new_d, un * sizeof(double), st), R) &&
+            cuda_ok(pool_alloc((void**)&L.new_t, un * sizeof(Time3), st), R) &&
+            cuda_ok(pool_alloc((void**)&L.new_f, un, st), R) &&
+            cuda_ok(pool_alloc((void**)&ctrl, sizeof(Ctrl), st), R);
   Ctrl h_ctrl{};
   h_ctrl.T = delta;
   h_ctrl.minrej = 0x7ff0000000000000ULL;   // +infinity
@@ -974,7 +974,7 @@ int extension3d(double* distance, double** ext, const double* phi, const double*
   cudaStream_t st = cur_stream();
   Staging stg(st);
   const Box b{{0, 0, 0}, {nx, ny, nz}};
-  double* dd = (double*)stg.add(distance, b, 8, kOut, "distance_function", R);
+  double* dd = (double*)stg.add(distance, b, 8, kOutFull, "distance_function", R);
   const double* dp = dd ? (const double*)stg.add(phi, b, 8, kIn, "phi", R) : nullptr;
   const double* dm = nullptr;
   if (dp && mask) dm = (const double*)stg.add(mask, b, 8, kIn, "mask", R);
@@ -987,7 +987,7 @@ int extension3d(double* distance, double** ext, const double* phi, const double*
     X.emask = dem;
     X.nf = nf - group < kMaxFields ? nf - group : kMaxFields;
     for (int k = 0; k < X.nf; k++) {
-      X.ext[k] = (double*)stg.add(ext[group + k], b, 8, kOut, "extension_field", R);
+      X.ext[k] = (double*)stg.add(ext[group + k], b, 8, kOutFull, "extension_field", R);
       X.src[k] = X.ext[k] ? (const double*)stg.add(src[group + k], b, 8, kIn, "source_field",
                                                    R)
                           : nullptr;
@@ -1038,7 +1038,7 @@ int eikonal3d(double* phi, const double* speed, const double* mask, int order,
   if (df && mask) dm = (const double*)stg.add(mask, b, 8, kIn, "mask", R);
   if (!dd || !df || (mask && !dm)) return lsmgpu_peek_last_error();
   double* phi0 = nullptr;
-  bool ok = cuda_ok(cudaMallocAsync((void**)&phi0, (size_t)n * sizeof(double), st), R) &&
+  bool ok = cuda_ok(pool_alloc((void**)&phi0, (size_t)n * sizeof(double), st), R) &&
             cuda_ok(cudaMemcpyAsync(phi0, dd, (size_t)n * sizeof(double),
                                     cudaMemcpyDeviceToDevice, st), R);
   ok = ok && solve_device(dd, nullptr, dm, ExtSet{}, Eik{df, phi0}, order, grid_dims, dx,

@@ -44,6 +44,7 @@ _EXT = {
     "lsmgpu_free": (ctypes.c_int, [ctypes.c_void_p]),
     "lsmgpu_host_alloc": (ctypes.c_void_p, [ctypes.c_size_t]),
     "lsmgpu_host_free": (ctypes.c_int, [ctypes.c_void_p]),
+    "lsmgpu_release_scratch": (ctypes.c_int, []),
     "lsmgpu_memcpy_htod": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     "lsmgpu_memcpy_dtoh": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     "lsmgpu_memcpy_dtod": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),

@@ -22,7 +22,7 @@ def lib():
 def gpu_distance(lib, phi, order, dx, mask=None):
     """lsmgpu_distance_function3d on host arrays (nz, ny, nx), dx in x, y, z."""
     phi = np.ascontiguousarray(phi, dtype=np.float64)
-    out = np.zeros_like(phi)
+    out = np.full_like(phi, np.nan)      # every cell is written: nothing is copied in
     dims = (ctypes.c_int * 3)(*phi.shape[::-1])
     h = (ctypes.c_double * 3)(*dx)
     passes = ctypes.c_int(0)
@@ -90,6 +90,18 @@ def test_distance_device_arrays(lib):
     assert same_bits(out.cpu().numpy(), want)
 
 
+def test_distance_after_scratch_release(lib):
+    """The scratch the library keeps between calls can be handed back to the
+    driver at any time; the next call maps new scratch and agrees bit for
+    bit."""
+    phi, dx = seeded_spheres((30, 26, 34), 10)
+    first, _ = gpu_distance(lib, phi, 2, dx)
+    assert lib.lsmgpu_release_scratch() == 0
+    again, _ = gpu_distance(lib, phi, 2, dx)
+    assert same_bits(first, again)
+    assert same_bits(again, oracle.oracle_fmm()(phi, 2, dx))
+
+
 def test_distance_edge_cases(lib):
     phi = np.ones((5, 6, 7))
     got, _ = gpu_distance(lib, phi, 1, [1.0, 1.0, 1.0])
@@ -126,8 +138,8 @@ def gpu_extension(lib, phi, sources, order, dx, mask=None, emask=None):
     """lsmgpu_extension_fields3d on host arrays: (distance, [fields])."""
     phi = np.ascontiguousarray(phi, dtype=np.float64)
     src = [np.ascontiguousarray(a, dtype=np.float64) for a in sources]
-    ext = [np.zeros_like(phi) for _ in src]
-    dist = np.zeros_like(phi)
+    ext = [np.full_like(phi, np.nan) for _ in src]
+    dist = np.full_like(phi, np.nan)
     nf = len(src)
     src_p = (ctypes.c_void_p * max(nf, 1))(*[a.ctypes.data for a in src])
     ext_p = (ctypes.c_void_p * max(nf, 1))(*[a.ctypes.data for a in ext])
@@ -195,8 +207,8 @@ def test_extension_c_abi_entry_point(lib):
     fn.restype = ctypes.c_int
     fn.argtypes = [P, P, P, P, P, P, ctypes.c_int, ctypes.c_int, P, P]
     phi = np.ascontiguousarray(phi)
-    dist = np.zeros_like(phi)
-    ext = [np.zeros_like(phi) for _ in src]
+    dist = np.full_like(phi, np.nan)
+    ext = [np.full_like(phi, np.nan) for _ in src]
     src = [np.ascontiguousarray(a) for a in src]
     ext_p = (ctypes.c_void_p * 2)(*[a.ctypes.data for a in ext])
     src_p = (ctypes.c_void_p * 2)(*[a.ctypes.data for a in src])
