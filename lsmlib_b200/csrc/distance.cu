@@ -510,6 +510,25 @@ struct Lists {
   unsigned char* new_f;      //   bit 1: an extension field changed)
 };
 
+// grid coordinates of point o (the entry points limit grids to 2^31 - 1
+// points, so 32-bit division is exact)
+__device__ __forceinline__ void point_coords(long o, int nx, int ny, int c[3]) {
+  const unsigned u = (unsigned)o, q = u / (unsigned)nx;
+  c[0] = (int)(u - q * (unsigned)nx);
+  c[1] = (int)(q % (unsigned)ny);
+  c[2] = (int)(q / (unsigned)ny);
+}
+
+// the smallest of the warp's values (every lane takes part)
+__device__ __forceinline__ unsigned long long warp_min(unsigned long long v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(0xffffffffu, v, off);
+    v = o < v ? o : v;
+  }
+  return v;
+}
+
 __device__ __forceinline__ void push_once(long p, int stamp_val, int* stamp, int* list,
                                           int* count) {
   if (atomicExch(stamp + p, stamp_val) != stamp_val) list[atomicAdd(count, 1)] = (int)p;
@@ -524,7 +543,8 @@ __global__ void k_fmm_seed(const unsigned char* st, int nx, int ny, int nz, List
   for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < n;
        o += (long)gridDim.x * blockDim.x) {
     if (st[o] != kFree) continue;
-    const int c[3] = {(int)(o % nx), (int)((o / nx) % ny), (int)(o / s[2])};
+    int c[3];
+    point_coords(o, nx, ny, c);
     bool near = false;
 #pragma unroll
     for (int q = 0; q < 6; q++) {
@@ -543,14 +563,18 @@ template <int ORDER, bool EIK>
 __global__ void __launch_bounds__(128, ORDER == 1 ? 4 : 3)
 k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz,
            double i2x, double i2y, double i2z, Lists L, Ctrl* ctrl, ExtSet X, Eik E) {
-  // the control words are loaded together (no load waits on another)
+  // the control words, and the first slot of both active lists (the pass
+  // number picks one), are loaded together: no load waits on another
+  const long n = (long)nx * ny * nz;
+  const int w_first = blockIdx.x * blockDim.x + threadIdx.x;
+  const int first0 = w_first < n ? L.active[w_first] : 0;
+  const int first1 = w_first < n ? L.active[n + w_first] : 0;
   const int it = ctrl->pass;
   const int count0 = ctrl->count[0], count1 = ctrl->count[1];
   const int ep = ctrl->epoch;
   const double T = ctrl->T;
   const int par = it & 1;
   const int count = par ? count1 : count0;
-  const long n = (long)nx * ny * nz;
   const int* cur = L.active + par * n;
   int* pend = L.pending + (ep & 1) * n;
   int* pend_count = &ctrl->pend_count[ep & 1];
@@ -558,14 +582,15 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
   const int nn[3] = {nx, ny, nz};
   const long s[3] = {1L, (long)nx, (long)nx * ny};
   unsigned long long minrej = ~0ULL;
-  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < count; w += gridDim.x * blockDim.x) {
-    const long o = cur[w];
+  for (int w = w_first; w < count; w += gridDim.x * blockDim.x) {
+    const long o = w == w_first ? (par ? first1 : first0) : cur[w];
     // only free points are ever queued; the status, value and time of the
     // point itself are loaded beside its stencil
     const unsigned char self = st[o];
     const double old = d[o];
     const Time3 told = tm[o];
-    const int c[3] = {(int)(o % nx), (int)((o / nx) % ny), (int)(o / s[2])};
+    int c[3];
+    point_coords(o, nx, ny, c);
     Stencil nb;
     double val;
     Time3 tv, trig;
@@ -603,7 +628,8 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
     L.new_t[w] = tv;
     L.new_f[w] = f;
   }
-  if (minrej != ~0ULL) atomicMin(&ctrl->minrej, minrej);
+  minrej = warp_min(minrej);
+  if ((threadIdx.x & 31) == 0 && minrej != ~0ULL) atomicMin(&ctrl->minrej, minrej);
 }
 
 // Between passes (the last block of k_fmm_apply, one thread).  Each
@@ -619,33 +645,38 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
 constexpr int kTailFraction = 8;
 
 __device__ void fmm_control(double delta, volatile Ctrl* ctrl) {
-  if (ctrl->done) return;
-  const int par = ctrl->pass & 1;
-  const int queued = ctrl->count[par ^ 1];
-  ctrl->advance = 0;
-  if (queued > ctrl->peak) ctrl->peak = queued;
-  if ((long)queued * kTailFraction <= ctrl->peak) {
-    const int ep = ctrl->epoch;
-    const int np = ctrl->pend_count[ep & 1];
+  // every word in one round of loads (none waits on another)
+  const int done = ctrl->done, pass = ctrl->pass, peak0 = ctrl->peak, ep = ctrl->epoch;
+  const int count0 = ctrl->count[0], count1 = ctrl->count[1];
+  const int pend0 = ctrl->pend_count[0], pend1 = ctrl->pend_count[1];
+  const unsigned long long rej = ctrl->minrej, keep = ctrl->minkeep;
+  const double T = ctrl->T;
+  if (done) return;
+  const int par = pass & 1;
+  const int queued = par ? count0 : count1;
+  const int peak = queued > peak0 ? queued : peak0;
+  int advance = 0;
+  if ((long)queued * kTailFraction <= peak) {
+    const int np = (ep & 1) ? pend1 : pend0;
     if (np == 0) {
       if (queued == 0) ctrl->done = 1;
     } else {
-      const unsigned long long rej = ctrl->minrej, keep = ctrl->minkeep;
       const unsigned long long m = rej < keep ? rej : keep;
       const double lo = __longlong_as_double((long long)m);
-      const double step = ctrl->T + delta;
+      const double step = T + delta;
       ctrl->T = lo > step ? lo : step;
-      ctrl->advance = 1;
+      advance = 1;
       ctrl->filter_count = np;
       ctrl->pend_count[(ep & 1) ^ 1] = 0;
       ctrl->epoch = ep + 1;
-      ctrl->peak = queued;
       ctrl->minrej = __double_as_longlong(INFINITY);
       ctrl->minkeep = __double_as_longlong(INFINITY);
     }
   }
+  ctrl->peak = advance ? queued : peak;
+  ctrl->advance = advance;
   ctrl->count[par] = 0;
-  ctrl->pass = ctrl->pass + 1;
+  ctrl->pass = pass + 1;
 }
 
 // The second half of a pass: the values and times evaluated by k_fmm_pass are
@@ -665,19 +696,33 @@ __global__ void __launch_bounds__(256)
 k_fmm_apply(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz, Lists L,
             Ctrl* ctrl, double delta) {
   constexpr int kReaders = 6 * ORDER;
+  const long n = (long)nx * ny * nz;
+  const int lane = threadIdx.x & 31;
+  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  // the words of the first slot (both active lists for the point: the pass
+  // number picks one) load beside the control words
+  const int w_first = warp * 32 + lane;
+  unsigned char f_first = 0;
+  int first0 = 0, first1 = 0;
+  double d_first = 0;
+  Time3 t_first{0, 0, 0};
+  if (w_first < n) {
+    f_first = L.new_f[w_first];
+    first0 = L.active[w_first];
+    first1 = L.active[n + w_first];
+    d_first = L.new_d[w_first];
+    t_first = L.new_t[w_first];
+  }
   const int it = ctrl->pass;
   const int count0 = ctrl->count[0], count1 = ctrl->count[1];
   const int par = it & 1;
   const int count = par ? count1 : count0;
-  const long n = (long)nx * ny * nz;
   const int* cur = L.active + par * n;
   int* next = L.active + (par ^ 1) * n;
   int* next_count = &ctrl->count[par ^ 1];
   const int nn[3] = {nx, ny, nz};
   const long s[3] = {1L, (long)nx, (long)nx * ny};
-  const int lane = threadIdx.x & 31;
-  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
   // the loop bound is the same for the 32 lanes of a warp
   for (int w0 = warp * 32; w0 < count; w0 += nwarps * 32) {
     const int w = w0 + lane;
@@ -686,10 +731,17 @@ k_fmm_apply(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int n
     double val = 0;
     Time3 tv{0, 0, 0};
     if (w < count) {
-      f = L.new_f[w];
-      o = cur[w];
-      val = L.new_d[w];
-      tv = L.new_t[w];
+      if (w == w_first) {
+        f = f_first;
+        o = par ? first1 : first0;
+        val = d_first;
+        tv = t_first;
+      } else {
+        f = L.new_f[w];
+        o = cur[w];
+        val = L.new_d[w];
+        tv = L.new_t[w];
+      }
     }
     if (f & 1) {
       d[o] = val;
@@ -699,7 +751,8 @@ k_fmm_apply(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int n
     long on[kReaders];
     unsigned won = 0;
     if (f & 2) {
-      const int c[3] = {(int)(o % nx), (int)((o / nx) % ny), (int)(o / s[2])};
+      int c[3];
+    point_coords(o, nx, ny, c);
       unsigned char sn[kReaders];
       unsigned cand = 0;
 #pragma unroll
@@ -780,7 +833,8 @@ __global__ void k_fmm_filter(const double* d, const Time3* tm, long n, Lists L, 
       mk = bits < mk ? bits : mk;
     }
   }
-  if (mk != ~0ULL) atomicMin(&ctrl->minkeep, mk);
+  mk = warp_min(mk);
+  if ((threadIdx.x & 31) == 0 && mk != ~0ULL) atomicMin(&ctrl->minkeep, mk);
 }
 
 // free points no front reached: the reference's default value -1 (distance
