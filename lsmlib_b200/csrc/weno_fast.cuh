@@ -170,14 +170,30 @@ static __device__ __noinline__ float2 weno5_face_fp64(float u0, float u1, float 
 //   p1 - p2 = (ta - tb)/3,  p3 - p2 = (tb - tc)/6,
 // where ta, tb, tc are the second differences of V already formed for the
 // smoothness indicators; for the reversed (plus) stencil the two third
-// differences swap and change sign.  When KINK64 is set (FP32 form) a face
-// whose indicators differ by more than a factor 1e3 is recomputed in FP64.
+// differences swap and change sign.  So
+//   vm = p2m + (2 Pbc T1 + 3 Pab T2) / (60 sm),
+//   vp = p2p - (2 Pab T2 + 3 Pbc T1) / (60 sp),
+// with T1 = ta - tb, T2 = tb - tc and sm, sp the weight sums.  Three more
+// rearrangements change only rounding:
+//  * the reconstruction is homogeneous of degree one in V and its weights
+//    of degree zero (but for the floor of eps), so it runs on the undivided
+//    differences D = u[m+1] - u[m] and the two results are scaled by 1/dx
+//    once;
+//  * the eps maximum is max|D| squared (rounding is monotone, so this is
+//    exactly the largest square);
+//  * in FP64 one reciprocal of 60 sm sp serves both sides (the products stay
+//    below 2^210; in FP32 they would overflow, so FP32 takes two).
+// When KINK64 is set (FP32 form) a face whose indicators differ by more than
+// a factor 1e3 is recomputed in FP64.
 template <typename T, bool KINK64>
 __device__ __forceinline__ void weno5_face(const T* u, T inv, T& vp, T& vm) {
-  const T V1 = (u[1] - u[0]) * inv, V2 = (u[2] - u[1]) * inv,
-          V3 = (u[3] - u[2]) * inv, V4 = (u[4] - u[3]) * inv,
-          V5 = (u[5] - u[4]) * inv;
-  const T m = fmax(fmax(fmax(V1 * V1, V2 * V2), fmax(V3 * V3, V4 * V4)), V5 * V5);
+  const T V1 = u[1] - u[0], V2 = u[2] - u[1], V3 = u[3] - u[2], V4 = u[4] - u[3],
+          V5 = u[5] - u[4];
+  const T amax = fmax(fmax(fmax(fabs(V1), fabs(V2)), fmax(fabs(V3), fabs(V4))), fabs(V5));
+  const T m = amax * amax;
+  // the reference's 1e-6 max(v^2) + tiny, in units of the undivided
+  // differences (the floor, reached only where every |D| < 1e-46, is kept
+  // in these units)
   const T eps = T(1e-6) * m + Consts<T>::tiny;
   const T c13_12 = T(13.0 / 12.0), c14 = T(0.25);
   const T ta = V1 - T(2) * V2 + V3, tb = V2 - T(2) * V3 + V4, tc = V3 - T(2) * V4 + V5;
@@ -203,14 +219,22 @@ __device__ __forceinline__ void weno5_face(const T* u, T inv, T& vp, T& vm) {
   const T qa = Sa * sc + es, qb = Sb * sc + es, qc = Sc * sc + es;
   const T Qa = qa * qa, Qb = qb * qb, Qc = qc * qc;
   const T Pbc = Qb * Qc, Pac = Qa * Qc, Pab = Qa * Qb;
-  const T T1 = ta - tb, T2 = tb - tc;
-  const T sm = T(0.1) * Pbc + T(0.6) * Pac + T(0.3) * Pab;
-  const T sp = T(0.1) * Pab + T(0.6) * Pac + T(0.3) * Pbc;
-  const T d6 = T(1.0 / 6.0), e6 = T(5.0 / 6.0), a3 = T(1.0 / 3.0);
-  const T p2m = a3 * V4 + e6 * V3 - d6 * V2;
-  const T p2p = a3 * V2 + e6 * V3 - d6 * V4;
-  vm = p2m + (Pbc * (T1 * T(1.0 / 30.0)) + Pab * (T2 * T(1.0 / 20.0))) * rcp_nr(sm);
-  vp = p2p - (Pab * (T2 * T(1.0 / 30.0)) + Pbc * (T1 * T(1.0 / 20.0))) * rcp_nr(sp);
+  const T A = Pbc * (ta - tb), B = Pab * (tb - tc);
+  const T num_m = T(2) * A + T(3) * B, num_p = T(2) * B + T(3) * A;
+  const T e3 = T(5.0 / 6.0) * V3;
+  const T p2m = T(1.0 / 3.0) * V4 + (e3 - T(1.0 / 6.0) * V2);
+  const T p2p = T(1.0 / 3.0) * V2 + (e3 - T(1.0 / 6.0) * V4);
+  // 60 sm and 60 sp
+  const T sm = T(6) * Pbc + T(36) * Pac + T(18) * Pab;
+  const T sp = T(6) * Pab + T(36) * Pac + T(18) * Pbc;
+  if constexpr (sizeof(T) == 8) {
+    const T r = rcp_nr(sm * sp);
+    vm = (p2m + num_m * (sp * r)) * inv;
+    vp = (p2p - num_p * (sm * r)) * inv;
+  } else {
+    vm = (p2m + num_m * rcp_nr(sm)) * inv;
+    vp = (p2p - num_p * rcp_nr(sp)) * inv;
+  }
 }
 
 static __device__ __noinline__ float2 weno5_face_fp64(float u0, float u1, float u2,
