@@ -170,30 +170,37 @@ __device__ __forceinline__ T fetch_bc(const Grid3<const T>& g,
 // One-sided WENO5 from seven consecutive phi values w[0..6] = phi(c-3..c+3).
 template <typename T, bool FAST>
 __device__ __forceinline__ T weno_minus7(const T* w, T inv) {
+  if (FAST)
+    return weno5_side_fast(w[1] - w[0], w[2] - w[1], w[3] - w[2], w[4] - w[3], w[5] - w[4],
+                           inv);
   const T v1 = (w[1] - w[0]) * inv, v2 = (w[2] - w[1]) * inv,
           v3 = (w[3] - w[2]) * inv, v4 = (w[4] - w[3]) * inv,
           v5 = (w[5] - w[4]) * inv;
-  return FAST ? weno5_fast(v1, v2, v3, v4, v5) : weno5_strict(v1, v2, v3, v4, v5);
+  return weno5_strict(v1, v2, v3, v4, v5);
 }
 template <typename T, bool FAST>
 __device__ __forceinline__ T weno_plus7(const T* w, T inv) {
+  if (FAST)
+    return weno5_side_fast(w[6] - w[5], w[5] - w[4], w[4] - w[3], w[3] - w[2], w[2] - w[1],
+                           inv);
   const T v1 = (w[6] - w[5]) * inv, v2 = (w[5] - w[4]) * inv,
           v3 = (w[4] - w[3]) * inv, v4 = (w[3] - w[2]) * inv,
           v5 = (w[2] - w[1]) * inv;
-  return FAST ? weno5_fast(v1, v2, v3, v4, v5) : weno5_strict(v1, v2, v3, v4, v5);
+  return weno5_strict(v1, v2, v3, v4, v5);
 }
 
 // FP32 form: the same values, with kink stencils recomputed in FP64 from the
-// FP32 phi values.
+// FP32 phi values (the kink test is scale-free, so it reads the undivided
+// differences).
 template <typename T, bool FAST>
 __device__ __forceinline__ T weno_side(const T* w, T inv, bool plus,
                                        bool fp64_kinks) {
   if (sizeof(T) == 4 && fp64_kinks) {
-    const T v1 = plus ? (w[6] - w[5]) * inv : (w[1] - w[0]) * inv;
-    const T v2 = plus ? (w[5] - w[4]) * inv : (w[2] - w[1]) * inv;
-    const T v3 = plus ? (w[4] - w[3]) * inv : (w[3] - w[2]) * inv;
-    const T v4 = plus ? (w[3] - w[2]) * inv : (w[4] - w[3]) * inv;
-    const T v5 = plus ? (w[2] - w[1]) * inv : (w[5] - w[4]) * inv;
+    const T v1 = plus ? w[6] - w[5] : w[1] - w[0];
+    const T v2 = plus ? w[5] - w[4] : w[2] - w[1];
+    const T v3 = plus ? w[4] - w[3] : w[3] - w[2];
+    const T v4 = plus ? w[3] - w[2] : w[4] - w[3];
+    const T v5 = plus ? w[2] - w[1] : w[5] - w[4];
     if (weno5_is_kink(v1, v2, v3, v4, v5)) {
       double wd[7];
 #pragma unroll
@@ -202,7 +209,7 @@ __device__ __forceinline__ T weno_side(const T* w, T inv, bool plus,
       return (T)(plus ? weno_plus7<double, true>(wd, id)
                       : weno_minus7<double, true>(wd, id));
     }
-    return weno5_fast(v1, v2, v3, v4, v5);
+    return weno5_side_fast(v1, v2, v3, v4, v5, inv);
   }
   return plus ? weno_plus7<T, FAST>(w, inv) : weno_minus7<T, FAST>(w, inv);
 }

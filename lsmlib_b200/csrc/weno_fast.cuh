@@ -44,31 +44,35 @@ __device__ __forceinline__ float inv_pow2_of(float x) {
   return __int_as_float((254 - e) << 23);
 }
 
-// Reconstruction from five scaled differences v1..v5 (reference ordering:
-// minus side v = V(i-2..i+2); plus side v = V(i+3..i-1)).
+// One side of HJ-WENO5 from the five undivided differences D1..D5 in the
+// reference's ordering (v_k = D_k / dx); returns the reconstruction of the
+// scaled differences.  The same rearrangement as weno5_face below: the
+// weights see only ratios of D (scaling by 1/dx is applied once at the end),
+// eps is taken from max|D|, and with w2 = 1 - w1 - w3
+//   phi = p2 + (2 P23 (ta - tb) + 3 P12 (tb - tc)) / (6 P23 + 36 P13 + 18 P12),
+// P_xy = (q_x q_y)^2, ta, tb, tc the second differences of the smoothness
+// indicators.
 template <typename T>
-__device__ __forceinline__ T weno5_fast(T v1, T v2, T v3, T v4, T v5) {
-  const T s1 = v1 * v1, s2 = v2 * v2, s3 = v3 * v3, s4 = v4 * v4, s5 = v5 * v5;
-  const T m = fmax(fmax(fmax(s1, s2), fmax(s3, s4)), s5);
-  const T eps = T(1e-6) * m + Consts<T>::tiny;
-  const T p1 = T(1.0 / 3.0) * v1 - T(7.0 / 6.0) * v2 + T(11.0 / 6.0) * v3;
-  const T p2 = -T(1.0 / 6.0) * v2 + T(5.0 / 6.0) * v3 + T(1.0 / 3.0) * v4;
-  const T p3 = T(1.0 / 3.0) * v3 + T(5.0 / 6.0) * v4 - T(1.0 / 6.0) * v5;
-  T t = v1 - T(2) * v2 + v3, u = v1 - T(4) * v2 + T(3) * v3;
-  const T S1 = T(13.0 / 12.0) * (t * t) + T(0.25) * (u * u);
-  t = v2 - T(2) * v3 + v4;
-  u = v2 - v4;
-  const T S2 = T(13.0 / 12.0) * (t * t) + T(0.25) * (u * u);
-  t = v3 - T(2) * v4 + v5;
-  u = T(3) * v3 - T(4) * v4 + v5;
-  const T S3 = T(13.0 / 12.0) * (t * t) + T(0.25) * (u * u);
+__device__ __forceinline__ T weno5_side_fast(T D1, T D2, T D3, T D4, T D5, T inv) {
+  const T amax = fmax(fmax(fmax(fabs(D1), fabs(D2)), fmax(fabs(D3), fabs(D4))), fabs(D5));
+  const T eps = T(1e-6) * (amax * amax) + Consts<T>::tiny;
+  const T c13_12 = T(13.0 / 12.0), c14 = T(0.25);
+  const T ta = D1 - T(2) * D2 + D3, tb = D2 - T(2) * D3 + D4, tc = D3 - T(2) * D4 + D5;
+  T t = D1 - T(4) * D2 + T(3) * D3;
+  const T S1 = c13_12 * (ta * ta) + c14 * (t * t);
+  t = D2 - D4;
+  const T S2 = c13_12 * (tb * tb) + c14 * (t * t);
+  t = T(3) * D3 - T(4) * D4 + D5;
+  const T S3 = c13_12 * (tc * tc) + c14 * (t * t);
   const T sc = inv_pow2_of(eps);
   const T es = eps * sc;
   const T q1 = S1 * sc + es, q2 = S2 * sc + es, q3 = S3 * sc + es;
   const T Q1 = q1 * q1, Q2 = q2 * q2, Q3 = q3 * q3;
-  const T n1 = T(0.1) * (Q2 * Q3), n2 = T(0.6) * (Q1 * Q3), n3 = T(0.3) * (Q1 * Q2);
-  const T r = rcp_nr(n1 + n2 + n3);
-  return (n1 * p1 + n2 * p2 + n3 * p3) * r;
+  const T P23 = Q2 * Q3, P13 = Q1 * Q3, P12 = Q1 * Q2;
+  const T num = T(2) * (P23 * (ta - tb)) + T(3) * (P12 * (tb - tc));
+  const T den = T(6) * P23 + T(36) * P13 + T(18) * P12;
+  const T p2 = T(1.0 / 3.0) * D4 + (T(5.0 / 6.0) * D3 - T(1.0 / 6.0) * D2);
+  return (p2 + num * rcp_nr(den)) * inv;
 }
 
 // Weights and combination of one side from its smoothness indicators,
