@@ -54,8 +54,8 @@ WORKLOAD = ("256^3 normal-velocity level set (6 spheres, F = 1 + 0.2 sin sin sin
 # DRAM bytes (read + write) per launch and FP64-pipe utilisation of the fused
 # stage kernels on the 256^3 workload, from the ncu capture summarised in
 # profiles/k_stage_fp64_config2_256.md (distinct phi_s and phi^n)
-NCU_TRAFFIC = {"stage_reinit_rk32": 390.9e6, "stage_normal_rk32": 535.7e6}
-NCU_FP64_PIPE = {"stage_reinit_rk32": 48.9, "stage_normal_rk32": 51.7}
+NCU_TRAFFIC = {"stage_reinit_rk32": 390.8e6, "stage_normal_rk32": 536.0e6}
+NCU_FP64_PIPE = {"stage_reinit_rk32": 46.8, "stage_normal_rk32": 49.7}
 
 def env_int(name, default):
     try:
