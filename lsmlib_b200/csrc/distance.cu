@@ -293,7 +293,9 @@ __device__ __forceinline__ double fmm_root(double A, double B, double disc) {
 // when a pass queues nothing, T moves to max(T + delta, smallest
 // candidate) and the pending points it reaches are queued.  A pass is two
 // kernels: k_fmm_pass evaluates every queued point from the values before
-// the pass, k_fmm_apply stores the changes and queues their readers.
+// the pass (and, after a threshold advance, moves the pending points the
+// new T reaches to the next queue), k_fmm_apply stores the changes, queues
+// their readers and runs the threshold control in its last block.
 
 // the threshold advances by this many of the smallest spacing per step
 constexpr double kDeltaCells = 2.0;
@@ -573,6 +575,7 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
   const int count0 = ctrl->count[0], count1 = ctrl->count[1];
   const int ep = ctrl->epoch;
   const double T = ctrl->T;
+  const int advance = ctrl->advance, filter_count = ctrl->filter_count;
   const int par = it & 1;
   const int count = par ? count1 : count0;
   const int* cur = L.active + par * n;
@@ -630,6 +633,31 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
   }
   minrej = warp_min(minrej);
   if ((threadIdx.x & 31) == 0 && minrej != ~0ULL) atomicMin(&ctrl->minrej, minrej);
+  // After a threshold advance (the control step that ended the last pass):
+  // the pending points of the last epoch that the new threshold reaches join
+  // the queue of the next pass beside the readers k_fmm_apply queues (same
+  // list, same stamp); the others wait in this epoch's pending list.  Values
+  // and times do not change during this kernel, so the test reads them as
+  // the pass does.
+  if (advance) {
+    const int* src = L.pending + ((ep - 1) & 1) * n;
+    int* next = L.active + (par ^ 1) * n;
+    unsigned long long mk = ~0ULL;
+    for (int w = w_first; w < filter_count; w += gridDim.x * blockDim.x) {
+      const long o = src[w];
+      if (fabs(d[o]) <= DBL_MAX) continue;   // reached since
+      const double t = tm[o].a;
+      if (t <= T) {
+        push_once(o, it + 2, L.stamp, next, &ctrl->count[par ^ 1]);
+      } else if (t < INFINITY) {
+        push_once(o, ep + 1, L.pend_stamp, pend, pend_count);
+        const unsigned long long bits = __double_as_longlong(t);
+        mk = bits < mk ? bits : mk;
+      }
+    }
+    mk = warp_min(mk);
+    if ((threadIdx.x & 31) == 0 && mk != ~0ULL) atomicMin(&ctrl->minkeep, mk);
+  }
 }
 
 // Between passes (the last block of k_fmm_apply, one thread).  Each
@@ -638,8 +666,8 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
 // tail (the fixed point does not depend on when T moves, only the amount of
 // revision does).  So once the queued points fall to 1/kTailFraction of the
 // step's largest pass, the threshold moves to max(T + delta, smallest
-// waiting candidate) and the pending list is filtered (next kernel) into the
-// queue beside them.  With nothing queued and nothing waiting, the solve is
+// waiting candidate) and the pending list is filtered (by the next pass
+// kernel) into the queue after it.  With nothing queued and nothing waiting, the solve is
 // done.  The words are read volatile: other blocks of the same launch wrote
 // the queue length.
 constexpr int kTailFraction = 8;
@@ -809,34 +837,6 @@ k_fmm_apply(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int n
   }
 }
 
-// After a threshold advance: the pending points the threshold reaches join
-// the active list, the others wait in the other pending list.
-__global__ void k_fmm_filter(const double* d, const Time3* tm, long n, Lists L, Ctrl* ctrl) {
-  if (!ctrl->advance) return;
-  const int ep = ctrl->epoch;              // already advanced
-  const int np = ctrl->filter_count;
-  const int* src = L.pending + ((ep - 1) & 1) * n;
-  int* keep = L.pending + (ep & 1) * n;
-  const int par = ctrl->pass & 1;          // the coming pass
-  int* next = L.active + par * n;
-  const double T = ctrl->T;
-  unsigned long long mk = ~0ULL;
-  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < np; w += gridDim.x * blockDim.x) {
-    const long o = src[w];
-    if (fabs(d[o]) <= DBL_MAX) continue;   // reached since
-    const double t = tm[o].a;
-    if (t <= T) {
-      push_once(o, ctrl->pass + 1, L.stamp, next, &ctrl->count[par]);
-    } else if (t < INFINITY) {
-      push_once(o, ep + 1, L.pend_stamp, keep, &ctrl->pend_count[ep & 1]);
-      const unsigned long long bits = __double_as_longlong(t);
-      mk = bits < mk ? bits : mk;
-    }
-  }
-  mk = warp_min(mk);
-  if ((threadIdx.x & 31) == 0 && mk != ~0ULL) atomicMin(&ctrl->minkeep, mk);
-}
-
 // free points no front reached: the reference's default value -1 (distance
 // and extension fields), or the Eikonal solver's input
 __global__ void k_fmm_unreached(double* d, const unsigned char* st, long n, ExtSet X,
@@ -914,7 +914,7 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
   }
   // a pass touches only the band, so a few blocks per SM cover it; the
   // grid-stride loops take any count
-  const int pass_blocks = 4 * sms, apply_blocks = 2 * sms, filter_blocks = 2 * sms;
+  const int pass_blocks = 4 * sms, apply_blocks = 2 * sms;
   const int batch = 32;
   auto launch_batch = [&](cudaStream_t s) {
     for (int q = 0; q < batch; q++) {
@@ -936,7 +936,6 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
       else
         k_fmm_apply<2><<<apply_blocks, 256, 0, s>>>(dd, tm, status, nx, ny, nz, L, ctrl,
                                                      delta);
-      k_fmm_filter<<<filter_blocks, 256, 0, s>>>(dd, tm, n, L, ctrl);
     }
   };
   // The kernels read the pass number and lists from ``ctrl``, so every batch
@@ -963,7 +962,7 @@ bool solve_device(double* dd, const double* dp, const double* dm, const ExtSet& 
     if (gexec) ok = cuda_ok(cudaGraphLaunch(gexec, st), R);
     else launch_batch(st);
     launched += batch;
-    launch_counter() += 3 * batch;
+    launch_counter() += 2 * batch;
     ok = ok && cuda_ok(cudaGetLastError(), R) &&
          cuda_ok(cudaMemcpyAsync(&h_ctrl, ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st), R) &&
          cuda_ok(cudaStreamSynchronize(st), R);
