@@ -20,7 +20,7 @@ def declared_functions():
     skip = {"if", "defined", "sizeof"}
     return sorted({n for n in names if n not in skip and
                    (n.startswith("lsm3d") or n.startswith("lsmgpu_") or
-                    n.startswith("compute"))})
+                    n.startswith("compute") or n.startswith("solve"))})
 
 
 def test_header_declares_all_reference_symbols():
