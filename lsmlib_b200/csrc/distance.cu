@@ -560,7 +560,9 @@ __global__ void k_fmm_seed(const unsigned char* st, int nx, int ny, int nz, List
 
 // The first half of a pass over the active list (count[pass & 1]): each
 // point's value and time from the values before the pass, into the list's
-// side arrays; rejected points join the pending list.
+// side arrays, with what changed; rejected points join the pending list.
+// After a threshold advance it also filters the last epoch's pending list
+// (below the main loop).
 template <int ORDER, bool EIK>
 __global__ void __launch_bounds__(128, ORDER == 1 ? 4 : 3)
 k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz,
