@@ -41,6 +41,12 @@ def write_data_array(file_name, data, grid_dims_ghostbox=None, zip_status=NO_ZIP
         raise ValueError("data has dims %s, grid says %s" % (dims, tuple(grid_dims_ghostbox)))
     payload = (np.asarray(dims, dtype=np.intc).tobytes() +
                np.asarray(a, dtype=dtype).tobytes(order="A"))
+    return _write(file_name, payload, zip_status)
+
+
+def _write(file_name, payload, zip_status):
+    """The file, compressed in place to name.gz / name.bz2 by zip status
+    (zipFile, lsm_file.c:55-90); returns the name written."""
     if zip_status == GZIP:
         file_name = file_name + ".gz"
         with gzip.open(file_name, "wb") as f:
@@ -55,9 +61,9 @@ def write_data_array(file_name, data, grid_dims_ghostbox=None, zip_status=NO_ZIP
     return file_name
 
 
-def read_data_array(file_name, dtype=np.float64):
-    """readDataArray: (grid_dims_ghostbox, array of shape (nx, ny, nz) in
-    Fortran order).  Compressed names are read through the decompressor."""
+def _read(file_name):
+    """The file's bytes, through the decompressor its name asks for
+    (checkUnzipFile, lsm_file.c:18-53)."""
     if file_name.endswith(".gz"):
         opener = gzip.open
     elif file_name.endswith(".bz2"):
@@ -67,7 +73,13 @@ def read_data_array(file_name, dtype=np.float64):
     if not os.path.exists(file_name):
         raise FileNotFoundError(file_name)
     with opener(file_name, "rb") as f:
-        raw = f.read()
+        return f.read()
+
+
+def read_data_array(file_name, dtype=np.float64):
+    """readDataArray: (grid_dims_ghostbox, array of shape (nx, ny, nz) in
+    Fortran order).  Compressed names are read through the decompressor."""
+    raw = _read(file_name)
     head = np.dtype(np.intc).itemsize * 3
     dims = tuple(int(v) for v in np.frombuffer(raw[:head], dtype=np.intc))
     n = dims[0] * dims[1] * dims[2]
@@ -75,3 +87,23 @@ def read_data_array(file_name, dtype=np.float64):
     if vals.size != n:
         raise ValueError("%s: %d values for dims %s" % (file_name, vals.size, dims))
     return dims, vals.reshape(dims, order="F").copy(order="F")
+
+
+def write_data_array_1d(file_name, data, zip_status=NO_ZIP, dtype=np.float64):
+    """writeDataArray1d (lsm_data_arrays.c:439-454): the number of elements
+    as one native int, then the values.  Returns the name written."""
+    a = np.asarray(data, dtype=dtype).ravel()
+    payload = np.asarray([a.size], dtype=np.intc).tobytes() + a.tobytes()
+    return _write(file_name, payload, zip_status)
+
+
+def read_data_array_1d(file_name, dtype=np.float64):
+    """readDataArray1d (lsm_data_arrays.c:457-489): the values as a 1D
+    array."""
+    raw = _read(file_name)
+    head = np.dtype(np.intc).itemsize
+    n = int(np.frombuffer(raw[:head], dtype=np.intc)[0])
+    vals = np.frombuffer(raw[head:head + n * np.dtype(dtype).itemsize], dtype=dtype)
+    if vals.size != n:
+        raise ValueError("%s: %d values for %d elements" % (file_name, vals.size, n))
+    return vals.copy()
