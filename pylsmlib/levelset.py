@@ -49,7 +49,12 @@ class Grid:
         gd = self.grid_dims_ghostbox
         self.gb = (0, gd[0] - 1, 0, gd[1] - 1, 0, gd[2] - 1)
         self.D1_fb = (1, gd[0] - 2, 1, gd[1] - 2, 1, gd[2] - 2)
-        lo_shift, hi_shift = {"LOW": (0, 1), "MEDIUM": (1, 2), "HIGH": (2, 3),
+        self.D2_fb = (2, gd[0] - 3, 2, gd[1] - 3, 2, gd[2] - 3)
+        self.D3_fb = (3, gd[0] - 4, 3, gd[1] - 4, 3, gd[2] - 4)
+        # setIndexSpaceLimitsENO1/ENO2/ENO3/WENO5 (lsm_grid.c:831-982): the
+        # scheme's fill box is the D1 box shrunk by these amounts (D2 and D3
+        # boxes are the ghost box shrunk by 2 and 3)
+        lo_shift, hi_shift = {"LOW": (0, 1), "MEDIUM": (2, 2), "HIGH": (3, 4),
                               "VERY_HIGH": (2, 3)}[accuracy]
         d = self.D1_fb
         self.fb = (d[0] + lo_shift, d[1] - hi_shift, d[2] + lo_shift, d[3] - hi_shift,

@@ -6,7 +6,7 @@ from pylsmlib import Grid
 
 
 @pytest.mark.parametrize("accuracy,ghost,lo_shift,hi_shift",
-                         [("LOW", 2, 0, 1), ("MEDIUM", 3, 1, 2), ("HIGH", 5, 2, 3),
+                         [("LOW", 2, 0, 1), ("MEDIUM", 3, 2, 2), ("HIGH", 5, 3, 4),
                           ("VERY_HIGH", 4, 2, 3)])
 def test_index_spaces(accuracy, ghost, lo_shift, hi_shift):
     g = Grid.set_grid_dims((20, 12, 9), (-1.0, 0.0, 2.0), (1.0, 0.6, 2.9), accuracy)
@@ -37,3 +37,77 @@ def test_grid_point_coordinates():
     assert float(x[0, 0, 5]) == g.x_lo_ghostbox[0] + 0.1 * 5
     assert float(y[0, 3, 0]) == g.x_lo_ghostbox[1] + 0.2 * 3
     assert float(z[2, 0, 0]) == g.x_lo_ghostbox[2] + 0.25 * 2
+
+
+# ---- pinned against the reference's own grid constructors ------------------------
+
+import ctypes  # noqa: E402
+import importlib.util  # noqa: E402
+import json  # noqa: E402
+import os  # noqa: E402
+
+import numpy as np  # noqa: E402
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def ours(ctor, arg, x_lo, x_hi, accuracy):
+    if ctor == "set_grid_dims":
+        return Grid.set_grid_dims(arg, x_lo, x_hi, accuracy)
+    return Grid.set_dx(arg, x_lo, x_hi, accuracy)
+
+
+def as_fields(g):
+    return {"num_dims": g.num_dims, "x_lo": list(g.x_lo), "x_hi": list(g.x_hi),
+            "x_lo_ghostbox": list(g.x_lo_ghostbox), "x_hi_ghostbox": list(g.x_hi_ghostbox),
+            "grid_dims": list(g.grid_dims), "grid_dims_ghostbox": list(g.grid_dims_ghostbox),
+            "dx": list(g.dx), "num_gridpts": g.num_gridpts, "gb": list(g.gb),
+            "fb": list(g.fb), "D1_fb": list(g.D1_fb), "D2_fb": list(g.D2_fb),
+            "D3_fb": list(g.D3_fb)}
+
+
+GOLDEN = json.load(open(os.path.join(GOLDEN_DIR, "grid_golden.json")))
+
+
+@pytest.mark.parametrize("case", GOLDEN, ids=["%s-%s-%d" % (c["ctor"], c["accuracy"], i)
+                                              for i, c in enumerate(GOLDEN)])
+def test_grid_matches_reference_golden(case):
+    """Every field of the reference's Grid, as createGridSetDx /
+    createGridSetDxDyDz / createGridSetGridDims filled it, is ours exactly."""
+    g = ours(case["ctor"], case["arg"], case["x_lo"], case["x_hi"], case["accuracy"])
+    assert as_fields(g) == case["grid"]
+
+
+def test_grid_matches_reference_live_on_seeded_extents():
+    """Where the reference's grid code is built (oracle/_ref/libgrid.so),
+    seeded spacings and extents agree field by field."""
+    lib_path = os.path.join(os.path.dirname(GOLDEN_DIR), "..", "oracle", "_ref", "libgrid.so")
+    if not os.path.exists(lib_path):
+        pytest.skip("oracle/_ref/libgrid.so not built (make -C oracle ref)")
+    spec = importlib.util.spec_from_file_location(
+        "gen_grid_golden", os.path.join(GOLDEN_DIR, "gen_grid_golden.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    lib = ctypes.CDLL(lib_path)
+    lib.createGridSetDxDyDz.restype = ctypes.POINTER(gen.RefGrid)
+    lib.createGridSetDxDyDz.argtypes = [ctypes.c_int] + [ctypes.c_double] * 3 + [
+        gen.D3, gen.D3, ctypes.c_int]
+    lib.createGridSetGridDims.restype = ctypes.POINTER(gen.RefGrid)
+    lib.createGridSetGridDims.argtypes = [ctypes.c_int, gen.I3, gen.D3, gen.D3, ctypes.c_int]
+    lib.destroyGrid.argtypes = [ctypes.POINTER(gen.RefGrid)]
+    rng = np.random.default_rng(11)
+    for _ in range(40):
+        lo = rng.uniform(-2, 1, 3)
+        hi = lo + rng.uniform(0.1, 3, 3)
+        h = rng.uniform(0.005, 0.2, 3)
+        dims = rng.integers(1, 90, 3)
+        acc = int(rng.integers(0, 4))
+        p = lib.createGridSetDxDyDz(3, *h, gen.D3(*lo), gen.D3(*hi), acc)
+        assert gen.fields(p.contents) == as_fields(
+            Grid.set_dx(tuple(h), tuple(lo), tuple(hi), gen.ACCURACY[acc]))
+        lib.destroyGrid(p)
+        p = lib.createGridSetGridDims(3, gen.I3(*dims), gen.D3(*lo), gen.D3(*hi), acc)
+        assert gen.fields(p.contents) == as_fields(
+            Grid.set_grid_dims(tuple(int(v) for v in dims), tuple(lo), tuple(hi),
+                               gen.ACCURACY[acc]))
+        lib.destroyGrid(p)
