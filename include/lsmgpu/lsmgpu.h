@@ -399,8 +399,8 @@ void lsm3dcomputereinitializationeqnrhssubcellfixorder1_(
  * the values of the reference's first- (order 1) or second-order (order 2)
  * fast marching method: points on the interface hold +-1e-11, points no
  * front reaches -1, points with mask < 0 (mask may be NULL)
- * LSMLIB_REAL_MAX.  Computed on the GPU as the march's fixed point, tile by
- * tile (no heap).  Arrays are host or device pointers (see above); the call
+ * LSMLIB_REAL_MAX.  Computed on the GPU as the march's fixed point, by
+ * passes over a band of active points (no heap).  Arrays are host or device pointers (see above); the call
  * returns after the work finishes.  Returns 0, 2 for an order other than 1
  * or 2 (LSM_FMM_ERR_INVALID_SPATIAL_DISCRETIZATION_ORDER), -1 for any other
  * failure (the error is recorded for lsmgpu_get_last_error). */
@@ -430,6 +430,22 @@ int computeExtensionFields3d(LSMLIB_REAL *distance_function,
  * or speed < 1e-11 get LSMLIB_REAL_MAX; points no boundary value reaches
  * keep their input.  Same return codes as computeDistanceFunction3d. */
 int solveEikonalEquation3d(LSMLIB_REAL *phi, LSMLIB_REAL *speed, LSMLIB_REAL *mask,
+                           int spatial_discretization_order, int *grid_dims,
+                           LSMLIB_REAL *dx);
+/* lsm_fast_marching_method.h:124-134, 179-185, 256-262: the 2D forms, with
+ * grid_dims[2] and dx[2] in x, y order and the same arguments, values and
+ * return codes.  Each runs the 3D solve on a grid one plane thick; the
+ * reference's own 2D and 3D routines give bit-identical results there. */
+int computeExtensionFields2d(LSMLIB_REAL *distance_function,
+                             LSMLIB_REAL **extension_fields, LSMLIB_REAL *phi,
+                             LSMLIB_REAL *mask, LSMLIB_REAL **source_fields,
+                             LSMLIB_REAL *extension_mask, int num_extension_fields,
+                             int spatial_discretization_order, int *grid_dims,
+                             LSMLIB_REAL *dx);
+int computeDistanceFunction2d(LSMLIB_REAL *distance_function, LSMLIB_REAL *phi,
+                              LSMLIB_REAL *mask, int spatial_discretization_order,
+                              int *grid_dims, LSMLIB_REAL *dx);
+int solveEikonalEquation2d(LSMLIB_REAL *phi, LSMLIB_REAL *speed, LSMLIB_REAL *mask,
                            int spatial_discretization_order, int *grid_dims,
                            LSMLIB_REAL *dx);
 
@@ -673,7 +689,7 @@ int lsmgpu_adjoint_phi_final(lsmgpu_adjoint *h, double *host);
  * LSMGPU_ERR_INVALID_VALUE for an order other than 1 or 2, a dx <= 0 or an
  * input without a fixed point (NaN), LSMGPU_ERR_INVALID_BOX for an empty
  * grid; ``passes`` (may be NULL) receives the number of passes over the
- * active tiles of 16 x 8 x 8 points that the solve took. */
+ * band of active points that the solve took. */
 int lsmgpu_distance_function3d(double *distance_function, const double *phi,
                                const double *mask, int order,
                                const int grid_dims[3], const double dx[3],

@@ -1164,4 +1164,73 @@ int lsmgpu_eikonal3d(double* phi, const double* speed, const double* mask, int o
   return eikonal3d(phi, speed, mask, order, grid_dims, dx, passes, "lsmgpu_eikonal3d");
 }
 
+// The 2D forms (lsm_fast_marching_method.h:124-134, 179-185, 256-262): the
+// 3D solve on a grid one plane thick, on which the reference's own 2D and 3D
+// routines agree bit for bit.  grid_dims and dx hold x and y; the z spacing
+// is taken as dx[0] (a single plane has no z neighbours, and the threshold
+// step then still follows the smallest of dx and dy).  Null arguments pass
+// through as null, so the 3D checks report them.
+static void plane_grid(const int* grid_dims, const double* dx, int d3[3], double h3[3],
+                       const int** pd, const double** ph) {
+  *pd = nullptr;
+  *ph = nullptr;
+  if (grid_dims) {
+    d3[0] = grid_dims[0];
+    d3[1] = grid_dims[1];
+    d3[2] = 1;
+    *pd = d3;
+  }
+  if (dx) {
+    h3[0] = dx[0];
+    h3[1] = dx[1];
+    h3[2] = dx[0];
+    *ph = h3;
+  }
+}
+
+int computeExtensionFields2d(double* distance_function, double** extension_fields,
+                             double* phi, double* mask, double** source_fields,
+                             double* extension_mask, int num_extension_fields,
+                             int spatial_discretization_order, int* grid_dims, double* dx) {
+  if (spatial_discretization_order != 1 && spatial_discretization_order != 2) return 2;
+  int d3[3];
+  double h3[3];
+  const int* pd;
+  const double* ph;
+  plane_grid(grid_dims, dx, d3, h3, &pd, &ph);
+  const int rc = extension3d(distance_function, extension_fields, phi, mask, source_fields,
+                             extension_mask, num_extension_fields,
+                             spatial_discretization_order, pd, ph, nullptr,
+                             "computeExtensionFields2d");
+  return rc == LSMGPU_SUCCESS ? 0 : -1;
+}
+
+int computeDistanceFunction2d(double* distance_function, double* phi, double* mask,
+                              int spatial_discretization_order, int* grid_dims,
+                              double* dx) {
+  if (spatial_discretization_order != 1 && spatial_discretization_order != 2) return 2;
+  int d3[3];
+  double h3[3];
+  const int* pd;
+  const double* ph;
+  plane_grid(grid_dims, dx, d3, h3, &pd, &ph);
+  const int rc = extension3d(distance_function, nullptr, phi, mask, nullptr, nullptr, 0,
+                             spatial_discretization_order, pd, ph, nullptr,
+                             "computeDistanceFunction2d");
+  return rc == LSMGPU_SUCCESS ? 0 : -1;
+}
+
+int solveEikonalEquation2d(double* phi, double* speed, double* mask,
+                           int spatial_discretization_order, int* grid_dims, double* dx) {
+  if (spatial_discretization_order != 1 && spatial_discretization_order != 2) return 2;
+  int d3[3];
+  double h3[3];
+  const int* pd;
+  const double* ph;
+  plane_grid(grid_dims, dx, d3, h3, &pd, &ph);
+  const int rc = eikonal3d(phi, speed, mask, spatial_discretization_order, pd, ph, nullptr,
+                           "solveEikonalEquation2d");
+  return rc == LSMGPU_SUCCESS ? 0 : -1;
+}
+
 }  // extern "C"

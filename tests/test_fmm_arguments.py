@@ -118,3 +118,31 @@ def test_eikonal_rejects_bad_arguments(lib):
     d = np.array([2048, 2048, 1024], dtype=np.intc)
     assert lib.lsmgpu_eikonal3d(phi.ctypes.data, speed.ctypes.data, None, 1, d.ctypes.data,
                                 dx.ctypes.data, None) == INVALID_BOX
+
+
+def test_2d_entry_points_check_arguments(lib):
+    """The 2D forms (lsm_fast_marching_method.h:124-134, 179-185, 256-262)
+    keep the reference's return codes: 2 for a bad order, -1 otherwise."""
+    phi = np.zeros((5, 4))
+    out = np.zeros_like(phi)
+    dims = np.array([4, 5], dtype=np.intc)
+    dx = np.array([1.0, 1.0])
+    f = lib.computeDistanceFunction2d
+    f.argtypes, f.restype = [P] * 3 + [ctypes.c_int, P, P], ctypes.c_int
+    assert f(out.ctypes.data, phi.ctypes.data, None, 3, dims.ctypes.data, dx.ctypes.data) == 2
+    assert f(out.ctypes.data, None, None, 1, dims.ctypes.data, dx.ctypes.data) == -1
+    assert f(out.ctypes.data, phi.ctypes.data, None, 1, None, dx.ctypes.data) == -1
+    assert f(out.ctypes.data, phi.ctypes.data, None, 1, dims.ctypes.data, None) == -1
+    bad = np.array([1.0, -1.0])
+    assert f(out.ctypes.data, phi.ctypes.data, None, 2, dims.ctypes.data, bad.ctypes.data) == -1
+    assert "dx" in message(lib)
+    g = lib.computeExtensionFields2d
+    g.argtypes, g.restype = [P] * 6 + [ctypes.c_int, ctypes.c_int, P, P], ctypes.c_int
+    assert g(out.ctypes.data, None, phi.ctypes.data, None, None, None, 0, 0,
+             dims.ctypes.data, dx.ctypes.data) == 2
+    assert g(out.ctypes.data, None, phi.ctypes.data, None, None, None, -2, 1,
+             dims.ctypes.data, dx.ctypes.data) == -1
+    e = lib.solveEikonalEquation2d
+    e.argtypes, e.restype = [P] * 3 + [ctypes.c_int, P, P], ctypes.c_int
+    assert e(phi.ctypes.data, phi.ctypes.data, None, 5, dims.ctypes.data, dx.ctypes.data) == 2
+    assert e(phi.ctypes.data, None, None, 1, dims.ctypes.data, dx.ctypes.data) == -1

@@ -9,6 +9,7 @@
 * The same for the extension fields (computeExtensionFields3d) and the
   Eikonal solver (solveEikonalEquation3d).
 """
+import ctypes
 import os
 
 import numpy as np
@@ -230,3 +231,58 @@ def test_pylsmlib_distance_argument_errors():
         computeDistanceFunction(phi, dx=1.0, order=3)
     with pytest.raises(ValueError, match="mask"):
         computeDistanceFunction(phi, dx=1.0, mask=np.ones((5, 4)))
+
+
+def _ref_2d_and_3d():
+    lib = ctypes.CDLL(oracle.FMM_SO)
+    if not hasattr(lib, "computeDistanceFunction2d"):
+        pytest.skip("oracle/_ref/libfmm.so built without the 2D sources")
+    return lib
+
+
+@pytest.mark.parametrize("shape,seed,noise", [((30, 40), 3, 0.0), ((57, 41), 5, 0.01),
+                                              ((33, 64), 9, 0.01)])
+@pytest.mark.parametrize("order", [1, 2])
+def test_reference_2d_routines_equal_3d_on_one_plane(shape, seed, order, noise):
+    """The reference's 2D routines (lsm_fast_marching_method.h:124-262) give
+    bit for bit what its 3D routines give on a grid one plane thick. So the
+    2D entry points of the GPU library, which run the 3D solve on such a
+    grid, inherit the 3D parity."""
+    lib = _ref_2d_and_3d()
+    P = ctypes.c_void_p
+    ny, nx = shape
+    phi3, dx = seeded_spheres((1, ny, nx), seed, noise=noise)
+    phi = np.ascontiguousarray(phi3[0])
+    d2, d3 = np.array([nx, ny], dtype=np.intc), np.array([nx, ny, 1], dtype=np.intc)
+    h2, h3 = np.array(dx[:2]), np.array(dx)
+    a, b = np.zeros_like(phi), np.zeros_like(phi)
+    assert lib.computeDistanceFunction2d(a.ctypes.data_as(P), phi.ctypes.data_as(P), None, order,
+                                         d2.ctypes.data_as(P), h2.ctypes.data_as(P)) == 0
+    assert lib.computeDistanceFunction3d(b.ctypes.data_as(P), phi.ctypes.data_as(P), None, order,
+                                         d3.ctypes.data_as(P), h3.ctypes.data_as(P)) == 0
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    # extension fields: two sources
+    src = [np.ascontiguousarray(np.sin(3 * np.arange(phi.size)).reshape(phi.shape)),
+           np.ascontiguousarray(np.cos(np.arange(phi.size) / 7.0).reshape(phi.shape))]
+    outs = []
+    for d, h, fn in ((d2, h2, lib.computeExtensionFields2d), (d3, h3, lib.computeExtensionFields3d)):
+        dist = np.zeros_like(phi)
+        ext = [np.zeros_like(phi) for _ in src]
+        ext_p = (P * 2)(*[e.ctypes.data for e in ext])
+        src_p = (P * 2)(*[s_.ctypes.data for s_ in src])
+        assert fn(dist.ctypes.data_as(P), ext_p, phi.ctypes.data_as(P), None, src_p, None, 2,
+                  order, d.ctypes.data_as(P), h.ctypes.data_as(P)) == 0
+        outs.append([dist] + ext)
+    for x, y in zip(*outs):
+        assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
+    # Eikonal: phi <= 0 (shifted) as boundary data, varying speed
+    m = phi.min()
+    yy, xx = np.meshgrid(np.linspace(-1, 1, ny), np.linspace(-1, 1, nx), indexing="ij")
+    speed = np.ascontiguousarray(1 + 0.5 * np.sin(3 * xx) * np.cos(2 * yy))
+    e2 = np.ascontiguousarray(np.where(phi > 0, m - 1.0, phi) - m)
+    e3 = e2.copy()
+    assert lib.solveEikonalEquation2d(e2.ctypes.data_as(P), speed.ctypes.data_as(P), None, order,
+                                      d2.ctypes.data_as(P), h2.ctypes.data_as(P)) == 0
+    assert lib.solveEikonalEquation3d(e3.ctypes.data_as(P), speed.ctypes.data_as(P), None, order,
+                                      d3.ctypes.data_as(P), h3.ctypes.data_as(P)) == 0
+    assert np.array_equal(e2.view(np.uint64), e3.view(np.uint64))
