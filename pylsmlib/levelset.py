@@ -17,6 +17,7 @@ torch's current CUDA stream.
 """
 import math
 
+import numpy as np
 import torch
 
 from lsmlib_b200 import gpu, integrator
@@ -63,6 +64,15 @@ class Grid:
          self.khi_gb) = self.gb
         (self.ilo_fb, self.ihi_fb, self.jlo_fb, self.jhi_fb, self.klo_fb,
          self.khi_fb) = self.fb
+        # narrow-band parameters of the serial package's local method, as
+        # setIndexSpaceLimits sets them (lsm_grid.c:986-1005); carried into
+        # grid files
+        self.num_nb_levels = g
+        self.mark_gb, self.mark_D1, self.mark_D2, self.mark_D3 = 120, 119, 118, 117
+        self.mark_fb = 120 - g
+        wide = accuracy in ("HIGH", "VERY_HIGH")
+        self.beta = (3 if wide else 2) * self.dx[0]
+        self.gamma = (6 if wide else 4) * self.dx[0]
 
     # -- constructors of lsm_grid.c -------------------------------------------
     @classmethod
@@ -80,6 +90,65 @@ class Grid:
         grid_dims."""
         dx = [(h - l) / n for l, h, n in zip(x_lo, x_hi, grid_dims)]
         return cls(grid_dims, x_lo, x_hi, dx, accuracy)
+
+    # -- grid files (lsm_grid.c:613-787) -------------------------------------------
+    def write_binary(self, file_name, zip_status=0):
+        """writeGridToBinaryFile: the fields in the reference's order, native
+        ints and doubles with no padding; zip_status 1 (GZIP) or 2 (BZIP2)
+        compresses the file to name.gz / name.bz2.  Returns the name
+        written."""
+        from .data_arrays import _write
+        ints = lambda v: np.asarray(v, dtype=np.intc).tobytes()
+        reals = lambda v: np.asarray(v, dtype=np.float64).tobytes()
+        payload = b"".join([
+            ints([self.num_dims]), reals(self.x_lo), reals(self.x_hi),
+            reals(self.x_lo_ghostbox), reals(self.x_hi_ghostbox), ints(self.grid_dims),
+            ints(self.grid_dims_ghostbox), reals(self.dx), ints([self.num_gridpts]),
+            ints(self.gb), ints(self.fb), ints(self.D1_fb), ints(self.D2_fb),
+            ints(self.D3_fb), ints([self.num_nb_levels]),
+            bytes([self.mark_gb, self.mark_D1, self.mark_D2, self.mark_D3, self.mark_fb]),
+            reals([self.beta]), reals([self.gamma])])
+        return _write(file_name, payload, zip_status)
+
+    @classmethod
+    def read_binary(cls, file_name):
+        """readGridFromBinaryFile: every field as the file holds it (names
+        ending in .gz / .bz2 are decompressed).  The accuracy is the one
+        whose ghost width the file's narrow-band level count gives."""
+        from .data_arrays import _read
+        raw = _read(file_name)
+        pos = 0
+
+        def take(dtype, n):
+            nonlocal pos
+            size = np.dtype(dtype).itemsize * n
+            if pos + size > len(raw):
+                raise ValueError("%s: truncated grid file" % file_name)
+            v = np.frombuffer(raw[pos:pos + size], dtype=dtype)
+            pos += size
+            return v
+
+        g = cls.__new__(cls)
+        g.num_dims = int(take(np.intc, 1)[0])
+        for name in ("x_lo", "x_hi", "x_lo_ghostbox", "x_hi_ghostbox"):
+            setattr(g, name, tuple(float(v) for v in take(np.float64, 3)))
+        g.grid_dims = tuple(int(v) for v in take(np.intc, 3))
+        g.grid_dims_ghostbox = tuple(int(v) for v in take(np.intc, 3))
+        g.dx = tuple(float(v) for v in take(np.float64, 3))
+        g.num_gridpts = int(take(np.intc, 1)[0])
+        for name in ("gb", "fb", "D1_fb", "D2_fb", "D3_fb"):
+            setattr(g, name, tuple(int(v) for v in take(np.intc, 6)))
+        g.num_nb_levels = int(take(np.intc, 1)[0])
+        (g.mark_gb, g.mark_D1, g.mark_D2, g.mark_D3,
+         g.mark_fb) = (int(v) for v in take(np.uint8, 5))
+        g.beta = float(take(np.float64, 1)[0])
+        g.gamma = float(take(np.float64, 1)[0])
+        by_width = {w: a for a, w in ACCURACY_GHOSTCELLS.items()}
+        g.accuracy = by_width.get(g.num_nb_levels)
+        g.num_ghostcells = g.num_nb_levels
+        (g.ilo_gb, g.ihi_gb, g.jlo_gb, g.jhi_gb, g.klo_gb, g.khi_gb) = g.gb
+        (g.ilo_fb, g.ihi_fb, g.jlo_fb, g.jhi_fb, g.klo_fb, g.khi_fb) = g.fb
+        return g
 
     # -- fields -------------------------------------------------------------------
     @property

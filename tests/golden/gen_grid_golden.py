@@ -1,8 +1,9 @@
 """Writes tests/golden/grid_golden.json with the reference's own grid
-constructors.
+constructors, and grid_{very_high,high}.bin with its binary grid writer.
 
 createGridSetDx, createGridSetDxDyDz and createGridSetGridDims
-(src/serial/lsm_grid.c:50-250, with setIndexSpaceLimits* at :788-982) come
+(src/serial/lsm_grid.c:50-250, with setIndexSpaceLimits* at :788-1040) and
+writeGridToBinaryFile (:613-676) come
 from oracle/_ref/libgrid.so, built by `make -C oracle ref` from the reference
 sources. Run from the repository root:
 
@@ -52,7 +53,10 @@ def fields(g):
             "x_lo_ghostbox": list(g.x_lo_ghostbox), "x_hi_ghostbox": list(g.x_hi_ghostbox),
             "grid_dims": list(g.grid_dims), "grid_dims_ghostbox": list(g.grid_dims_ghostbox),
             "dx": list(g.dx), "num_gridpts": g.num_gridpts, "gb": box("gb"), "fb": box("fb"),
-            "D1_fb": box("D1_fb"), "D2_fb": box("D2_fb"), "D3_fb": box("D3_fb")}
+            "D1_fb": box("D1_fb"), "D2_fb": box("D2_fb"), "D3_fb": box("D3_fb"),
+            "num_nb_levels": g.num_nb_levels,
+            "marks": [g.mark_gb, g.mark_D1, g.mark_D2, g.mark_D3, g.mark_fb],
+            "beta": g.beta, "gamma": g.gamma}
 
 
 def main():
@@ -78,6 +82,14 @@ def main():
             lib.destroyGrid(p)
     with open(os.path.join(HERE, "grid_golden.json"), "w") as f:
         json.dump(out, f, indent=0)
+    # binary grid files: the second set_dxdydz case at two accuracies
+    lib.writeGridToBinaryFile.argtypes = [ctypes.POINTER(RefGrid), ctypes.c_char_p,
+                                          ctypes.c_int]
+    _, h, lo, hi = CASES[3]
+    for acc, name in ((3, "very_high"), (2, "high")):
+        p = lib.createGridSetDxDyDz(3, *h, D3(*lo), D3(*hi), acc)
+        lib.writeGridToBinaryFile(p, os.path.join(HERE, "grid_%s.bin" % name).encode(), 0)
+        lib.destroyGrid(p)
 
 
 if __name__ == "__main__":

@@ -63,7 +63,9 @@ def as_fields(g):
             "grid_dims": list(g.grid_dims), "grid_dims_ghostbox": list(g.grid_dims_ghostbox),
             "dx": list(g.dx), "num_gridpts": g.num_gridpts, "gb": list(g.gb),
             "fb": list(g.fb), "D1_fb": list(g.D1_fb), "D2_fb": list(g.D2_fb),
-            "D3_fb": list(g.D3_fb)}
+            "D3_fb": list(g.D3_fb), "num_nb_levels": g.num_nb_levels,
+            "marks": [g.mark_gb, g.mark_D1, g.mark_D2, g.mark_D3, g.mark_fb],
+            "beta": g.beta, "gamma": g.gamma}
 
 
 GOLDEN = json.load(open(os.path.join(GOLDEN_DIR, "grid_golden.json")))
@@ -111,3 +113,44 @@ def test_grid_matches_reference_live_on_seeded_extents():
             Grid.set_grid_dims(tuple(int(v) for v in dims), tuple(lo), tuple(hi),
                                gen.ACCURACY[acc]))
         lib.destroyGrid(p)
+
+
+# ---- binary grid files (lsm_grid.c:613-787) ---------------------------------------
+
+def _golden_binary_case():
+    case = [c for c in GOLDEN if c["ctor"] == "set_dxdydz"][4]   # the second such case
+    return case["arg"], case["x_lo"], case["x_hi"]
+
+
+@pytest.mark.parametrize("accuracy,name", [("VERY_HIGH", "very_high"), ("HIGH", "high")])
+def test_binary_grid_file_matches_reference_writer(tmp_path, accuracy, name):
+    """writeGridToBinaryFile of the reference wrote the golden files; ours
+    writes the same bytes and reads them back field by field."""
+    h, lo, hi = _golden_binary_case()
+    g = Grid.set_dx(tuple(h), tuple(lo), tuple(hi), accuracy)
+    golden = os.path.join(GOLDEN_DIR, "grid_%s.bin" % name)
+    ours = g.write_binary(str(tmp_path / "grid.bin"))
+    assert open(ours, "rb").read() == open(golden, "rb").read()
+    back = Grid.read_binary(golden)
+    assert as_fields(back) == as_fields(g) and back.accuracy == accuracy
+
+
+@pytest.mark.parametrize("zip_status,suffix", [(0, ""), (1, ".gz"), (2, ".bz2")])
+def test_reference_reads_our_binary_grid_files(tmp_path, zip_status, suffix):
+    lib_path = os.path.join(os.path.dirname(GOLDEN_DIR), "..", "oracle", "_ref", "libgrid.so")
+    if not os.path.exists(lib_path):
+        pytest.skip("oracle/_ref/libgrid.so not built (make -C oracle ref)")
+    spec = importlib.util.spec_from_file_location(
+        "gen_grid_golden", os.path.join(GOLDEN_DIR, "gen_grid_golden.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    lib = ctypes.CDLL(lib_path)
+    lib.readGridFromBinaryFile.restype = ctypes.POINTER(gen.RefGrid)
+    lib.readGridFromBinaryFile.argtypes = [ctypes.c_char_p]
+    lib.destroyGrid.argtypes = [ctypes.POINTER(gen.RefGrid)]
+    g = Grid.set_grid_dims((21, 17, 9), (-1.0, 0.0, 0.5), (1.0, 0.8, 1.4), "MEDIUM")
+    name = g.write_binary(str(tmp_path / "grid.bin"), zip_status=zip_status)
+    assert name.endswith("grid.bin" + suffix)
+    p = lib.readGridFromBinaryFile(name.encode())
+    assert gen.fields(p.contents) == as_fields(g)
+    lib.destroyGrid(p)
