@@ -233,6 +233,33 @@ def test_pylsmlib_distance_argument_errors():
         computeDistanceFunction(phi, dx=1.0, mask=np.ones((5, 4)))
 
 
+def test_pylsmlib_reference_doctest_errors():
+    """The argument errors of the reference package's own doctests
+    (pylsmlib/pylsmlib/__init__.py:442-449, 504-511, 625-635, 770-794), with
+    their messages; all are raised before any GPU work."""
+    from pylsmlib import computeDistanceFunction as distance
+    from pylsmlib import computeExtensionFields, travel_time
+    with pytest.raises(ValueError, match="dx must be of length len"):
+        distance([[-1, 1], [1, 1]], dx=(1, 2, 3))
+    with pytest.raises(ValueError, match="phi and speed must have the same shape"):
+        computeExtensionFields([[-1, 1], [1, 1]], speed=[1, 1])
+    for order in (0, 3):
+        with pytest.raises(ValueError, match="order must be 1 or 2"):
+            distance([-1, 1], order=order)
+    with pytest.raises(ValueError, match="dx must be greater than zero"):
+        distance([1, 0, 1, 1], 0)
+    with pytest.raises(ValueError, match="dx must be of length len"):
+        distance([0, 0, 1, 0, 0], [0, 0, 1, 0, 0])
+    with pytest.raises(ValueError, match="phi and speed must have the same shape"):
+        travel_time([-1, 1], [2])
+    with pytest.raises(ValueError, match="phi and speed must have the same shape"):
+        travel_time([0, 0, 1, 1], 2)
+    with pytest.raises(ValueError, match="dx must be of length len"):
+        travel_time([-1, 1], [2, 2], [2, 2, 2, 2])
+    with pytest.raises(ValueError, match="could not convert string to float"):
+        distance(np.array(["a", "b"]))
+
+
 def _ref_2d_and_3d():
     lib = ctypes.CDLL(oracle.FMM_SO)
     if not hasattr(lib, "computeDistanceFunction2d"):

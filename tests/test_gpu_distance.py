@@ -352,3 +352,34 @@ def test_2d_entry_points_reproduce_reference_golden(lib):
         assert eik_fn(sol.ctypes.data, speed.ctypes.data, None, order, dims.ctypes.data,
                       h.ctypes.data) == 0
         assert same_bits(sol, z["spheres2d|eik%d" % order][0])
+
+
+# ---- the reference package's own known-answer doctests, through pylsmlib ---------
+
+from fmm_reference_cases import CASES as REFERENCE_CASES  # noqa: E402
+
+
+class PylsmlibBackend:
+    """pylsmlib's front door on the GPU, in the reference package's calls."""
+
+    @staticmethod
+    def distance(phi, dx, order):
+        from pylsmlib import computeDistanceFunction
+        return computeDistanceFunction(phi, dx=dx, order=order)
+
+    @staticmethod
+    def extension(phi, speed, dx, order, ext_mask):
+        from pylsmlib import computeExtensionFields
+        return computeExtensionFields(phi, speed, dx=dx, order=order, ext_mask=ext_mask)
+
+    @staticmethod
+    def travel_time(phi, speed, dx, order):
+        from pylsmlib import travel_time
+        return travel_time(phi, speed, dx, order)
+
+
+@pytest.mark.parametrize("case", REFERENCE_CASES, ids=[c.__name__ for c in REFERENCE_CASES])
+def test_pylsmlib_reference_doctest_case(case):
+    """pylsmlib/pylsmlib/__init__.py:196-800; the same cases pass on the
+    reference's own routines and on the oracle (test_fmm_reference_doctests.py)."""
+    case(PylsmlibBackend())
