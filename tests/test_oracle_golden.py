@@ -23,3 +23,21 @@ def test_every_routine_has_golden_cases():
     from lsmlib_b200 import abi
     syms = {c[1] for c in CASES}
     assert syms == set(abi.SIGNATURES)
+
+
+# ---- the reference's boundary-condition examples as a property --------------------
+
+import oracle  # noqa: E402
+from neumann_property import LIMIT, boundary_errors  # noqa: E402
+
+
+@pytest.mark.parametrize("scheme", sorted(LIMIT))
+@pytest.mark.parametrize("impl", ["reference", "oracle"])
+def test_neumann_fill_zeroes_normal_derivatives(impl, scheme):
+    if impl == "reference":
+        if not oracle.reference_available():
+            pytest.skip("oracle/_ref/libref.so not built")
+        tb = oracle.reference_toolbox()
+    else:
+        tb = oracle.oracle_toolbox()
+    assert max(boundary_errors(tb.call, scheme)) <= LIMIT[scheme]
