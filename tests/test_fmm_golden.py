@@ -313,3 +313,54 @@ def test_reference_2d_routines_equal_3d_on_one_plane(shape, seed, order, noise):
     assert lib.solveEikonalEquation3d(e3.ctypes.data_as(P), speed.ctypes.data_as(P), None, order,
                                       d3.ctypes.data_as(P), h3.ctypes.data_as(P)) == 0
     assert np.array_equal(e2.view(np.uint64), e3.view(np.uint64))
+
+
+# ---- the reference's fast marching examples ------------------------------------
+
+import fmm_example_cases as examples  # noqa: E402
+
+
+def _plane(a):
+    return np.ascontiguousarray(a)[None]
+
+
+@pytest.mark.skipif(not oracle.fmm_available(), reason="oracle/_ref/libfmm.so not built")
+def test_reference_examples_oracle_matches_reference():
+    """The inputs of examples/serial/fast_marching_method/*.c through the
+    routines each example calls (the 2D ones for the 2D examples), against
+    the oracle's 3D march (one plane thick for 2D), bit for bit."""
+    lib = _ref_2d_and_3d()
+    P = ctypes.c_void_p
+    phi, dx = examples.distance_3d()
+    want = oracle.oracle_fmm()(phi, 2, dx)
+    assert np.array_equal(oracle.reference_fmm()(phi, 2, dx).view(np.uint64),
+                          want.view(np.uint64))
+    phi, dx = examples.distance_2d()
+    out = np.zeros_like(phi)
+    d = np.array(phi.shape[::-1], dtype=np.intc)
+    h = np.array(dx)
+    assert lib.computeDistanceFunction2d(out.ctypes.data_as(P), phi.ctypes.data_as(P), None, 2,
+                                         d.ctypes.data_as(P), h.ctypes.data_as(P)) == 0
+    want = oracle.oracle_fmm()(_plane(phi), 2, dx + [1.0])[0]
+    assert np.array_equal(out.view(np.uint64), want.view(np.uint64))
+    phi, src, dx = examples.extension_2d()
+    dist = np.zeros_like(phi)
+    ext = [np.zeros_like(phi) for _ in src]
+    ext_p = (P * 2)(*[e.ctypes.data for e in ext])
+    src_p = (P * 2)(*[s_.ctypes.data for s_ in src])
+    d = np.array(phi.shape[::-1], dtype=np.intc)
+    h = np.array(dx)
+    assert lib.computeExtensionFields2d(dist.ctypes.data_as(P), ext_p, phi.ctypes.data_as(P),
+                                        None, src_p, None, 2, 2, d.ctypes.data_as(P),
+                                        h.ctypes.data_as(P)) == 0
+    wd, wf = oracle.oracle_extension()(_plane(phi), [_plane(s_) for s_ in src], 2, dx + [1.0])
+    for got, want in zip([dist] + ext, [wd[0]] + [f[0] for f in wf]):
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+    phi, speed, dx = examples.eikonal_2d()
+    sol = phi.copy()
+    d = np.array(phi.shape[::-1], dtype=np.intc)
+    h = np.array(dx)
+    assert lib.solveEikonalEquation2d(sol.ctypes.data_as(P), speed.ctypes.data_as(P), None, 2,
+                                      d.ctypes.data_as(P), h.ctypes.data_as(P)) == 0
+    want = oracle.oracle_eikonal()(_plane(phi), _plane(speed), 2, dx + [1.0])[0]
+    assert np.array_equal(sol.view(np.uint64), want.view(np.uint64))

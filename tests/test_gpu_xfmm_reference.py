@@ -96,3 +96,56 @@ def test_pylsmlib_reference_doctest_case(case):
     """pylsmlib/pylsmlib/__init__.py:196-800; the same cases pass on the
     reference's own routines and on the oracle (test_fmm_reference_doctests.py)."""
     case(PylsmlibBackend())
+
+
+# ---- the reference's fast marching examples, through the C entry points ------------
+
+import fmm_example_cases as examples  # noqa: E402
+import oracle  # noqa: E402
+
+
+def test_reference_examples_match_oracle(lib):
+    """The inputs of examples/serial/fast_marching_method/*.c through the
+    entry points each example calls (computeDistanceFunction3d and the 2D
+    forms), on host arrays, bit for bit against the oracle (one plane thick
+    for 2D)."""
+    P = ctypes.c_void_p
+    f3 = lib.computeDistanceFunction3d
+    f2 = lib.computeDistanceFunction2d
+    for f in (f3, f2):
+        f.argtypes, f.restype = [P] * 3 + [ctypes.c_int, P, P], ctypes.c_int
+    e2 = lib.computeExtensionFields2d
+    e2.argtypes, e2.restype = [P] * 6 + [ctypes.c_int, ctypes.c_int, P, P], ctypes.c_int
+    k2 = lib.solveEikonalEquation2d
+    k2.argtypes, k2.restype = [P] * 3 + [ctypes.c_int, P, P], ctypes.c_int
+
+    def grid(phi, dx):
+        return np.array(phi.shape[::-1], dtype=np.intc), np.array(dx, dtype=np.float64)
+
+    phi, dx = examples.distance_3d()
+    out = np.full_like(phi, np.nan)
+    d, h = grid(phi, dx)
+    assert f3(out.ctypes.data, phi.ctypes.data, None, 2, d.ctypes.data, h.ctypes.data) == 0
+    assert same_bits(out, oracle.oracle_fmm()(phi, 2, dx))
+    phi, dx = examples.distance_2d()
+    out = np.full_like(phi, np.nan)
+    d, h = grid(phi, dx)
+    assert f2(out.ctypes.data, phi.ctypes.data, None, 2, d.ctypes.data, h.ctypes.data) == 0
+    assert same_bits(out, oracle.oracle_fmm()(phi[None], 2, dx + [1.0])[0])
+    phi, src, dx = examples.extension_2d()
+    dist = np.full_like(phi, np.nan)
+    ext = [np.full_like(phi, np.nan) for _ in src]
+    ext_p = (P * 2)(*[e.ctypes.data for e in ext])
+    src_p = (P * 2)(*[s.ctypes.data for s in src])
+    d, h = grid(phi, dx)
+    assert e2(dist.ctypes.data, ctypes.cast(ext_p, P), phi.ctypes.data, None,
+              ctypes.cast(src_p, P), None, 2, 2, d.ctypes.data, h.ctypes.data) == 0
+    wd, wf = oracle.oracle_extension()(phi[None], [s[None] for s in src], 2, dx + [1.0])
+    assert same_bits(dist, wd[0])
+    for got, want in zip(ext, wf):
+        assert same_bits(got, want[0])
+    phi, speed, dx = examples.eikonal_2d()
+    sol = phi.copy()
+    d, h = grid(phi, dx)
+    assert k2(sol.ctypes.data, speed.ctypes.data, None, 2, d.ctypes.data, h.ctypes.data) == 0
+    assert same_bits(sol, oracle.oracle_eikonal()(phi[None], speed[None], 2, dx + [1.0])[0])
