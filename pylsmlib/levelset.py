@@ -110,6 +110,43 @@ class Grid:
             reals([self.beta]), reals([self.gamma])])
         return _write(file_name, payload, zip_status)
 
+    def describe(self):
+        """printGrid (lsm_grid.c:322-440): the grid as the reference prints it,
+        3D form (C's %g for reals, %u for the marks)."""
+        r = lambda v: "%g" % v
+
+        def box(b):
+            return "[%d,%d] x [%d,%d] x [%d,%d]" % tuple(b)
+        lines = [
+            "Number of dimensions: %d" % self.num_dims,
+            "Geometric limits (without ghostcells): [%s,%s] x [%s,%s] x [%s,%s]" % tuple(
+                r(v) for pair in zip(self.x_lo, self.x_hi) for v in pair),
+            "Geometric limits (with ghostcells): [%s,%s] x [%s,%s] x [%s,%s]" % tuple(
+                r(v) for pair in zip(self.x_lo_ghostbox, self.x_hi_ghostbox) for v in pair),
+            "Grid size (without ghostcells): %d x %d x %d" % tuple(self.grid_dims),
+            "Grid size (with ghostcells): %d x %d x %d" % tuple(self.grid_dims_ghostbox),
+            "Grid spacing: dx = %s, dy = %s, dz = %s " % tuple(r(v) for v in self.dx),
+            "Total number of grid points: %d" % self.num_gridpts,
+            "Ghost box index limits: " + box(self.gb),
+            "Fill box index limits: " + box(self.fb),
+            "1st order differences fill box: " + box(self.D1_fb),
+            "2nd order differences fill box: " + box(self.D2_fb),
+            "3rd order differences fill box: " + box(self.D3_fb),
+            "Number of narrow band levels (local method) %d" % self.num_nb_levels,
+            "Boundary layer marks (local method) gb %u D1 %u D2 %u D3 %u fb %u" % (
+                self.mark_gb, self.mark_D1, self.mark_D2, self.mark_D3, self.mark_fb),
+            "Narrow band width (local method) beta(inner) %s gamma(outer) %s" % (
+                r(self.beta), r(self.gamma)),
+        ]
+        return "\n".join(lines) + "\n"
+
+    def write_ascii(self, file_name, zip_status=0):
+        """writeGridToAsciiFile (lsm_grid.c:601-611): the printGrid text,
+        optionally compressed to name.gz / name.bz2.  Returns the name
+        written."""
+        from .data_arrays import _write
+        return _write(file_name, self.describe().encode(), zip_status)
+
     @classmethod
     def read_binary(cls, file_name):
         """readGridFromBinaryFile: every field as the file holds it (names

@@ -1,5 +1,6 @@
 """Writes tests/golden/grid_golden.json with the reference's own grid
-constructors, and grid_{very_high,high}.bin with its binary grid writer.
+constructors, grid_{very_high,high}.bin with its binary grid writer and
+grid_very_high.txt with its ASCII grid writer.
 
 createGridSetDx, createGridSetDxDyDz and createGridSetGridDims
 (src/serial/lsm_grid.c:50-250, with setIndexSpaceLimits* at :788-1040) and
@@ -86,9 +87,13 @@ def main():
     lib.writeGridToBinaryFile.argtypes = [ctypes.POINTER(RefGrid), ctypes.c_char_p,
                                           ctypes.c_int]
     _, h, lo, hi = CASES[3]
+    lib.writeGridToAsciiFile.argtypes = [ctypes.POINTER(RefGrid), ctypes.c_char_p,
+                                         ctypes.c_int]
     for acc, name in ((3, "very_high"), (2, "high")):
         p = lib.createGridSetDxDyDz(3, *h, D3(*lo), D3(*hi), acc)
         lib.writeGridToBinaryFile(p, os.path.join(HERE, "grid_%s.bin" % name).encode(), 0)
+        if name == "very_high":
+            lib.writeGridToAsciiFile(p, os.path.join(HERE, "grid_%s.txt" % name).encode(), 0)
         lib.destroyGrid(p)
 
 

@@ -154,3 +154,48 @@ def test_reference_reads_our_binary_grid_files(tmp_path, zip_status, suffix):
     p = lib.readGridFromBinaryFile(name.encode())
     assert gen.fields(p.contents) == as_fields(g)
     lib.destroyGrid(p)
+
+
+def test_ascii_grid_file_matches_reference_writer(tmp_path):
+    """writeGridToAsciiFile (printGrid) of the reference wrote the golden
+    text; ours writes the same bytes."""
+    h, lo, hi = _golden_binary_case()
+    g = Grid.set_dx(tuple(h), tuple(lo), tuple(hi), "VERY_HIGH")
+    ours = g.write_ascii(str(tmp_path / "grid.txt"))
+    assert open(ours, "rb").read() == open(os.path.join(GOLDEN_DIR, "grid_very_high.txt"),
+                                           "rb").read()
+
+
+def test_ascii_grid_description_matches_reference_live(tmp_path):
+    """Every golden grid printed by the reference's printGrid and by ours."""
+    lib_path = os.path.join(os.path.dirname(GOLDEN_DIR), "..", "oracle", "_ref", "libgrid.so")
+    if not os.path.exists(lib_path):
+        pytest.skip("oracle/_ref/libgrid.so not built (make -C oracle ref)")
+    spec = importlib.util.spec_from_file_location(
+        "gen_grid_golden", os.path.join(GOLDEN_DIR, "gen_grid_golden.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    lib = ctypes.CDLL(lib_path)
+    for f in ("createGridSetDx", "createGridSetDxDyDz", "createGridSetGridDims"):
+        getattr(lib, f).restype = ctypes.POINTER(gen.RefGrid)
+    lib.createGridSetDx.argtypes = [ctypes.c_int, ctypes.c_double, gen.D3, gen.D3, ctypes.c_int]
+    lib.createGridSetDxDyDz.argtypes = [ctypes.c_int] + [ctypes.c_double] * 3 + [
+        gen.D3, gen.D3, ctypes.c_int]
+    lib.createGridSetGridDims.argtypes = [ctypes.c_int, gen.I3, gen.D3, gen.D3, ctypes.c_int]
+    lib.writeGridToAsciiFile.argtypes = [ctypes.POINTER(gen.RefGrid), ctypes.c_char_p,
+                                         ctypes.c_int]
+    lib.destroyGrid.argtypes = [ctypes.POINTER(gen.RefGrid)]
+    name = str(tmp_path / "ref.txt")
+    for case in GOLDEN:
+        acc = gen.ACCURACY.index(case["accuracy"])
+        lo, hi, arg = gen.D3(*case["x_lo"]), gen.D3(*case["x_hi"]), case["arg"]
+        if case["ctor"] == "set_dx":
+            p = lib.createGridSetDx(3, arg, lo, hi, acc)
+        elif case["ctor"] == "set_dxdydz":
+            p = lib.createGridSetDxDyDz(3, *arg, lo, hi, acc)
+        else:
+            p = lib.createGridSetGridDims(3, gen.I3(*arg), lo, hi, acc)
+        lib.writeGridToAsciiFile(p, name.encode(), 0)
+        lib.destroyGrid(p)
+        g = ours(case["ctor"], case["arg"], case["x_lo"], case["x_hi"], case["accuracy"])
+        assert open(name).read() == g.describe(), case
