@@ -41,3 +41,24 @@ def test_neumann_fill_zeroes_normal_derivatives(impl, scheme):
     else:
         tb = oracle.oracle_toolbox()
     assert max(boundary_errors(tb.call, scheme)) <= LIMIT[scheme]
+
+
+def test_heaviside_matches_reference_macro():
+    """LSM_HEAVISIDE (lsm_calculus_toolbox.h:41-45), compiled from the
+    reference header (oracle/_ref/libcalculus.so), against the oracle's
+    restatement that the adjoint loss uses: bit for bit, across the smoothed
+    band and past both ends, for two band widths."""
+    import ctypes
+    import os
+
+    import numpy as np
+    path = os.path.join(os.path.dirname(oracle.__file__), "_ref", "libcalculus.so")
+    if not os.path.exists(path):
+        pytest.skip("oracle/_ref/libcalculus.so not built (make -C oracle ref)")
+    lib = ctypes.CDLL(path)
+    lib.ref_heaviside.restype = ctypes.c_double
+    lib.ref_heaviside.argtypes = [ctypes.c_double, ctypes.c_double]
+    for eps in (1.5 / 128, 0.3):
+        x = np.concatenate([np.linspace(-2 * eps, 2 * eps, 4001), [-eps, eps, 0.0]])
+        ref = np.array([lib.ref_heaviside(v, eps) for v in x])
+        assert np.array_equal(ref.view(np.uint64), oracle.heaviside(x, eps).view(np.uint64))
