@@ -611,13 +611,13 @@ def run_distance(n=256, n_cpu=128, reps=3):
                 if size == n_cpu:
                     t0 = time.perf_counter()
                     if solver == "distance":
-                        want = [oracle.oracle_fmm()(phi.T, order, dx)]
+                        want = [oracle.oracle_fmm(ordered=True)(phi.T, order, dx)]
                     elif solver == "extension":
-                        dist, fields = oracle.oracle_extension()(phi.T, [x.T for x in srcs],
+                        dist, fields = oracle.oracle_extension(ordered=True)(phi.T, [x.T for x in srcs],
                                                                  order, dx)
                         want = [dist] + fields
                     else:
-                        want = [oracle.oracle_eikonal()(eik_data.T, speed.T, order, dx)]
+                        want = [oracle.oracle_eikonal(ordered=True)(eik_data.T, speed.T, order, dx)]
                     t_cpu = time.perf_counter() - t0
                     got = [host.T] + ([x.T for x in hext] if solver == "extension" else [])
                     r["cpu_oracle"] = {"ms": round(1e3 * t_cpu, 1), "value": pts / t_cpu,

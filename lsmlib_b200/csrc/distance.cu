@@ -26,9 +26,15 @@
 //   3. points no front reaches keep the reference's default -1; points with
 //      mask < 0 are outside the domain and hold LSMLIB_REAL_MAX.
 // Built with --fmad=false so the update rounds as the reference's C does.
-// Exact ties in time (equal keys) are broken by neighbour slot here and by
-// heap position in the reference; only there can the results differ.
+// "Before" is the order of (acceptance time, linear point index): the time
+// decides, and the index breaks exact ties.  Where no two keys tie this is
+// the heap's pop order.  Where keys tie exactly (symmetric inputs, flat
+// fronts, quantised data) the reference's binary heap pops the tied points in
+// an order set by its whole history of insertions and removals, which no
+// rule over a neighbourhood can reproduce; there the result is that of the
+// same march popping ties by index.
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <string>
 
@@ -62,6 +68,19 @@ __device__ __forceinline__ bool tless(const Time3& x, const Time3& y) {
 
 __device__ __forceinline__ bool tequal(const Time3& x, const Time3& y) {
   return x.a == y.a && x.b == y.b && x.c == y.c;
+}
+
+// point x (time tx, linear index ix) is accepted before point y: by time,
+// exact ties by index
+__device__ __forceinline__ bool kless(const Time3& tx, long ix, const Time3& ty, long iy) {
+  if (tless(tx, ty)) return true;
+  if (tless(ty, tx)) return false;
+  return ix < iy;
+}
+
+// linear index of the k-th point (k = 1, 2) from o in slot q's direction
+__device__ __forceinline__ long nb_index(long o, const long s[3], int q, int k) {
+  return o + ((q & 1) ? k : -k) * s[q >> 1];
 }
 
 // the time of a point with key ``a`` whose trigger has time ``x`` (no free
@@ -219,16 +238,16 @@ struct Stencil {
 // neighbour is taken when included and replaced by the plus one when its
 // |d| is strictly smaller.  At second order the next point in the chosen
 // direction counts when it was KNOWN at the update -- a front point, or a
-// free point accepted before the trigger (time ``trig``; the front phase
-// comes before every free point) -- and its |d| is not above the
-// neighbour's.  ``cterm`` is what the constant term loses: 1 for the
+// free point accepted before the trigger (time ``trig``, index ``itrig``;
+// the front phase comes before every free point) -- and its |d| is not above
+// the neighbour's.  ``cterm`` is what the constant term loses: 1 for the
 // distance function, 1/F^2 for the Eikonal solver (lsm_FMM_eikonal.c:427,
 // :621).  Returns the discriminant B^2 - 4AC.
 template <int ORDER>
 __device__ __forceinline__ double fmm_coeffs(const Stencil& n, int incl,
-                                             const Time3& trig, bool has_trigger,
-                                             const double i2[3], double cterm, double& A,
-                                             double& B) {
+                                             const Time3& trig, long itrig, bool has_trigger,
+                                             long o, const long s3[3], const double i2[3],
+                                             double cterm, double& A, double& B) {
   double C = 0;
   A = 0;
   B = 0;
@@ -245,7 +264,8 @@ __device__ __forceinline__ double fmm_coeffs(const Stencil& n, int incl,
       u2 = DBL_MAX;
       sw = 0;
       if (ORDER == 2 && (n.has2 & (1 << q)) && fabs(n.v2[q]) <= fabs(u1) &&
-          ((n.front2 & (1 << q)) || (has_trigger && tless(n.t2[q], trig)))) {
+          ((n.front2 & (1 << q)) ||
+           (has_trigger && kless(n.t2[q], nb_index(o, s3, q, 2), trig, itrig)))) {
         u2 = n.v2[q];
         sw = 1;
       }
@@ -319,7 +339,7 @@ __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
                                           const unsigned char* st, long o, const int c[3],
                                           const int n[3], const long s[3], const double i2[3],
                                           const Eik& E, Stencil& nb, double& val, Time3& tv,
-                                          int& incl_out, Time3& trig_out,
+                                          int& incl_out, Time3& trig_out, long& itrig_out,
                                           bool& trig_free_out) {
   // every load first, at in-range addresses (the point itself stands in
   // for a neighbour off the grid), so that they are in flight together
@@ -370,37 +390,46 @@ __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
   const int free1 = nb.has1 & ~nb.front1;
   const double cterm = EIK ? 1 / E.speed[o] / E.speed[o] : 1.0;
   const double none = EIK ? E.phi0[o] : -1.0;   // the value without an update
-  Time3 cap{INFINITY, INFINITY, INFINITY};   // only neighbours before this
+  // only neighbours before this (time, index)
+  Time3 cap{INFINITY, INFINITY, INFINITY};
+  long icap = LONG_MAX;
   for (;;) {
     int incl = nb.front1;
     bool have = incl != 0, trig_free = false;
     Time3 trig{-INFINITY, -1.0, -1.0};
+    long itrig = -1;
     double cur = none;
     if (have) {
       double A, B;
-      const double disc = fmm_coeffs<ORDER>(nb, incl, trig, false, i2, cterm, A, B);
+      const double disc =
+          fmm_coeffs<ORDER>(nb, incl, trig, itrig, false, o, s, i2, cterm, A, B);
       if (disc >= 0) cur = fmm_root<EIK>(A, B, disc);
     }
     for (int rem = free1; rem;) {
-      // the earliest remaining free neighbour (ties by slot)
-      int best = 0;
+      // the earliest remaining free neighbour
+      int best = -1;
       Time3 bt{INFINITY, INFINITY, INFINITY};
+      long ib = LONG_MAX;
 #pragma unroll
       for (int q = 5; q >= 0; q--) {
         if (!(rem & (1 << q))) continue;
-        if (!tless(bt, nb.t1[q])) {
+        const long iq = nb_index(o, s, q, 1);
+        if (best < 0 || kless(nb.t1[q], iq, bt, ib)) {
           best = q;
           bt = nb.t1[q];
+          ib = iq;
         }
       }
       rem &= ~(1 << best);
-      if (!tless(bt, cap)) break;
-      if (have && !tless(bt, tafter(trig, fabs(cur), trig_free))) break;
+      if (!kless(bt, ib, cap, icap)) break;
+      if (have && !kless(bt, ib, tafter(trig, fabs(cur), trig_free), o)) break;
       incl |= 1 << best;
       trig = bt;
+      itrig = ib;
       trig_free = true;
       double A, B;
-      const double disc = fmm_coeffs<ORDER>(nb, incl, trig, true, i2, cterm, A, B);
+      const double disc =
+          fmm_coeffs<ORDER>(nb, incl, trig, itrig, true, o, s, i2, cterm, A, B);
       if (disc >= 0) cur = fmm_root<EIK>(A, B, disc);
       have = true;
     }
@@ -408,21 +437,28 @@ __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
     // the earliest neighbour in the set not accepted before the point
     bool bad = false;
     Time3 badt{INFINITY, INFINITY, INFINITY};
+    long ibad = LONG_MAX;
 #pragma unroll
-    for (int q = 0; q < 6; q++)
-      if ((incl & free1 & (1 << q)) && !tless(nb.t1[q], t) && tless(nb.t1[q], badt)) {
+    for (int q = 0; q < 6; q++) {
+      if (!(incl & free1 & (1 << q))) continue;
+      const long iq = nb_index(o, s, q, 1);
+      if (!kless(nb.t1[q], iq, t, o) && kless(nb.t1[q], iq, badt, ibad)) {
         bad = true;
         badt = nb.t1[q];
+        ibad = iq;
       }
+    }
     if (!bad) {
       val = cur;
       tv = t;
       incl_out = incl;
       trig_out = trig;
+      itrig_out = itrig;
       trig_free_out = trig_free;
       return true;
     }
     cap = badt;
+    icap = ibad;
   }
 }
 
@@ -436,8 +472,9 @@ __device__ __forceinline__ bool fmm_point(const double* d, const Time3* tm,
 // did.
 template <int ORDER>
 __device__ __forceinline__ bool fmm_ext(const Stencil& n, int incl, const Time3& trig,
-                                        bool has_trigger, double val, const double i2[3],
-                                        const ExtSet& X, long o, const long s[3]) {
+                                        long itrig, bool has_trigger, double val,
+                                        const double i2[3], const ExtSet& X, long o,
+                                        const long s[3]) {
   double g[3];
   long a[3];
   bool used[3];
@@ -455,7 +492,8 @@ __device__ __forceinline__ bool fmm_ext(const Stencil& n, int incl, const Time3&
       sw = 0;
       side_used = side;
       if (ORDER == 2 && (n.has2 & (1 << q)) && fabs(n.v2[q]) <= fabs(u1) &&
-          ((n.front2 & (1 << q)) || (has_trigger && tless(n.t2[q], trig)))) {
+          ((n.front2 & (1 << q)) ||
+           (has_trigger && kless(n.t2[q], nb_index(o, s, q, 2), trig, itrig)))) {
         u2 = n.v2[q];
         sw = 1;
       }
@@ -599,11 +637,12 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
     Stencil nb;
     double val;
     Time3 tv, trig;
+    long itrig;
     int incl;
     bool trig_free;
     bool ext_changed = false;
     const bool reached = fmm_point<ORDER, EIK>(d, tm, st, o, c, nn, s, i2, E, nb, val, tv,
-                                               incl, trig, trig_free);
+                                               incl, trig, itrig, trig_free);
     if (self != kFree) {
       L.new_f[w] = 0;
       continue;
@@ -619,7 +658,7 @@ k_fmm_pass(double* d, Time3* tm, const unsigned char* st, int nx, int ny, int nz
       const unsigned long long bits = __double_as_longlong(tv.a);
       minrej = bits < minrej ? bits : minrej;
     } else if (!EIK && X.nf) {
-      ext_changed = fmm_ext<ORDER>(nb, incl, trig, trig_free, val, i2, X, o, s);
+      ext_changed = fmm_ext<ORDER>(nb, incl, trig, itrig, trig_free, val, i2, X, o, s);
     }
     // what k_fmm_apply does with the slot: bit 0 store the value and time,
     // bit 1 queue the readers (the change is visible: the value is finite

@@ -77,10 +77,13 @@ def reference_fmm():
     return _distance_fn(_load(FMM_SO).computeDistanceFunction3d, "computeDistanceFunction3d")
 
 
-def oracle_fmm():
-    """The C restatement of the same heap march (fmm_oracle.c), same call."""
-    return _distance_fn(oracle_lib().orc_computeDistanceFunction3d,
-                        "orc_computeDistanceFunction3d")
+def oracle_fmm(ordered=False):
+    """The C restatement of the same heap march (fmm_oracle.c), same call.
+    ``ordered``: the march popping exact key ties by (acceptance time, index),
+    which is what the GPU solver computes; without ties it is the reference's
+    march."""
+    nm = "orc_computeDistanceFunction3d" + ("_ordered" if ordered else "")
+    return _distance_fn(getattr(oracle_lib(), nm), nm)
 
 
 def _extension_fn(fn, name):
@@ -119,10 +122,11 @@ def reference_extension():
     return _extension_fn(_load(FMM_SO).computeExtensionFields3d, "computeExtensionFields3d")
 
 
-def oracle_extension():
-    """The C restatement of the same march with extension fields, same call."""
-    return _extension_fn(oracle_lib().orc_computeExtensionFields3d,
-                         "orc_computeExtensionFields3d")
+def oracle_extension(ordered=False):
+    """The C restatement of the same march with extension fields, same call
+    (``ordered`` as for oracle_fmm)."""
+    nm = "orc_computeExtensionFields3d" + ("_ordered" if ordered else "")
+    return _extension_fn(getattr(oracle_lib(), nm), nm)
 
 
 def _eikonal_fn(fn, name):
@@ -153,9 +157,11 @@ def reference_eikonal():
     return _eikonal_fn(_load(FMM_SO).solveEikonalEquation3d, "solveEikonalEquation3d")
 
 
-def oracle_eikonal():
-    """The C restatement of the same march (fmm_oracle.c), same call."""
-    return _eikonal_fn(oracle_lib().orc_solveEikonalEquation3d, "orc_solveEikonalEquation3d")
+def oracle_eikonal(ordered=False):
+    """The C restatement of the same march (fmm_oracle.c), same call
+    (``ordered`` as for oracle_fmm)."""
+    nm = "orc_solveEikonalEquation3d" + ("_ordered" if ordered else "")
+    return _eikonal_fn(getattr(oracle_lib(), nm), nm)
 
 
 def heaviside(x, eps):

@@ -60,17 +60,40 @@ typedef struct {
   int pos;    /* position in the heap order */
 } hnode;
 
+/* Acceptance time of a point in the ordered march (below): lexicographic
+ * (a, b, c). */
+typedef struct {
+  real a, b, c;
+} time3;
+
 typedef struct {
   hnode *nodes; /* by handle */
   int *heap;    /* position -> handle */
   int size, cap;
+  const time3 *tm; /* NULL: keyed on the value, as the reference's heap;
+                      else keyed on (tm[idx], idx), a total order */
 } fheap;
+
+static int t3_less(const time3 *x, const time3 *y) {
+  return x->a < y->a || (x->a == y->a && (x->b < y->b || (x->b == y->b && x->c < y->c)));
+}
+
+/* node of handle ha before node of handle hb */
+static int h_less(const fheap *h, int ha, int hb) {
+  const hnode *x = &h->nodes[ha], *y = &h->nodes[hb];
+  if (!h->tm) return x->value < y->value;
+  const time3 *tx = &h->tm[x->idx], *ty = &h->tm[y->idx];
+  if (t3_less(tx, ty)) return 1;
+  if (t3_less(ty, tx)) return 0;
+  return x->idx < y->idx;
+}
 
 static void h_init(fheap *h, int cap) {
   h->cap = cap > 16 ? cap : 16;
   h->size = 0;
   h->nodes = (hnode *)malloc(sizeof(hnode) * h->cap);
   h->heap = (int *)malloc(sizeof(int) * h->cap);
+  h->tm = NULL;
 }
 
 static void h_free(fheap *h) {
@@ -97,8 +120,7 @@ static void h_swap(fheap *h, int a, int b) {
 }
 
 static void h_up(fheap *h, int p) {
-  while (p > 0 &&
-         h->nodes[h->heap[p]].value < h->nodes[h->heap[parent_pos(p)]].value) {
+  while (p > 0 && h_less(h, h->heap[p], h->heap[parent_pos(p)])) {
     h_swap(h, p, parent_pos(p));
     p = parent_pos(p);
   }
@@ -108,6 +130,14 @@ static void h_down(fheap *h, int p) {
   for (;;) {
     int l = left_pos(p), r = right_pos(p);
     if (l >= h->size) return;
+    if (h->tm) {
+      /* total order: the smaller child moves up while it is before p */
+      int c = (r < h->size && h_less(h, h->heap[r], h->heap[l])) ? r : l;
+      if (!h_less(h, h->heap[c], h->heap[p])) return;
+      h_swap(h, p, c);
+      p = c;
+      continue;
+    }
     real cur = h->nodes[h->heap[p]].value;
     real lv = h->nodes[h->heap[l]].value;
     real rv = r < h->size ? h->nodes[h->heap[r]].value : REAL_MAX;
@@ -167,7 +197,7 @@ static hnode h_extract(fheap *h, long *moved_idx, int *moved_handle) {
 static void h_update(fheap *h, int handle, real value) {
   h->nodes[handle].value = value;
   int p = h->nodes[handle].pos;
-  if (p > 0 && value < h->nodes[h->heap[parent_pos(p)]].value)
+  if (p > 0 && h_less(h, handle, h->heap[parent_pos(p)]))
     h_up(h, p);
   else
     h_down(h, p);
@@ -188,8 +218,31 @@ typedef struct {
   real **src;
   const real *emask;
   const real *speed; /* the Eikonal solver's speed (NULL: distance function) */
+  time3 *tm;         /* the ordered march only: acceptance times */
   fheap trial;
 } march_t;
+
+/* The acceptance time of a point whose last update came from the acceptance
+ * of a point of time x (has_trigger: a free point; else the front), for a
+ * value of magnitude a: a new first level when a is above x's first level;
+ * otherwise one level under x's, right after x (the heap pops a point an
+ * update has lowered below the key just popped next).  Past the third level
+ * the point keeps x's time. */
+static time3 t3_after(const time3 *x, real a, int has_trigger) {
+  time3 t = {a, -1.0, -1.0};
+  if (!has_trigger || a > x->a) return t;
+  t.a = x->a;
+  if (x->b < 0 || a > x->b) {
+    t.b = a;
+    return t;
+  }
+  t.b = x->b;
+  if (x->c < 0 || a > x->c) {
+    t.c = a;
+    return t;
+  }
+  return *x;
+}
 
 static real trial_update(march_t *m, long o, const int c[3]) {
   real A = 0, B = 0, C = 0;
@@ -281,7 +334,7 @@ static real trial_update(march_t *m, long o, const int c[3]) {
   return out;
 }
 
-static void update_neighbors(march_t *m, long o) {
+static void update_neighbors(march_t *m, long o, int from_free) {
   int c[3];
   c[0] = (int)(o % m->n[0]);
   c[1] = (int)((o / m->n[0]) % m->n[1]);
@@ -295,6 +348,7 @@ static void update_neighbors(march_t *m, long o) {
       if (m->st[oq] == KNOWN || m->st[oq] == OUTSIDE) continue;
       real v = trial_update(m, oq, q);
       if (v < 0) v = -v;
+      if (m->tm) m->tm[oq] = t3_after(&m->tm[o], v, from_free);
       if (m->st[oq] == FAR) {
         m->st[oq] = TRIAL;
         m->handle[oq] = h_insert(&m->trial, oq, v);
@@ -309,9 +363,9 @@ static void update_neighbors(march_t *m, long o) {
  * (distance function and extension fields together); arrays x fastest,
  * grid_dims and dx in x, y, z order.  Returns 0, or 2 for an order other
  * than 1 and 2. */
-int orc_computeExtensionFields3d(real *distance, real **ext, const real *phi, const real *mask,
-                                 real **src, const real *emask, int nf, int order,
-                                 const int *grid_dims, const real *dx) {
+static int extension_march(real *distance, real **ext, const real *phi, const real *mask,
+                           real **src, const real *emask, int nf, int order,
+                           const int *grid_dims, const real *dx, int ordered) {
   if (order != 1 && order != 2) return 2;
   march_t m;
   m.d = distance;
@@ -322,6 +376,7 @@ int orc_computeExtensionFields3d(real *distance, real **ext, const real *phi, co
   m.src = src;
   m.emask = emask;
   m.speed = NULL;
+  m.tm = NULL;
   for (int q = 0; q < 3; q++) {
     m.n[q] = grid_dims[q];
     m.dx[q] = dx[q];
@@ -332,6 +387,7 @@ int orc_computeExtensionFields3d(real *distance, real **ext, const real *phi, co
   long np = m.s[2] * m.n[2];
   m.st = (unsigned char *)calloc((size_t)np, 1);
   m.handle = (int *)malloc(sizeof(int) * (size_t)np);
+  if (ordered) m.tm = (time3 *)calloc((size_t)np, sizeof(time3));
   for (long o = 0; o < np; o++) {
     distance[o] = -1;
     for (int k = 0; k < nf; k++) ext[k][o] = -1;
@@ -345,6 +401,7 @@ int orc_computeExtensionFields3d(real *distance, real **ext, const real *phi, co
   fheap known;
   h_init(&known, m.n[0] + m.n[1] + m.n[2]);
   h_init(&m.trial, m.n[0] + m.n[1] + m.n[2]);
+  m.trial.tm = m.tm;
 
   /* the front (first-order initialisation at both orders) */
   real *fsum = nf ? (real *)malloc(sizeof(real) * nf) : NULL;
@@ -409,7 +466,7 @@ int orc_computeExtensionFields3d(real *distance, real **ext, const real *phi, co
     long mi;
     int mh;
     hnode nd = h_extract(&known, &mi, &mh);
-    if (nd.value < REAL_MAX) update_neighbors(&m, nd.idx);
+    if (nd.value < REAL_MAX) update_neighbors(&m, nd.idx, 0);
   }
   /* the march */
   while (m.trial.size > 0) {
@@ -418,13 +475,20 @@ int orc_computeExtensionFields3d(real *distance, real **ext, const real *phi, co
     hnode nd = h_extract(&m.trial, &mi, &mh);
     if (mh != -1) m.handle[mi] = mh;
     m.st[nd.idx] = KNOWN;
-    update_neighbors(&m, nd.idx);
+    update_neighbors(&m, nd.idx, 1);
   }
   h_free(&known);
   h_free(&m.trial);
   free(m.st);
   free(m.handle);
+  free(m.tm);
   return 0;
+}
+
+int orc_computeExtensionFields3d(real *distance, real **ext, const real *phi, const real *mask,
+                                 real **src, const real *emask, int nf, int order,
+                                 const int *grid_dims, const real *dx) {
+  return extension_march(distance, ext, phi, mask, src, emask, nf, order, grid_dims, dx, 0);
 }
 
 /* orc_computeDistanceFunction3d: the distance function alone. */
@@ -437,8 +501,8 @@ int orc_computeDistanceFunction3d(real *distance, const real *phi, const real *m
 /* orc_solveEikonalEquation3d: the reference's solveEikonalEquation3d; phi is
  * the boundary data on input (the front: phi > -1e-11) and the solution on
  * output.  Returns 0, or 2 for an order other than 1 and 2. */
-int orc_solveEikonalEquation3d(real *phi, const real *speed, const real *mask, int order,
-                               const int *grid_dims, const real *dx) {
+static int eikonal_march(real *phi, const real *speed, const real *mask, int order,
+                         const int *grid_dims, const real *dx, int ordered) {
   if (order != 1 && order != 2) return 2;
   march_t m;
   m.d = phi;
@@ -449,6 +513,7 @@ int orc_solveEikonalEquation3d(real *phi, const real *speed, const real *mask, i
   m.src = NULL;
   m.emask = NULL;
   m.speed = speed;
+  m.tm = NULL;
   for (int q = 0; q < 3; q++) {
     m.n[q] = grid_dims[q];
     m.dx[q] = dx[q];
@@ -459,6 +524,7 @@ int orc_solveEikonalEquation3d(real *phi, const real *speed, const real *mask, i
   long np = m.s[2] * m.n[2];
   m.st = (unsigned char *)calloc((size_t)np, 1);
   m.handle = (int *)malloc(sizeof(int) * (size_t)np);
+  if (ordered) m.tm = (time3 *)calloc((size_t)np, sizeof(time3));
   for (long o = 0; o < np; o++) {
     m.handle[o] = -1;
     if ((mask && mask[o] < 0) || speed[o] < ZERO_TOL) {
@@ -469,6 +535,7 @@ int orc_solveEikonalEquation3d(real *phi, const real *speed, const real *mask, i
   fheap known;
   h_init(&known, m.n[0] + m.n[1] + m.n[2]);
   h_init(&m.trial, m.n[0] + m.n[1] + m.n[2]);
+  m.trial.tm = m.tm;
   for (long o = 0; o < np; o++)
     if (phi[o] > -ZERO_TOL && m.st[o] != OUTSIDE) {
       m.st[o] = KNOWN;
@@ -478,7 +545,7 @@ int orc_solveEikonalEquation3d(real *phi, const real *speed, const real *mask, i
     long mi;
     int mh;
     hnode nd = h_extract(&known, &mi, &mh);
-    if (nd.value < REAL_MAX) update_neighbors(&m, nd.idx);
+    if (nd.value < REAL_MAX) update_neighbors(&m, nd.idx, 0);
   }
   while (m.trial.size > 0) {
     long mi;
@@ -486,11 +553,47 @@ int orc_solveEikonalEquation3d(real *phi, const real *speed, const real *mask, i
     hnode nd = h_extract(&m.trial, &mi, &mh);
     if (mh != -1) m.handle[mi] = mh;
     m.st[nd.idx] = KNOWN;
-    update_neighbors(&m, nd.idx);
+    update_neighbors(&m, nd.idx, 1);
   }
   h_free(&known);
   h_free(&m.trial);
   free(m.st);
   free(m.handle);
+  free(m.tm);
   return 0;
+}
+
+int orc_solveEikonalEquation3d(real *phi, const real *speed, const real *mask, int order,
+                               const int *grid_dims, const real *dx) {
+  return eikonal_march(phi, speed, mask, order, grid_dims, dx, 0);
+}
+
+/* ---- the ordered march ----------------------------------------------------
+ * The same march with the trial heap keyed on a total order instead of the
+ * value: (acceptance time, linear index), the time set at every update by
+ * t3_after from the time of the point whose acceptance made the update.
+ * Where no two keys tie, this pops in the reference's order and the results
+ * are the reference's bit for bit.  Where keys tie exactly (symmetric
+ * inputs, flat fronts, quantised data), the reference's binary heap pops the
+ * tied points in an order set by its whole history of insertions and
+ * removals; this march pops them by time and then by index.  The GPU solver
+ * computes this march's result, except where updates among exactly equal
+ * values lower points more than three levels deep (t3_after keeps the
+ * trigger's time there); that has been seen at first order only, with
+ * differences of a few ulps. */
+int orc_computeExtensionFields3d_ordered(real *distance, real **ext, const real *phi,
+                                         const real *mask, real **src, const real *emask,
+                                         int nf, int order, const int *grid_dims,
+                                         const real *dx) {
+  return extension_march(distance, ext, phi, mask, src, emask, nf, order, grid_dims, dx, 1);
+}
+
+int orc_computeDistanceFunction3d_ordered(real *distance, const real *phi, const real *mask,
+                                          int order, const int *grid_dims, const real *dx) {
+  return extension_march(distance, NULL, phi, mask, NULL, NULL, 0, order, grid_dims, dx, 1);
+}
+
+int orc_solveEikonalEquation3d_ordered(real *phi, const real *speed, const real *mask, int order,
+                                       const int *grid_dims, const real *dx) {
+  return eikonal_march(phi, speed, mask, order, grid_dims, dx, 1);
 }

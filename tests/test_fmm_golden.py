@@ -8,6 +8,12 @@
   spheres, bit for bit (these pin the restatement).
 * The same for the extension fields (computeExtensionFields3d) and the
   Eikonal solver (solveEikonalEquation3d).
+* The ordered march (the same march popping exact key ties by acceptance
+  time and then point index, which the GPU solver computes) equals the
+  reference on every case without exact ties: the golden and seeded cases
+  above are run through it too.  Where keys tie (the reference's own
+  symmetric examples), the two differ only by the order in which tied
+  points are accepted (test_tied_keys_*).
 """
 import ctypes
 import os
@@ -64,20 +70,22 @@ def test_reference_fmm_reproduces_golden(name, order):
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("order", [1, 2])
-def test_oracle_fmm_reproduces_golden(name, order):
+@pytest.mark.parametrize("ordered", [False, True], ids=["heap", "ordered"])
+def test_oracle_fmm_reproduces_golden(name, order, ordered):
     z = np.load(GOLDEN)
     phi, dx, mask = _case(z, name)
-    got = oracle.oracle_fmm()(phi, order, dx, mask)
+    got = oracle.oracle_fmm(ordered)(phi, order, dx, mask)
     assert np.array_equal(got.view(np.uint64), z["%s|out%d" % (name, order)].view(np.uint64))
 
 
 @pytest.mark.skipif(not oracle.fmm_available(), reason="oracle/_ref/libfmm.so not built")
 @pytest.mark.parametrize("shape,seed", [((33, 41, 29), 1), ((20, 64, 48), 2), ((1, 80, 90), 3)])
 @pytest.mark.parametrize("order", [1, 2])
-def test_oracle_fmm_matches_reference(shape, seed, order):
+@pytest.mark.parametrize("ordered", [False, True], ids=["heap", "ordered"])
+def test_oracle_fmm_matches_reference(shape, seed, order, ordered):
     phi, dx = seeded_spheres(shape, seed)
     mask = seeded_mask(shape, seed)
-    a = oracle.oracle_fmm()(phi, order, dx, mask)
+    a = oracle.oracle_fmm(ordered)(phi, order, dx, mask)
     b = oracle.reference_fmm()(phi, order, dx, mask)
     assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
 
@@ -132,11 +140,12 @@ def test_reference_extension_reproduces_golden(name, order):
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("order", [1, 2])
-def test_oracle_extension_reproduces_golden(name, order):
+@pytest.mark.parametrize("ordered", [False, True], ids=["heap", "ordered"])
+def test_oracle_extension_reproduces_golden(name, order, ordered):
     z = np.load(GOLDEN)
     phi, dx, mask = _case(z, name)
     src, emask = ext_case(z, name)
-    dist, fields = oracle.oracle_extension()(phi, src, order, dx, mask, emask)
+    dist, fields = oracle.oracle_extension(ordered)(phi, src, order, dx, mask, emask)
     assert np.array_equal(dist.view(np.uint64), z["%s|out%d" % (name, order)].view(np.uint64))
     for k, f in enumerate(fields):
         assert np.array_equal(f.view(np.uint64), z["%s|ext%d_%d" % (name, order, k)].view(np.uint64))
@@ -145,7 +154,8 @@ def test_oracle_extension_reproduces_golden(name, order):
 @pytest.mark.skipif(not oracle.fmm_available(), reason="oracle/_ref/libfmm.so not built")
 @pytest.mark.parametrize("shape,seed", [((33, 41, 29), 1), ((20, 64, 48), 2), ((1, 50, 60), 3)])
 @pytest.mark.parametrize("order", [1, 2])
-def test_oracle_extension_matches_reference(shape, seed, order):
+@pytest.mark.parametrize("ordered", [False, True], ids=["heap", "ordered"])
+def test_oracle_extension_matches_reference(shape, seed, order, ordered):
     phi, dx = seeded_spheres(shape, seed)
     mask = seeded_mask(shape, seed)
     emask = None
@@ -153,7 +163,7 @@ def test_oracle_extension_matches_reference(shape, seed, order):
         emask = np.where(np.random.default_rng(seed).random(shape) < 0.3, -1.0, 1.0)
     src = seeded_sources(shape, seed)
     a = oracle.reference_extension()(phi, src, order, dx, mask, emask)
-    b = oracle.oracle_extension()(phi, src, order, dx, mask, emask)
+    b = oracle.oracle_extension(ordered)(phi, src, order, dx, mask, emask)
     for x, y in zip([a[0]] + a[1], [b[0]] + b[1]):
         assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
 
@@ -191,21 +201,23 @@ def test_reference_eikonal_reproduces_golden(name, order):
 
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("order", [1, 2])
-def test_oracle_eikonal_reproduces_golden(name, order):
+@pytest.mark.parametrize("ordered", [False, True], ids=["heap", "ordered"])
+def test_oracle_eikonal_reproduces_golden(name, order, ordered):
     z = np.load(GOLDEN)
     data, speed, mask = eik_case(z, name)
-    got = oracle.oracle_eikonal()(data, speed, order, z[name + "|dx"][::-1], mask)
+    got = oracle.oracle_eikonal(ordered)(data, speed, order, z[name + "|dx"][::-1], mask)
     assert np.array_equal(got.view(np.uint64), z["%s|eik%d" % (name, order)].view(np.uint64))
 
 
 @pytest.mark.skipif(not oracle.fmm_available(), reason="oracle/_ref/libfmm.so not built")
 @pytest.mark.parametrize("shape,seed", [((33, 41, 29), 1), ((20, 64, 48), 2), ((1, 50, 60), 3)])
 @pytest.mark.parametrize("order", [1, 2])
-def test_oracle_eikonal_matches_reference(shape, seed, order):
+@pytest.mark.parametrize("ordered", [False, True], ids=["heap", "ordered"])
+def test_oracle_eikonal_matches_reference(shape, seed, order, ordered):
     data, speed, dx = seeded_eikonal(shape, seed)
     mask = seeded_mask(shape, seed)
     a = oracle.reference_eikonal()(data, speed, order, dx, mask)
-    b = oracle.oracle_eikonal()(data, speed, order, dx, mask)
+    b = oracle.oracle_eikonal(ordered)(data, speed, order, dx, mask)
     assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
 
 
@@ -364,3 +376,63 @@ def test_reference_examples_oracle_matches_reference():
                                       d.ctypes.data_as(P), h.ctypes.data_as(P)) == 0
     want = oracle.oracle_eikonal()(_plane(phi), _plane(speed), 2, dx + [1.0])[0]
     assert np.array_equal(sol.view(np.uint64), want.view(np.uint64))
+
+
+# ---- exact key ties: the reference's heap order against the ordered march ------
+
+def _quantised(shape, seed):
+    phi, dx = seeded_spheres(shape, seed)
+    return np.round(phi * 8) / 8, dx
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_tied_keys_distance_examples_unaffected(order):
+    """The reference's distance and extension examples hold ties that do not
+    change any value: the ordered march gives the heap march's result bit for
+    bit on them."""
+    for phi, dx in (examples.distance_3d(), examples.distance_2d()):
+        phi = phi if phi.ndim == 3 else _plane(phi)
+        dx = list(dx) + [1.0] * (3 - len(dx))
+        a = oracle.oracle_fmm()(phi, order, dx)
+        b = oracle.oracle_fmm(True)(phi, order, dx)
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    phi, src, dx = examples.extension_2d()
+    a = oracle.oracle_extension()(_plane(phi), [_plane(s_) for s_ in src], order, dx + [1.0])
+    b = oracle.oracle_extension(True)(_plane(phi), [_plane(s_) for s_ in src], order, dx + [1.0])
+    for x, y in zip([a[0]] + a[1], [b[0]] + b[1]):
+        assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
+
+
+def test_tied_keys_first_order_differ_by_rounding_only():
+    """At first order a tie only decides whether a neighbour of equal value
+    joins an update, which leaves the root unchanged up to rounding: the
+    heap's order and the ordered march agree to 1e-13 relative (the
+    reference's 2D Eikonal example, quantised distance data)."""
+    phi, speed, dx = examples.eikonal_2d()
+    a = oracle.oracle_eikonal()(_plane(phi), _plane(speed), 1, dx + [1.0])
+    b = oracle.oracle_eikonal(True)(_plane(phi), _plane(speed), 1, dx + [1.0])
+    assert not np.array_equal(a, b)
+    assert np.max(np.abs(a - b) / np.maximum(np.abs(a), 1e-300)) < 1e-13
+    for seed in (1, 3):
+        phi, dx = _quantised((17, 23, 19), seed)
+        a = oracle.oracle_fmm()(phi, 1, dx)
+        b = oracle.oracle_fmm(True)(phi, 1, dx)
+        assert np.max(np.abs(a - b) / np.maximum(np.abs(a), 1e-300)) < 1e-13
+
+
+def test_tied_keys_second_order_stencil_choice():
+    """At second order a tie can decide whether the next point along an axis
+    was KNOWN at an update, i.e. whether that axis takes the second-order
+    stencil, so the two orders of acceptance give two different valid
+    solutions.  On the reference's 2D Eikonal example (solveEikonalEquation2d.c:
+    a disk of zeros, speed 1 / 2 split at x = 0, mirror-symmetric in y) the
+    first difference is at a point whose +y neighbours at distance 1 and 2
+    carry the same key; both results stay within 1e-2 of each other."""
+    phi, speed, dx = examples.eikonal_2d()
+    a = oracle.oracle_eikonal()(_plane(phi), _plane(speed), 2, dx + [1.0])[0]
+    b = oracle.oracle_eikonal(True)(_plane(phi), _plane(speed), 2, dx + [1.0])[0]
+    assert not np.array_equal(a, b)
+    assert np.max(np.abs(a - b)) < 1e-2
+    # (x, y) = (75, 43): keys of (75, 44) and (75, 45) are both 1/150
+    assert a[44, 75] == b[44, 75] == a[45, 75] == b[45, 75]
+    assert a[43, 75] != b[43, 75]

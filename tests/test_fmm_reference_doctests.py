@@ -58,7 +58,7 @@ class WrapperMirror:
 
 
 def backends():
-    out = [pytest.param("oracle", id="oracle")]
+    out = [pytest.param("oracle", id="oracle"), pytest.param("ordered", id="ordered")]
     if oracle.fmm_available():
         out.insert(0, pytest.param("reference", id="reference"))
     return out
@@ -69,8 +69,9 @@ def backend(request):
     if request.param == "reference":
         return WrapperMirror(oracle.reference_fmm(), oracle.reference_extension(),
                              oracle.reference_eikonal())
-    return WrapperMirror(oracle.oracle_fmm(), oracle.oracle_extension(),
-                         oracle.oracle_eikonal())
+    ordered = request.param == "ordered"   # the march the GPU solver computes
+    return WrapperMirror(oracle.oracle_fmm(ordered), oracle.oracle_extension(ordered),
+                         oracle.oracle_eikonal(ordered))
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c.__name__ for c in CASES])

@@ -53,7 +53,7 @@ def test_distance_reproduces_reference_golden(lib, name, order):
 def test_distance_matches_oracle(lib, shape, seed, order):
     phi, dx = seeded_spheres(shape, seed)
     mask = seeded_mask(shape, seed)
-    want = oracle.oracle_fmm()(phi, order, dx, mask)
+    want = oracle.oracle_fmm(ordered=True)(phi, order, dx, mask)
     got, passes = gpu_distance(lib, phi, order, dx, mask)
     assert same_bits(got, want), (np.mean(got == want), np.abs(got - want).max())
     assert passes > 0
@@ -80,7 +80,7 @@ def test_distance_device_arrays(lib):
     """Device pointers are used in place (torch tensors on cuda:0)."""
     import torch
     phi, dx = seeded_spheres((24, 30, 36), 9)
-    want = oracle.oracle_fmm()(phi, 2, dx)
+    want = oracle.oracle_fmm(ordered=True)(phi, 2, dx)
     tp = torch.from_numpy(phi).cuda()
     out = torch.empty_like(tp)
     dims = (ctypes.c_int * 3)(*phi.shape[::-1])
@@ -99,7 +99,7 @@ def test_distance_after_scratch_release(lib):
     assert lib.lsmgpu_release_scratch() == 0
     again, _ = gpu_distance(lib, phi, 2, dx)
     assert same_bits(first, again)
-    assert same_bits(again, oracle.oracle_fmm()(phi, 2, dx))
+    assert same_bits(again, oracle.oracle_fmm(ordered=True)(phi, 2, dx))
 
 
 def test_distance_edge_cases(lib):
@@ -111,7 +111,7 @@ def test_distance_edge_cases(lib):
     assert np.all(got == np.finfo(np.float64).max)   # all outside the domain
     phi = np.linspace(-1, 1, 9)[None, None, :] * np.ones((3, 4, 9))
     got, _ = gpu_distance(lib, phi, 1, [0.25, 1.0, 1.0])
-    assert same_bits(got, oracle.oracle_fmm()(phi, 1, [0.25, 1.0, 1.0]))
+    assert same_bits(got, oracle.oracle_fmm(ordered=True)(phi, 1, [0.25, 1.0, 1.0]))
     assert np.all(got[..., 4] == -1e-11)             # on the interface
     one = np.array([[[0.3]]])                        # a single point
     got, _ = gpu_distance(lib, one, 2, [1.0, 1.0, 1.0])
@@ -127,7 +127,7 @@ def test_pylsmlib_compute_distance_function():
     got = computeDistanceFunction(phi, dx, order=2)
     assert same_bits(got, z["spheres2d|out2"][0])
     got1 = computeDistanceFunction(phi[5], dx[1], order=1)      # 1D
-    assert same_bits(got1, oracle.oracle_fmm()(phi[5][None, None, :], 1, [dx[1], 1.0, 1.0])[0, 0])
+    assert same_bits(got1, oracle.oracle_fmm(ordered=True)(phi[5][None, None, :], 1, [dx[1], 1.0, 1.0])[0, 0])
 
 
 # ---- extension fields -------------------------------------------------------
@@ -178,7 +178,7 @@ def test_extension_matches_oracle(lib, shape, seed, order):
     if mask is not None:
         emask = np.where(np.random.default_rng(seed).random(shape) < 0.3, -1.0, 1.0)
     src = seeded_sources(shape, seed, n=3)
-    want = oracle.oracle_extension()(phi, src, order, dx, mask, emask)
+    want = oracle.oracle_extension(ordered=True)(phi, src, order, dx, mask, emask)
     got = gpu_extension(lib, phi, src, order, dx, mask, emask)
     assert same_bits(got[0], want[0])
     for a, b in zip(got[1], want[1]):
@@ -189,7 +189,7 @@ def test_extension_more_fields_than_one_solve(lib):
     """Nine fields: two groups of solves, each field as the oracle has it."""
     phi, dx = seeded_spheres((24, 28, 20), 6)
     src = seeded_sources((24, 28, 20), 6, n=9)
-    want = oracle.oracle_extension()(phi, src, 2, dx)
+    want = oracle.oracle_extension(ordered=True)(phi, src, 2, dx)
     got = gpu_extension(lib, phi, src, 2, dx)
     assert same_bits(got[0], want[0])
     for a, b in zip(got[1], want[1]):
@@ -232,7 +232,7 @@ def test_pylsmlib_compute_extension_fields():
     speed = np.stack([a[0] for a in src])
     em = np.random.default_rng(3).random(phi2.shape) < 0.2
     dist, ext = computeExtensionFields(phi2, speed, dx=[dx[1], dx[0]], order=1, ext_mask=em)
-    want = oracle.oracle_extension()(phi, src, 1, dx, None,
+    want = oracle.oracle_extension(ordered=True)(phi, src, 1, dx, None,
                                      (-em.astype(float) * 2.0 + 1.0)[None])
     assert same_bits(dist, want[0][0])
     assert ext.shape == speed.shape
@@ -272,7 +272,7 @@ def test_eikonal_reproduces_reference_golden(lib, name, order):
 def test_eikonal_matches_oracle(lib, shape, seed, order):
     data, speed, dx = seeded_eikonal(shape, seed)
     mask = seeded_mask(shape, seed)
-    want = oracle.oracle_eikonal()(data, speed, order, dx, mask)
+    want = oracle.oracle_eikonal(ordered=True)(data, speed, order, dx, mask)
     got = gpu_eikonal(lib, data, speed, order, dx, mask)
     assert same_bits(got, want), (np.mean(got == want), np.abs(got - want).max())
 
@@ -282,7 +282,7 @@ def test_eikonal_c_abi_entry_point(lib):
     the device, 2 for a bad order."""
     import torch
     data, speed, dx = seeded_eikonal((24, 30, 36), 9)
-    want = oracle.oracle_eikonal()(data, speed, 2, dx)
+    want = oracle.oracle_eikonal(ordered=True)(data, speed, 2, dx)
     fn = lib.solveEikonalEquation3d
     P = ctypes.c_void_p
     fn.restype = ctypes.c_int
@@ -303,7 +303,7 @@ def test_pylsmlib_solve_eikonal_equation():
     speed = 1.0 + 0.25 * np.cos(np.linspace(0, 7, sdf.size)).reshape(sdf.shape)
     minphi = sdf.min()
     data = np.where(sdf > 0, minphi - 1.0, sdf) - minphi
-    want = oracle.oracle_eikonal()(data, speed, 2, dx) + minphi
+    want = oracle.oracle_eikonal(ordered=True)(data, speed, 2, dx) + minphi
     got = solveEikonalEquation(sdf[0], speed[0], dx=[dx[1], dx[0]], order=2)
     assert same_bits(got, want[0])
     assert same_bits(travel_time(sdf[0], speed[0], dx=[dx[1], dx[0]]), np.abs(want[0]))

@@ -126,12 +126,12 @@ def test_reference_examples_match_oracle(lib):
     out = np.full_like(phi, np.nan)
     d, h = grid(phi, dx)
     assert f3(out.ctypes.data, phi.ctypes.data, None, 2, d.ctypes.data, h.ctypes.data) == 0
-    assert same_bits(out, oracle.oracle_fmm()(phi, 2, dx))
+    assert same_bits(out, oracle.oracle_fmm(ordered=True)(phi, 2, dx))
     phi, dx = examples.distance_2d()
     out = np.full_like(phi, np.nan)
     d, h = grid(phi, dx)
     assert f2(out.ctypes.data, phi.ctypes.data, None, 2, d.ctypes.data, h.ctypes.data) == 0
-    assert same_bits(out, oracle.oracle_fmm()(phi[None], 2, dx + [1.0])[0])
+    assert same_bits(out, oracle.oracle_fmm(ordered=True)(phi[None], 2, dx + [1.0])[0])
     phi, src, dx = examples.extension_2d()
     dist = np.full_like(phi, np.nan)
     ext = [np.full_like(phi, np.nan) for _ in src]
@@ -140,7 +140,7 @@ def test_reference_examples_match_oracle(lib):
     d, h = grid(phi, dx)
     assert e2(dist.ctypes.data, ctypes.cast(ext_p, P), phi.ctypes.data, None,
               ctypes.cast(src_p, P), None, 2, 2, d.ctypes.data, h.ctypes.data) == 0
-    wd, wf = oracle.oracle_extension()(phi[None], [s[None] for s in src], 2, dx + [1.0])
+    wd, wf = oracle.oracle_extension(ordered=True)(phi[None], [s[None] for s in src], 2, dx + [1.0])
     assert same_bits(dist, wd[0])
     for got, want in zip(ext, wf):
         assert same_bits(got, want[0])
@@ -148,4 +148,4 @@ def test_reference_examples_match_oracle(lib):
     sol = phi.copy()
     d, h = grid(phi, dx)
     assert k2(sol.ctypes.data, speed.ctypes.data, None, 2, d.ctypes.data, h.ctypes.data) == 0
-    assert same_bits(sol, oracle.oracle_eikonal()(phi[None], speed[None], 2, dx + [1.0])[0])
+    assert same_bits(sol, oracle.oracle_eikonal(ordered=True)(phi[None], speed[None], 2, dx + [1.0])[0])
