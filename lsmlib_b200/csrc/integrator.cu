@@ -249,6 +249,10 @@ StageArgs base_args(lsmgpu_workspace* ws, const FillBox& fb, const double dx[3])
   a.dx_sq = m * m;
   a.dt_dev = ws->scal + kDt;
   a.fp64_policy = ws->prec == 4 ? ws->fp64_policy : 0;
+  // the drivers' stage inputs are phi and the workspace arrays: their ghost
+  // cells take the boundary values before each stage, as the reference's
+  // boundary module fills them (edge and corner ghosts are not written)
+  a.ghosts_writable = 1;
   return a;
 }
 

@@ -100,15 +100,20 @@ extern "C" int lsmgpu_normal_rhs_dt_noalloc(double* rhs, double* dt,
   }
   if (!box_valid(g, "phi", R) || !covers(g, f, 3, "phi", R))
     return LSMGPU_ERR_INVALID_BOX;
-  const int tiles = stage_blocks(f);
-  if (tiles > kNoAllocMaxTiles) {
+  // the tile count in 64 bits: a box of more than 2^31 tiles must not wrap
+  // around to a count that passes the check below
+  const long tiles_l = (long)((f.n(0) + kStageTX - 1) / kStageTX) *
+                       (long)((f.n(1) + kStageTY - 1) / kStageTY) *
+                       (long)((f.n(2) + kStageTZ - 1) / kStageTZ);
+  if (tiles_l > kNoAllocMaxTiles) {
     set_error(LSMGPU_ERR_INVALID_BOX,
-              std::string(R) + ": fill box needs " + std::to_string(tiles) +
+              std::string(R) + ": fill box needs " + std::to_string(tiles_l) +
                   " tiles of " + std::to_string(kStageTX) + "x" + std::to_string(kStageTY) +
                   "x" + std::to_string(kStageTZ) + " cells; the static scratch holds " +
                   std::to_string(kNoAllocMaxTiles));
     return LSMGPU_ERR_INVALID_BOX;
   }
+  const int tiles = (int)tiles_l;
   // host arrays would need staging buffers, i.e. an allocation
   if (!is_device_pointer(rhs) || !is_device_pointer(phi) || !is_device_pointer(F)) {
     set_error(LSMGPU_ERR_INVALID_VALUE,

@@ -625,12 +625,253 @@ __device__ __forceinline__ double stage_tile_faces(const StageParams<T>& p, int 
   return hmax;
 }
 
+template <typename T> struct Pair2;
+template <> struct Pair2<double> { using type = double2; };
+template <> struct Pair2<float> { using type = float2; };
+
+// The face-shared two-sided kinds with two cells per thread: thread (t, ty)
+// of a TX/2 x TY block owns the cells x0+2t and x0+2t+1 of row j0+ty and
+// marches them along z.  Against one cell per thread this gives every
+// thread six independent face evaluations per plane (the FP64 dependency
+// chains of one cell no longer wait on each other), and the pair reads its
+// x stencil (7 values for its two faces) and both y columns with 16-byte
+// shared loads: the tile's x column of cell x is x - x0 + 4, so each pair
+// starts on an even column.  The faces in front of each row are evaluated
+// by row 0, those in front of each column by the last two rows (one column
+// each) -- one inlined evaluation for both, from a strided tile read -- and
+// the z face in front of the march before it starts.
+// The kernel reads every ghost cell as stored (k_face_ghosts writes the
+// boundary values first) and instantiates one face routine (K64: the FP32
+// form's FP64 kink recomputation), so that its loop holds seven face
+// evaluations and nothing else of size: its instruction footprint, not the
+// arithmetic, limited a version with boundary loads and both face routines
+// inlined (ncu: no_instruction stalls 4.1 per issue against 0.9).
+// Everything else -- roles of the halo cells in partial tiles, the face
+// owner of phi^- along each axis, the right-hand sides -- is that of
+// stage_tile_faces.
+constexpr int kPairPX = 4;
+
+template <typename T, bool K64>
+__device__ __forceinline__ void face_pm_t(const T* u, T inv, T& vp, T& vm) {
+  weno5_face<T, sizeof(T) == 4 && K64>(u, inv, vp, vm);
+}
+
+template <typename T, int KIND, bool K64, int TX, int TY, int TZ>
+__device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int bx, int by,
+                                                   int bz, T (*tile)[TY + 6][TX + 8],
+                                                   T (*fy)[TX], T* fx) {
+  using T2 = typename Pair2<T>::type;
+  static_assert(TX == 32, "a tile row is one half-warp of pairs");
+  static_assert(TY <= TX / 2, "row-start faces are spread over one row of threads");
+  static_assert(TY >= 3, "row 0 and the last two rows are distinct");
+  constexpr int NP = TX / 2;   // threads per row
+  constexpr int PX = kPairPX;
+  const int t = threadIdx.x, ty = threadIdx.y;
+  const int x0 = p.fb.lo[0] + bx * TX, j0 = p.fb.lo[1] + by * TY;
+  const int c0 = 2 * t;
+  const int i0 = x0 + c0, i1 = i0 + 1;
+  const int j = j0 + ty;
+  const int kb = p.fb.lo[2] + bz * TZ;
+  const int ke = min(kb + TZ - 1, p.fb.hi[2]);
+  const int hi0 = p.fb.hi[0], hi1 = p.fb.hi[1];
+  const bool rowin = j <= hi1;
+  const bool act0 = rowin && i0 <= hi0, act1 = rowin && i1 <= hi0;
+  const bool halo0 = !act0 && i0 <= hi0 + 3 && j <= hi1 + 3 && !(i0 > hi0 && j > hi1);
+  const bool halo1 = !act1 && i1 <= hi0 + 3 && j <= hi1 + 3 && !(i1 > hi0 && j > hi1);
+  const Grid3<const T> phi = make_grid(p.phi_s, p.gb);
+  const long sy = p.gb.sy(), sz = p.gb.sz();
+  const long base0 = -((long)p.gb.lo[0] + sy * p.gb.lo[1] + sz * p.gb.lo[2]);
+  const T dt = p.dt_dev ? (T)(*p.dt_dev) : (T)p.dt;
+  double hmax = -1.0;
+
+  // x strips: cells x0-3, x0-2 (t = 0), x0-1 (t = 1) on the left; on the
+  // right x0+TX, x0+TX+1 (t = NP-1) and x0+TX+2 (t = NP-2) where a cell of
+  // the fill box is within 3 of them
+  int hxa = 0, hxb = 0;
+  bool has_a = false, has_b = false;
+  if (rowin) {
+    if (t == 0) { hxa = x0 - 3; hxb = x0 - 2; has_a = has_b = true; }
+    else if (t == 1) { hxa = x0 - 1; has_a = true; }
+    else if (t == NP - 1) {
+      hxa = x0 + TX; hxb = x0 + TX + 1;
+      has_a = hxa <= hi0 + 3; has_b = hxb <= hi0 + 3;
+    } else if (t == NP - 2) { hxa = x0 + TX + 2; has_a = hxa <= hi0 + 3; }
+  }
+  const int cola = hxa - x0 + PX, colb = hxb - x0 + PX;
+  // y strips: rows j0-3..j0-1 (ty < 3) and j+3 (ty >= TY-3, row in the fill
+  // box), for the pair's cells that are fill-box columns
+  const int hj = ty < 3 ? j0 - 3 + ty : j + 3;
+  const bool has_hy = (ty < 3) || (ty >= TY - 3 && rowin);
+  const bool hy0 = has_hy && i0 <= hi0, hy1 = has_hy && i1 <= hi0;
+  const int trow = ty < 3 ? ty : ty + 6;
+  // faces in front of rows (row 0, thread t < TY serves row t) and columns
+  // (rows TY-2 and TY-1: column 2t and 2t+1 respectively)
+  const bool row_start = ty == 0 && t < TY && j0 + t <= hi1;
+  const int col_c = c0 + (ty == TY - 1 ? 1 : 0);
+  const bool col_start = ty >= TY - 2 && x0 + col_c <= hi0;
+  // the extra face as a strided read of buffer 0 (buffer 1 is one tile on)
+  const bool xtra = row_start || col_start;
+  const int xoff = row_start ? (t + 3) * (TX + 8) + PX - 3 : col_c + PX;
+  const int xstride = row_start ? 1 : TX + 8;
+  T* const xout = row_start ? &fx[t] : &fy[0][col_c];
+  const T xinv = row_start ? p.inv[0] : p.inv[1];
+
+  auto ld = [&](int a, int b, int c) -> T { return __ldg(phi.ptr(a, b, c)); };
+  // next plane's values: the window tops (active cells) or the own cells
+  // (halo cells), and the strip cells
+  T n0 = T(0), n1 = T(0), na = T(0), nb = T(0), ny0 = T(0), ny1 = T(0);
+  auto prefetch = [&](int k) {
+    if (act0) n0 = ld(i0, j, k + 3);
+    else if (halo0) n0 = ld(i0, j, k);
+    if (act1) n1 = ld(i1, j, k + 3);
+    else if (halo1) n1 = ld(i1, j, k);
+    if (has_a) na = ld(hxa, j, k);
+    if (has_b) nb = ld(hxb, j, k);
+    if (hy0) ny0 = ld(i0, hj, k);
+    if (hy1) ny1 = ld(i1, hj, k);
+  };
+
+  T w0[7], w1[7];
+  if (act0) {
+#pragma unroll
+    for (int m = 0; m < 6; m++) w0[m + 1] = ld(i0, j, kb - 3 + m);
+  }
+  if (act1) {
+#pragma unroll
+    for (int m = 0; m < 6; m++) w1[m + 1] = ld(i1, j, kb - 3 + m);
+  }
+  // phi_z^-(k) of each cell, from the face k-1/2 (first: the face in front
+  // of the march, from phi(kb-3 .. kb+2))
+  T zrun0 = T(0), zrun1 = T(0);
+  if (act0) {
+    T unused;
+    face_pm_t<T, K64>(w0 + 1, p.inv[2], unused, zrun0);
+    if (act1) face_pm_t<T, K64>(w1 + 1, p.inv[2], unused, zrun1);
+  }
+  prefetch(kb);
+  for (int k = kb; k <= ke; ++k) {
+    const int buf = (k - kb) & 1;
+    T v0 = n0, v1 = n1;
+    if (act0) {
+#pragma unroll
+      for (int m = 0; m < 6; m++) w0[m] = w0[m + 1];
+      w0[6] = n0;
+      v0 = w0[3];
+    }
+    if (act1) {
+#pragma unroll
+      for (int m = 0; m < 6; m++) w1[m] = w1[m + 1];
+      w1[6] = n1;
+      v1 = w1[3];
+    }
+    // the pair's own cells (a cell that is neither active nor halo is never
+    // read, so it may hold anything)
+    *reinterpret_cast<T2*>(&tile[buf][ty + 3][c0 + PX]) = T2{v0, v1};
+    if (has_a) tile[buf][ty + 3][cola] = na;
+    if (has_b) tile[buf][ty + 3][colb] = nb;
+    if (hy0 || hy1) *reinterpret_cast<T2*>(&tile[buf][trow][c0 + PX]) = T2{ny0, ny1};
+    __syncthreads();
+    if (k < ke) prefetch(k + 1);
+    const long o0 = base0 + (long)i0 + sy * j + sz * k;
+    T a00 = T(0), a01 = T(0), uc0 = T(0), uc1 = T(0);
+    T xp0 = T(0), xp1 = T(0), xm1 = T(0), xnext = T(0);
+    T yp0 = T(0), yp1 = T(0), zp0 = T(0), zp1 = T(0), znx0 = T(0), znx1 = T(0);
+    constexpr bool kAux = KIND == kStageNormal || KIND == kStageNormalRhs;
+    if (act0) {
+      if (kAux || (KIND == kStageReinit && p.use_phi0 == 1)) a00 = __ldg(p.aux0 + o0);
+      if (KIND != kStageNormalRhs && p.rk_kind != 1) uc0 = __ldg(p.phi_n + o0);
+    }
+    if (act1) {
+      if (kAux || (KIND == kStageReinit && p.use_phi0 == 1)) a01 = __ldg(p.aux0 + o0 + 1);
+      if (KIND != kStageNormalRhs && p.rk_kind != 1) uc1 = __ldg(p.phi_n + o0 + 1);
+    }
+    if (act0) {
+      // x: tile columns c0+2 .. c0+8 hold phi(x-2 .. x+4) of cell x = i0
+      T u[7];
+      const T2 q0 = *reinterpret_cast<const T2*>(&tile[buf][ty + 3][c0 + 2]);
+      const T2 q1 = *reinterpret_cast<const T2*>(&tile[buf][ty + 3][c0 + 4]);
+      const T2 q2 = *reinterpret_cast<const T2*>(&tile[buf][ty + 3][c0 + 6]);
+      u[0] = q0.x; u[1] = q0.y; u[2] = q1.x; u[3] = q1.y; u[4] = q2.x; u[5] = q2.y;
+      u[6] = tile[buf][ty + 3][c0 + 8];
+      face_pm_t<T, K64>(u, p.inv[0], xp0, xm1);
+      face_pm_t<T, K64>(u + 1, p.inv[0], xp1, xnext);
+      // y: both cells' columns, rows j-2 .. j+3
+      T ya[6], yb[6];
+#pragma unroll
+      for (int m = 0; m < 6; m++) {
+        const T2 q = *reinterpret_cast<const T2*>(&tile[buf][ty + 1 + m][c0 + PX]);
+        ya[m] = q.x;
+        yb[m] = q.y;
+      }
+      T ym0, ym1;
+      face_pm_t<T, K64>(ya, p.inv[1], yp0, ym0);
+      face_pm_t<T, K64>(yb, p.inv[1], yp1, ym1);
+      if (ty + 1 < TY) *reinterpret_cast<T2*>(&fy[ty + 1][c0]) = T2{ym0, ym1};
+      face_pm_t<T, K64>(w0 + 1, p.inv[2], zp0, znx0);
+      if (act1) face_pm_t<T, K64>(w1 + 1, p.inv[2], zp1, znx1);
+    }
+    const T xm_left = __shfl_up_sync(0xffffffffu, xnext, 1, NP);
+    if (xtra) {
+      const T* xb = &tile[buf][0][0] + xoff;
+      T u[6], unused;
+#pragma unroll
+      for (int m = 0; m < 6; m++) u[m] = xb[m * xstride];
+      face_pm_t<T, K64>(u, xinv, unused, *xout);
+    }
+    __syncthreads();
+    if (act0) {
+      const T2 ym = *reinterpret_cast<const T2*>(&fy[ty][c0]);
+      const T xm0 = t == 0 ? fx[ty] : xm_left;
+      const T L0 = two_sided_rhs<T, KIND>(p, a00, w0[3], xp0, yp0, zp0, xm0, ym.x, zrun0, hmax);
+      zrun0 = znx0;
+      if (KIND == kStageNormalRhs) p.rhs_out[o0] = L0;
+      else p.out[o0] = stage_out(p, o0, uc0, w0[3], L0, dt);
+      if (act1) {
+        const T L1 = two_sided_rhs<T, KIND>(p, a01, w1[3], xp1, yp1, zp1, xm1, ym.y, zrun1,
+                                            hmax);
+        zrun1 = znx1;
+        if (KIND == kStageNormalRhs) p.rhs_out[o0 + 1] = L1;
+        else p.out[o0 + 1] = stage_out(p, o0 + 1, uc1, w1[3], L1, dt);
+      }
+    }
+  }
+  return hmax;
+}
+
 template <typename T, int KIND, bool FAST, int TX>
 struct UseFaces {
   static constexpr bool value =
       (FAST || sizeof(T) == 4) && TX == 32 &&
       (KIND == kStageNormal || KIND == kStageReinit || KIND == kStageNormalRhs);
 };
+
+// kStageNormalRhs: the block's largest CFL speed into its partials slot,
+// compared as the reference does ("if (h > m) m = h"); NT threads per block
+template <int KIND, int NT, typename P>
+__device__ __forceinline__ void block_max_partial(const P& p, double hmax) {
+  if (KIND != kStageNormalRhs) return;
+  __shared__ double red[NT / 32];
+  double m = hmax;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const double o2 = __shfl_xor_sync(0xffffffffu, m, off);
+    m = (o2 > m) ? o2 : m;
+  }
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int lane = tid & 31, wid = tid >> 5;
+  if (lane == 0) red[wid] = m;
+  __syncthreads();
+  if (wid == 0) {
+    m = (lane < NT / 32) ? red[lane] : -1.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o2 = __shfl_xor_sync(0xffffffffu, m, off);
+      m = (o2 > m) ? o2 : m;
+    }
+    if (lane == 0)
+      p.partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = m;
+  }
+}
 
 // blocks per SM the register allocation must allow (default: 24 warps; with
 // the 80 registers this leaves, the config-2 FP64 and FP32 stages run 6-7 %
@@ -653,29 +894,91 @@ k_stage(StageParams<T> p) {
     hmax = stage_tile<T, KIND, FAST, TX, TY, TZ>(p, (int)blockIdx.x, (int)blockIdx.y,
                                                  (int)blockIdx.z, tile);
   }
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  if (KIND == kStageNormalRhs) {
-    // block maximum with the reference's "if (h > m) m = h" comparison
-    __shared__ double red[TX * TY / 32];
-    double m = hmax;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double o2 = __shfl_xor_sync(0xffffffffu, m, off);
-      m = (o2 > m) ? o2 : m;
+  block_max_partial<KIND, TX * TY>(p, hmax);
+}
+
+// blocks per SM the register allocation of the pair kernel must allow
+#ifndef LSMGPU_PAIR_MIN_BLOCKS
+#define LSMGPU_PAIR_MIN_BLOCKS 4
+#endif
+
+// The face-shared two-sided kinds, two cells per thread (stage_tile_pairs):
+// a block of TX/2 x TY threads covers the same TX x TY x TZ tile as k_stage.
+// Every ghost cell the stencils reach is read as stored.
+template <typename T, int KIND, bool K64, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TX / 2 * TY, LSMGPU_PAIR_MIN_BLOCKS)
+k_stage_pairs(StageParams<T> p) {
+  __shared__ __align__(16) T tile[2][TY + 6][TX + 8];
+  __shared__ __align__(16) T fy[TY][TX];
+  __shared__ T fx[TY];
+  const double hmax = stage_tile_pairs<T, KIND, K64, TX, TY, TZ>(
+      p, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, tile, fy, fx);
+  block_max_partial<KIND, TX / 2 * TY>(p, hmax);
+}
+
+// The face ghost cells of phi that the stencils of fill-box cells in planes
+// [k0, k1] read, written as stored values: beyond face f of the domain box
+// (bits of bc_mask as in fetch_bc) the 3 layers over the domain's
+// cross-section, from the same expressions as fetch_bc (linear: e0 +
+// (e0 - e1) dist; copy: e0; periodic: the cell one period in).  x and y
+// faces over planes [k0, k1]; the z faces when stencils of those planes
+// reach them.
+// Each value depends on cells of the domain box only (no edge or corner
+// ghost is read or written), so the threads are independent; the launcher
+// requires at least 3 domain cells along every axis with a bit set.
+template <typename T>
+__global__ void k_face_ghosts(T* phi, Box gb, FillBox dom, unsigned m, int k0, int k1) {
+  const int nx = dom.n(0), ny = dom.n(1), nz = dom.n(2);
+  const int np = k1 - k0 + 1;
+  const long nxf = 6L * ny * np, nyf = 6L * nx * np;
+  const bool zlo = k0 - 3 < dom.lo[2], zhi = k1 + 3 > dom.hi[2];
+  const long nzf = 3L * nx * ny;
+  const long total = nxf + nyf + (zlo ? nzf : 0) + (zhi ? nzf : 0);
+  const Grid3<T> g = make_grid(phi, gb);
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total;
+       q += (long)gridDim.x * blockDim.x) {
+    int face, i, j, k, dist;
+    long r = q;
+    if (r < nxf) {          // x faces: (side, layer, j, k)
+      face = (int)(r % 2); r /= 2;
+      dist = 1 + (int)(r % 3); r /= 3;
+      j = dom.lo[1] + (int)(r % ny); k = k0 + (int)(r / ny);
+      i = face ? dom.hi[0] + dist : dom.lo[0] - dist;
+    } else if ((r -= nxf) < nyf) {   // y faces
+      face = 2 + (int)(r % 2); r /= 2;
+      dist = 1 + (int)(r % 3); r /= 3;
+      i = dom.lo[0] + (int)(r % nx); k = k0 + (int)(r / nx);
+      j = face == 3 ? dom.hi[1] + dist : dom.lo[1] - dist;
+    } else {                // z faces
+      r -= nyf;
+      face = (zlo && r < nzf) ? 4 : 5;
+      if (face == 5 && zlo) r -= nzf;
+      dist = 1 + (int)(r % 3); r /= 3;
+      i = dom.lo[0] + (int)(r % nx); j = dom.lo[1] + (int)(r / nx);
+      k = face == 5 ? dom.hi[2] + dist : dom.lo[2] - dist;
     }
-    const int lane = (ty * TX + tx) & 31, wid = (ty * TX + tx) >> 5;
-    if (lane == 0) red[wid] = m;
-    __syncthreads();
-    if (wid == 0) {
-      m = (lane < TX * TY / 32) ? red[lane] : -1.0;
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double o2 = __shfl_xor_sync(0xffffffffu, m, off);
-        m = (o2 > m) ? o2 : m;
-      }
-      if (lane == 0)
-        p.partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = m;
+    const int d = face >> 1;
+    const bool hi = face & 1;
+    int c[3] = {i, j, k};
+    const int n = dom.n(d);
+    T v;
+    if (m & (1u << (16 + face))) {
+      c[d] += hi ? -n : n;
+      v = *g.ptr(c[0], c[1], c[2]);
+    } else if (m & (1u << (8 + face))) {
+      c[d] = hi ? dom.hi[d] : dom.lo[d];
+      v = *g.ptr(c[0], c[1], c[2]);
+    } else if (m & (1u << face)) {
+      c[d] = hi ? dom.hi[d] : dom.lo[d];
+      const T e0 = *g.ptr(c[0], c[1], c[2]);
+      c[d] += hi ? -1 : 1;
+      const T e1 = *g.ptr(c[0], c[1], c[2]);
+      const T slope = e0 - e1;
+      v = e0 + slope * (T)dist;
+    } else {
+      continue;
     }
+    *g.ptr(i, j, k) = v;
   }
 }
 

@@ -37,30 +37,69 @@ StageParams<T> to_params(const StageArgs& a) {
   return p;
 }
 
+#ifndef LSMGPU_STAGE_PAIRS
+#define LSMGPU_STAGE_PAIRS 1
+#endif
+
+// The boundary values of a.bc_mask can be stored in phi_s's ghost cells:
+// the caller allows it, and every axis with a boundary kind has at least 3
+// domain cells (so no ghost value depends on another ghost cell).
+bool ghosts_storable(const StageArgs& a) {
+  if (!a.ghosts_writable) return false;
+  for (int d = 0; d < 3; d++) {
+    const unsigned face_bits = 3u << (2 * d);
+    const bool any = (a.bc_mask & (face_bits | face_bits << 8 | face_bits << 16)) != 0u;
+    if (any && a.dom.n(d) < 3) return false;
+  }
+  return true;
+}
+
+// One kind: the face-shared two-cells-per-thread kernel where it applies
+// (FMA or FP32 arithmetic, two-sided kinds) and the ghost cells are stored
+// (no boundary kind, or k_face_ghosts writes them first); else one cell per
+// thread with the boundary values generated on the fly.  Both cover TX x TY
+// x TZ cells per block, so the grid (and the per-block CFL partials) are the
+// same.
+template <typename T, int KIND>
+void launch_kind(dim3 grid, const StageArgs& a, const StageParams<T>& p, cudaStream_t st) {
+  constexpr int TX = kStageTX, TY = kStageTY, TZ = kStageTZ;
+  if constexpr (LSMGPU_STAGE_PAIRS && UseFaces<T, KIND, STAGE_FAST, TX>::value) {
+    if (a.bc_mask == 0u || ghosts_storable(a)) {
+      StageParams<T> q = p;
+      if (a.bc_mask != 0u) {
+        // the planes of the fill box, and the z faces its stencils reach
+        k_face_ghosts<T><<<296, 256, 0, st>>>((T*)a.phi_s, a.gb, a.dom, a.bc_mask,
+                                               a.fb.lo[2], a.fb.hi[2]);
+        ++launch_counter();
+        q.bc_mask = 0u;
+      }
+      const dim3 blk(TX / 2, TY, 1);
+      if constexpr (sizeof(T) == 4) {
+        if (p.fp64_policy & kFp64Kinks) {
+          k_stage_pairs<T, KIND, true, TX, TY, TZ><<<grid, blk, 0, st>>>(q);
+          return;
+        }
+      }
+      k_stage_pairs<T, KIND, false, TX, TY, TZ><<<grid, blk, 0, st>>>(q);
+      return;
+    }
+  }
+  k_stage<T, KIND, STAGE_FAST, TX, TY, TZ><<<grid, dim3(TX, TY, 1), 0, st>>>(p);
+}
+
 template <typename T>
 cudaError_t launch_t(int kind, const StageArgs& a, cudaStream_t st) {
   constexpr int TX = kStageTX, TY = kStageTY, TZ = kStageTZ;
   const FillBox& fb = a.fb;
   dim3 grid((fb.n(0) + TX - 1) / TX, (fb.n(1) + TY - 1) / TY,
             (fb.n(2) + TZ - 1) / TZ);
-  dim3 blk(TX, TY, 1);
   const StageParams<T> p = to_params<T>(a);
   switch (kind) {
-    case kStageAdvect:
-      k_stage<T, kStageAdvect, STAGE_FAST, TX, TY, TZ><<<grid, blk, 0, st>>>(p);
-      break;
-    case kStageNormal:
-      k_stage<T, kStageNormal, STAGE_FAST, TX, TY, TZ><<<grid, blk, 0, st>>>(p);
-      break;
-    case kStageReinit:
-      k_stage<T, kStageReinit, STAGE_FAST, TX, TY, TZ><<<grid, blk, 0, st>>>(p);
-      break;
-    case kStageDeformation:
-      k_stage<T, kStageDeformation, STAGE_FAST, TX, TY, TZ><<<grid, blk, 0, st>>>(p);
-      break;
-    case kStageNormalRhs:
-      k_stage<T, kStageNormalRhs, STAGE_FAST, TX, TY, TZ><<<grid, blk, 0, st>>>(p);
-      break;
+    case kStageAdvect: launch_kind<T, kStageAdvect>(grid, a, p, st); break;
+    case kStageNormal: launch_kind<T, kStageNormal>(grid, a, p, st); break;
+    case kStageReinit: launch_kind<T, kStageReinit>(grid, a, p, st); break;
+    case kStageDeformation: launch_kind<T, kStageDeformation>(grid, a, p, st); break;
+    case kStageNormalRhs: launch_kind<T, kStageNormalRhs>(grid, a, p, st); break;
     default:
       return cudaErrorInvalidValue;
   }

@@ -28,6 +28,10 @@ struct StageArgs {
   const double* defo_tab;  // kStageDeformation (see StageParams)
   int defo_off[3];
   const double* g_dev;
+  // the stage input's ghost cells may be written (set by the drivers, whose
+  // arrays these are): the face-shared kinds then store the boundary values
+  // of bc_mask into phi_s's ghost cells and read them as stored
+  int ghosts_writable;
 };
 
 // tile of the stage kernels: TX x TY cells per block, TZ planes per block

@@ -123,33 +123,3 @@ def stage(kind, precision, out, phi_s, phi_n, aux, gb, fb, dx, dt, rk_kind,
                                      int(bc_mask), dbls(dx), dt_dev, float(dt),
                                      int(rk_kind), int(use_phi0))
     gpu.check_rc(rc, "lse_stage")
-
-
-def smoke_check():
-    """Two FP64 TVD-RK3 steps of a sphere under a constant velocity on cuda:0,
-    checked against the oracle's reference-order chain bit for bit."""
-    import oracle
-    from oracle.driver import Grid, Stepper
-
-    g = Grid((20, 18, 16), dx=(0.1, 0.1, 0.1))
-    x, y, z = g.centers((-1.0, -0.9, -0.8))
-    phi0 = np.sqrt((x - 0.1) ** 2 + (y + 0.05) ** 2 + z ** 2) - 0.35
-    vel = [g.field(np.full(g.shape, c)) for c in (1.0, 0.5, 0.25)]
-    dt = 0.02
-    ref = g.field(phi0)
-    st = Stepper(oracle.oracle_toolbox(), g)
-    for _ in range(2):
-        st.advect_step(ref, lambda c: vel, dt)
-    prev = get_fp_mode()
-    set_fp_mode(FP_STRICT)
-    try:
-        ws = Workspace(g.gb, 8)
-        d = gpu.DeviceArray.from_host(phi0)
-        dv = [gpu.DeviceArray.from_host(v.data) for v in vel]
-        ws.advect(d, dv, g.fb, g.dx, dt_fixed=dt, nsteps=2)
-        got = g.interior(g.field(d.download()))
-        want = g.interior(ref)
-        assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), \
-            "fused TVD-RK3 differs from the oracle"
-    finally:
-        set_fp_mode(prev)

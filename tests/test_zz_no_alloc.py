@@ -125,6 +125,27 @@ def test_rejects_fill_box_beyond_the_static_scratch():
     lib.lsmgpu_get_last_error()
 
 
+def test_rejects_tile_counts_that_wrap_32_bits():
+    """2^17 x 2^15 x 1 tiles = 2^32: a 32-bit count would wrap to 0 and pass
+    the size check.  The entry point counts in 64 bits and refuses the box
+    before it looks at the arrays (host arrays here: nothing reaches the
+    GPU)."""
+    from lsmlib_b200 import gpu
+    from lsmlib_b200.ext_abi import dbls, ints
+    lib = gpu.load()
+    a = np.zeros((4, 4, 4), order="F")
+    fb = (0, 32 * 2 ** 17 - 1, 0, 8 * 2 ** 15 - 1, 0, 15)
+    gb = (-3, fb[1] + 3, -3, fb[3] + 3, -3, fb[5] + 3)
+    dt = ctypes.c_double(0.0)
+    rc = lib.lsmgpu_normal_rhs_dt_noalloc(a.ctypes.data, ctypes.byref(dt), a.ctypes.data,
+                                          a.ctypes.data, ints(gb), ints(fb),
+                                          dbls((0.1, 0.1, 0.1)), 0.5)
+    assert rc == 1
+    msg = lib.lsmgpu_get_last_error_string().decode()
+    assert "4294967296 tiles" in msg
+    lib.lsmgpu_get_last_error()
+
+
 def test_rejects_host_arrays():
     from lsmlib_b200 import gpu
     from lsmlib_b200.ext_abi import dbls, ints
