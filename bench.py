@@ -24,8 +24,8 @@ against the CPU oracle of the reference's heap march).  Under torchrun every ran
 
 ``--impl reference`` times the reference's own toolbox routines (translated
 from its Fortran sources, oracle/_ref) on all host cores, patch-decomposed as
-the reference's parallel package does, on a bounded z-slab of the same
-workload; rank 0 alone runs it.
+the reference's parallel package does, on the same full workload (a bounded
+number of timed steps); rank 0 alone runs it.
 """
 import argparse
 import ctypes
@@ -150,6 +150,98 @@ def max_over_ranks(pg, v):
     return float(t.item())
 
 
+def bench_config(cfg, world):
+    """The workload as both arms report it (the same dict)."""
+    return {"workload": WORKLOAD, "grid": list(cfg["n"]), "ghost": 3, "cfl": cfg["cfl"],
+            "reinit_interval": cfg["reinit_interval"], "reinit_iters": cfg["reinit_iters"],
+            "seed": cfg["seed"],
+            "l2": "inputs larger than L2 (144 MB per field)",
+            "parallelism": "replicas" if world > 1 else "single GPU"}
+
+
+def sig(x, n=4):
+    """Floats rounded to n significant digits, recursively."""
+    if isinstance(x, float):
+        return float("%.*g" % (n, x)) if np.isfinite(x) else x
+    if isinstance(x, dict):
+        return {k: sig(v, n) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [sig(v, n) for v in x]
+    return x
+
+
+# short names of nested keys in the final line's summaries
+SHORT = {"error_vs_fp64.max_abs": "err_max", "error_vs_fp64.max_abs_band_5dx": "err_band5dx",
+         "error_vs_fp64.l1_mean": "err_l1", "fd_check.max_rel_err": "fd_max_rel",
+         "fd_check.max_err_over_max_grad": "fd_max_over_grad",
+         "fd_check.max_rel_err_components_above_1pct": "fd_max_rel_above_1pct",
+         "vs_initial.max_abs_band": "vs_phi0_band_max",
+         "speedup_vs_per_grid_launches": "vs_per_grid_launches"}
+
+
+def pick(d, *keys):
+    """The keys of d that exist (dotted keys reach into nested dicts), under
+    their short names."""
+    if not isinstance(d, dict):
+        return d
+    out = {}
+    for k in keys:
+        cur, ok = d, True
+        for part in k.split("."):
+            if isinstance(cur, dict) and part in cur:
+                cur = cur[part]
+            else:
+                ok = False
+                break
+        if ok:
+            out[SHORT.get(k, k)] = cur
+    return out
+
+
+def run_parity(cfg, steps=2, reinit_pseudo_steps=1):
+    """The timed configuration itself against the oracle: `steps` physical
+    steps of the full 256^3 workload through the device drivers in the
+    bench's arithmetic (FMA, single-reciprocal weights), then
+    `reinit_pseudo_steps` reinitialization pseudo-steps, against the oracle's
+    chain of the reference's routines in the reference integrators' order
+    (LevelSetFunctionIntegrator.cc:1319-1510, ReinitializationAlgorithm.cc:
+    177-330) over z-slab patches on all host cores.  Relative max-norm
+    difference over the interior."""
+    import oracle
+    from lsmlib_b200 import gpu, integrator, workloads
+    from oracle.driver import Grid, PatchedNormalStepper
+    n = cfg["n"]
+    gb, fb = workloads.boxes(n)
+    dx = cfg["dx"]
+    integrator.set_fp_mode(integrator.FP_FAST)
+    ws = integrator.Workspace(gb, 8)
+    d_phi = gpu.DeviceArray.from_host(cfg["phi"])
+    d_F = gpu.DeviceArray.from_host(cfg["F"])
+    ws.normal(d_phi, d_F, fb, dx, cfl=cfg["cfl"], nsteps=steps, step0=0,
+              reinit_interval=10 ** 9, reinit_iters=0, use_phi0=cfg["use_phi0"])
+    ws.reinit(d_phi, fb, dx, cfl=cfg["cfl"], iters=reinit_pseudo_steps,
+              use_phi0=cfg["use_phi0"])
+    got = d_phi.download()
+    del ws, d_phi, d_F
+    t0 = time.perf_counter()
+    g = Grid(tuple(n), dx=dx)
+    phi, F = g.field(cfg["phi"]), g.field(cfg["F"])
+    ps = PatchedNormalStepper(oracle.oracle_toolbox(), g, os.cpu_count() or 1)
+    parts, Fs = ps.scatter(phi), ps.scatter(F)
+    for _ in range(steps):
+        ps.normal_step(parts, Fs, cfg["cfl"])
+    ps.reinit(parts, cfg["cfl"], reinit_pseudo_steps, cfg["use_phi0"])
+    ps.gather(parts, phi)
+    t_cpu = time.perf_counter() - t0
+    want = g.interior(phi)
+    have = g.interior(g.field(got))
+    max_rel = float(np.max(np.abs(have - want)) / np.max(np.abs(want)))
+    return {"max_rel": max_rel, "bound": 1e-12, "ok": max_rel <= 1e-12,
+            "steps": steps, "reinit_pseudo_steps": reinit_pseudo_steps,
+            "mode": "fast: FMA, one-reciprocal WENO5 weights",
+            "oracle_s": round(t_cpu, 1)}
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -243,6 +335,9 @@ def run_ours(args, world, rank, local, pg):
                           "reinitialization sign, stochastic rounding of stage outputs"}
 
     # ---- dominant kernels, timed alone on the same stream -----------------
+    # the stage kernel the drivers launch: face-shared, two cells per
+    # thread, reading ghost cells the drivers have stored (bc_mask 0 here:
+    # phi64's ghost cells hold the drivers' last boundary values)
     peak, peak_kind = load_peaks()
     kern = {}
     for name, kind, rk, nbytes in (("stage_reinit_rk32", 2, 32, 3),
@@ -252,11 +347,11 @@ def run_ours(args, world, rank, local, pg):
         b = gpu.DeviceArray.from_host(phi64)
         c = gpu.DeviceArray.from_host(phi64)
         for _ in range(3):
-            integrator.stage(kind, 8, a, b, c, [d_F], gb, fb, dx, 1e-3, rk)
+            integrator.stage(kind, 8, a, b, c, [d_F], gb, fb, dx, 1e-3, rk, bc_mask=0)
         reps = 20
         timer.start()
         for _ in range(reps):
-            integrator.stage(kind, 8, a, b, c, [d_F], gb, fb, dx, 1e-3, rk)
+            integrator.stage(kind, 8, a, b, c, [d_F], gb, fb, dx, 1e-3, rk, bc_mask=0)
         timer.stop()
         t = timer.ms() / reps
         kern[name] = {"ms": t, "bytes": nbytes * 8 * cells}
@@ -337,29 +432,104 @@ def run_ours(args, world, rank, local, pg):
         deformation_res = run_config3(lib, pg, world,
                                       n_full=512 if args.config3_full else 256)
 
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = run_parity(cfg)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(cfg)
 
+    # every leg in full on a line of its own; the final line carries compact
+    # summaries (the driver keeps the last few KB of the output)
+    legs = {"parts": parts, "fp32": fp32, "batched": batched_res, "adjoint": adjoint_res,
+            "deformation": deformation_res, "toolbox": toolbox_res,
+            "distance": distance_res, "roofline": roofline, "e2e": e2e, "parity": parity,
+            "cpu_baseline": cpu}
+    if rank == 0:
+        for k, v in legs.items():
+            if v is not None:
+                print(json.dumps({"bench_detail": k, "data": v}), flush=True)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": K, "warmup": W, "ms_per_step": ms_max / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": list(n), "ghost": 3,
-                   "cfl": cfg["cfl"], "reinit_interval": interval,
-                   "reinit_iters": iters, "seed": cfg["seed"],
-                   "fp_mode": "fast (FMA, single-reciprocal WENO5 weights; <=1e-12 rel. vs reference)",
-                   "l2": "inputs larger than L2 (144 MB per field, 6 fields live)",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
-        "parts": parts, "fp32": fp32, "batched": batched_res, "adjoint": adjoint_res,
-        "deformation": deformation_res, "toolbox": toolbox_res, "distance": distance_res,
-        "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
-        "clocks": clk,
+        "config": bench_config(cfg, world),
+        "parts": {k: sig(pick(v, "value", "ms_per_pseudo_step", "ms_per_step"))
+                  for k, v in parts.items()}, "parity": sig(parity, 3) if parity else None,
+        "fp32": sig(pick(fp32, "value", "speedup_vs_fp64", "error_vs_fp64.max_abs",
+                         "error_vs_fp64.max_abs_band_5dx", "error_vs_fp64.l1_mean")),
+        "batched": sig(compact_batched(batched_res)),
+        "adjoint": sig(pick(adjoint_res, "reverse_over_forward", "gradient_over_forward",
+                            "forward_ms", "reverse_ms", "fd_check.max_rel_err",
+                            "fd_check.max_err_over_max_grad",
+                            "fd_check.max_rel_err_components_above_1pct")),
+        "deformation": sig(compact_deformation(deformation_res), 3),
+        "toolbox": sig(compact_toolbox(toolbox_res)),
+        "distance": sig(compact_distance(distance_res)),
+        "roofline": sig(pick(roofline, "bound", "achieved", "peak", "unit", "frac",
+                             "traffic", "kernel", "kernel_ms", "peak_source",
+                             "fp64_pipe_active_pct_ncu")),
+        "e2e": sig(pick(e2e, "value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step",
+                        "ms_per_step")),
+        "gpu_launches": int(launches),
+        "clocks": sig(clk),
     }
     if cpu is not None:
-        line["cpu_baseline"] = cpu
+        line["cpu_baseline"] = sig(pick(cpu, "value", "unit", "cores", "kind", "sample"))
+        line["cpu_baseline"]["sample"] = "256x256x64 slab, 1 step + its reinit share"
     return line
+
+
+def compact_batched(r):
+    if not r:
+        return r
+    out = {"cells": r.get("cells")}
+    for key in ("fp64", "fp32"):
+        e = r.get(key) or {}
+        out[key] = pick(e, "value", "ms_per_step", "speedup_vs_per_grid_launches",
+                        "error_vs_fp64.max_abs", "error_vs_fp64.max_abs_band_5dx")
+    if "cpu_baseline" in r:
+        out["cpu"] = pick(r["cpu_baseline"], "value", "cores")
+    return out
+
+
+def compact_deformation(r):
+    if not r:
+        return r
+    return {k: pick(v, "value", "vs_initial.max_abs_band", "error_vs_fp64.max_abs",
+                    "error_vs_fp64.max_abs_band_5dx")
+            for k, v in r.items() if isinstance(v, dict)}
+
+
+def compact_toolbox(r):
+    """Routine count and the spread of their HBM fractions (the per-routine
+    table is on its detail line)."""
+    if not r:
+        return r
+    r = r.get("routines", r)
+    fr = sorted(v["frac_of_measured_hbm"] for v in r.values()
+                if isinstance(v, dict) and "frac_of_measured_hbm" in v)
+    if not fr:
+        return {"routines": len(r)}
+    return {"routines": len(fr), "hbm_frac_min": fr[0], "hbm_frac_median": fr[len(fr) // 2],
+            "hbm_frac_max": fr[-1]}
+
+
+def compact_distance(r):
+    """Points/s of each solver and order at the largest grid, and whether
+    every result checked against the oracle was bit-exact (the full table is
+    on its detail line)."""
+    if not r or "sizes" not in r:
+        return r
+    sizes = r["sizes"]
+    big = max(sizes, key=lambda k: int(k.split("^")[0]))
+    pts = {k: v["value"] for k, v in sizes[big].items() if isinstance(v, dict) and "value" in v}
+    exact = [v["bitwise_vs_oracle"] for e in sizes.values() for v in e.values()
+             if isinstance(v, dict) and "bitwise_vs_oracle" in v]
+    return {"grid": big, "points_per_s": pts,
+            "bit_exact_all_checked": all(exact) if exact else None}
 
 
 def run_adjoint(n_fd=20, h=1e-6):
@@ -867,44 +1037,59 @@ def cpu_batched_sample():
                       "cells), one process per core, %.1f s" % (len(grids), cells / 1e6, wall)}
 
 
-def run_reference(args, world, rank):
+def run_reference(args, world, rank, budget_s=90.0):
+    """The reference's own toolbox routines (the translated Fortran when it
+    is built, else the C oracle) on the same workload as our arm: the full
+    256^3 grid, patch-decomposed in z with one patch per host thread (16
+    patches of 16 planes on a 16-core host), as the reference's parallel
+    package runs it -- a 3-cell ghost exchange before every stage and the
+    minimum of the patch dts (LevelSetFunctionIntegrator.cc:382, :567,
+    :1377).  A step is one time step plus its share of reinitialization
+    (2 pseudo-steps: 20 every 10 steps).  The warm-up steps run in full; the
+    timed steps stop once `budget_s` seconds have passed (the rate is the
+    same per step), so the run stays within a few minutes."""
     if rank != 0:
         return None
-    from oracle.driver import PatchedNormalStepper
+    from oracle.driver import Grid, PatchedNormalStepper
     from lsmlib_b200 import workloads
     cfg = workloads.config2(N_CELLS)
     threads = os.cpu_count() or 1
-    nz = max(8, 4 * threads)
     tb, kind = reference_toolbox()
-    g, phi, F = slab_case(cfg, nz)
+    g = Grid(tuple(cfg["n"]), dx=cfg["dx"])
     ps = PatchedNormalStepper(tb, g, threads)
-    parts, Fs = ps.scatter(phi), ps.scatter(F)
+    parts, Fs = ps.scatter(g.field(cfg["phi"])), ps.scatter(g.field(cfg["F"]))
     iters_per_step = cfg["reinit_iters"] // cfg["reinit_interval"]
 
     def step():
         ps.normal_step(parts, Fs, cfg["cfl"])
-        ps.reinit(parts, cfg["cfl"], iters_per_step)
+        ps.reinit(parts, cfg["cfl"], iters_per_step, cfg["use_phi0"])
 
     for _ in range(args.warmup):
         step()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    timed = 0
+    while timed < args.steps:
         step()
+        timed += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
     dt = time.perf_counter() - t0
     cells = g.n[0] * g.n[1] * g.n[2]
-    value = cells * args.steps / dt
+    value = cells * timed / dt
+    planes = sorted({pg.n[2] for pg, _ in ps.patches})
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / timed,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": WORKLOAD, "grid": list(cfg["n"]), "ghost": 3,
-                   "cfl": cfg["cfl"], "sample": "256x256x%d z-slab" % nz},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(ps.patches),
-                         "kind": kind,
-                         "sample": "256x256x%d slab, %d patches on %d threads; a step = "
-                                   "1 time step + %d reinit pseudo-steps"
-                                   % (nz, len(ps.patches), threads, iters_per_step)},
+        "config": bench_config(cfg, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": "full %s grid, %d z-patches of %s planes on %d threads; "
+                                   "%d of %d steps timed (%.0f s budget); a step = 1 time "
+                                   "step + %d reinit pseudo-steps"
+                                   % ("x".join(map(str, cfg["n"])), len(ps.patches),
+                                      "/".join(map(str, planes)), threads, timed,
+                                      args.steps, budget_s, iters_per_step)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -912,8 +1097,9 @@ def run_reference(args, world, rank):
 
 def profile_kernels():
     """Two launches each of the normal-velocity and reinitialization stage
-    kernels (TVD-RK3 stage 2, distinct phi_s and phi^n) on the workload's
-    grid, in FP64 and then in FP32."""
+    kernels (TVD-RK3 stage 2, distinct phi_s and phi^n, ghost cells read as
+    stored: the kernel the drivers launch) on the workload's grid, in FP64
+    and then in FP32."""
     from lsmlib_b200 import gpu, integrator, workloads
     cfg = workloads.config2(N_CELLS)
     gb, fb = workloads.boxes(cfg["n"])
@@ -925,7 +1111,8 @@ def profile_kernels():
         f = gpu.DeviceArray.from_host(cfg["F"].astype(dtype))
         for kind in (1, 2):
             for _ in range(2):
-                integrator.stage(kind, prec, a, b, c, [f], gb, fb, cfg["dx"], 1e-3, 32)
+                integrator.stage(kind, prec, a, b, c, [f], gb, fb, cfg["dx"], 1e-3, 32,
+                                 bc_mask=0)
         gpu.check_rc(gpu.load().lsmgpu_stream_synchronize(), "sync")
         del a, b, c, f
 
@@ -969,6 +1156,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the parity check of the timed configuration")
     ap.add_argument("--no-cpu", action="store_true",
                     help="skip the CPU baseline sample of our arm")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 form")

@@ -232,8 +232,11 @@ __device__ __forceinline__ T godunov_sq2(T vn, T xp, T yp, T zp, T xm, T ym,
 }
 
 // reinitialization RHS of one cell (lsm_reinitialization3d.f.in:158-199,
-// :218-256); with fp64_sign the FP32 form evaluates the smoothed sign in FP64
-template <typename T>
+// :218-256); with fp64_sign the FP32 form evaluates the smoothed sign in FP64.
+// FASTM: the divisions by square roots and the square root of |grad phi|^2
+// through rsqrt_nr (FMA arithmetic; the strict form keeps the reference's
+// correctly rounded division and square root).
+template <typename T, bool FASTM = false>
 __device__ __forceinline__ T reinit_cell(T pc, T xp, T yp, T zp, T xm, T ym,
                                          T zm, T dx_sq, bool use0,
                                          bool fp64_sign) {
@@ -255,8 +258,17 @@ __device__ __forceinline__ T reinit_cell(T pc, T xp, T yp, T zp, T xm, T ym,
   const T nsq = gs[0] * gs[0] + gs[1] * gs[1] + gs[2] * gs[2];
   if (sizeof(T) == 4 && fp64_sign) {
     const double pd = pc, nd = nsq, dd = dx_sq;
+    if (FASTM) {
+      // |pc| >= 1e-11, so the sums are positive normal numbers
+      const double sgn = pd * rsqrt_nr(use0 ? pd * pd + dd : pd * pd + nd * dd);
+      return (T)(sgn * (1.0 - sqrt_nr(nd)));
+    }
     const double sgn = use0 ? pd / sqrt(pd * pd + dd) : pd / sqrt(pd * pd + nd * dd);
     return (T)(sgn * (1.0 - sqrt(nd)));
+  }
+  if (FASTM) {
+    const T sgn = pc * rsqrt_nr(use0 ? pc * pc + dx_sq : pc * pc + nsq * dx_sq);
+    return sgn * (T(1) - sqrt_nr(nsq));
   }
   const T sgn = use0 ? pc / sqrtT(pc * pc + dx_sq)
                      : pc / sqrtT(pc * pc + nsq * dx_sq);
@@ -453,30 +465,33 @@ __device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
 
 // Right-hand side of the two-sided kinds (normal speed, reinitialization)
 // from the six one-sided derivatives; accumulates the CFL speed of
-// kStageNormalRhs into hmax.
-template <typename T, int KIND>
+// kStageNormalRhs into hmax.  FASTM as for reinit_cell.
+template <typename T, int KIND, bool FASTM = false>
 __device__ __forceinline__ T two_sided_rhs(const StageParams<T>& p, T a0, T pc,
                                            T xp, T yp, T zp, T xm, T ym, T zm,
                                            double& hmax) {
   if (KIND == kStageReinit) {
     const T s = p.use_phi0 == 1 ? a0 : pc;
-    return reinit_cell(s, xp, yp, zp, xm, ym, zm, p.dx_sq, p.use_phi0 == 1,
-                       (p.fp64_policy & kFp64Sign) != 0);
+    return reinit_cell<T, FASTM>(s, xp, yp, zp, xm, ym, zm, p.dx_sq, p.use_phi0 == 1,
+                                 (p.fp64_policy & kFp64Sign) != 0);
   }
   // LSM3D_ADD_NORMAL_VEL_TERM_TO_LSE_RHS (:209-231)
   const T f = a0;
   T L = T(0);
-  if (fabsT(f) >= stage_zero_tol<T>())
-    L = T(0) - f * sqrtT(godunov_sq2(f, xp, yp, zp, xm, ym, zm));
+  if (fabsT(f) >= stage_zero_tol<T>()) {
+    const T g2 = godunov_sq2(f, xp, yp, zp, xm, ym, zm);
+    L = T(0) - f * (FASTM ? sqrt_nr(g2) : sqrtT(g2));
+  }
   if (KIND == kStageNormalRhs) {
     // LSM3D_COMPUTE_STABLE_NORMAL_VEL_DT per-cell speed (FP64)
     const double cx = fmax2(fabs((double)xp), fabs((double)xm));
     const double cy = fmax2(fabs((double)yp), fabs((double)ym));
     const double cz = fmax2(fabs((double)zp), fabs((double)zm));
-    const double ng = sqrt(cx * cx + cy * cy + cz * cz + (double)p.dx_sq);
-    const double h = fabs((double)f) / ng *
-                     (cx * (double)p.inv[0] + cy * (double)p.inv[1] +
-                      cz * (double)p.inv[2]);
+    const double n2 = cx * cx + cy * cy + cz * cz + (double)p.dx_sq;
+    const double sum = cx * (double)p.inv[0] + cy * (double)p.inv[1] + cz * (double)p.inv[2];
+    // n2 >= dx_sq > 0
+    const double h = FASTM ? fabs((double)f) * rsqrt_nr(n2) * sum
+                           : fabs((double)f) / sqrt(n2) * sum;
     hmax = (h > hmax) ? h : hmax;
   }
   return L;
@@ -822,13 +837,14 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
     if (act0) {
       const T2 ym = *reinterpret_cast<const T2*>(&fy[ty][c0]);
       const T xm0 = t == 0 ? fx[ty] : xm_left;
-      const T L0 = two_sided_rhs<T, KIND>(p, a00, w0[3], xp0, yp0, zp0, xm0, ym.x, zrun0, hmax);
+      const T L0 =
+          two_sided_rhs<T, KIND, true>(p, a00, w0[3], xp0, yp0, zp0, xm0, ym.x, zrun0, hmax);
       zrun0 = znx0;
       if (KIND == kStageNormalRhs) p.rhs_out[o0] = L0;
       else p.out[o0] = stage_out(p, o0, uc0, w0[3], L0, dt);
       if (act1) {
-        const T L1 = two_sided_rhs<T, KIND>(p, a01, w1[3], xp1, yp1, zp1, xm1, ym.y, zrun1,
-                                            hmax);
+        const T L1 = two_sided_rhs<T, KIND, true>(p, a01, w1[3], xp1, yp1, zp1, xm1, ym.y,
+                                                  zrun1, hmax);
         zrun1 = znx1;
         if (KIND == kStageNormalRhs) p.rhs_out[o0 + 1] = L1;
         else p.out[o0 + 1] = stage_out(p, o0 + 1, uc1, w1[3], L1, dt);
@@ -922,63 +938,73 @@ k_stage_pairs(StageParams<T> p) {
 // cross-section, from the same expressions as fetch_bc (linear: e0 +
 // (e0 - e1) dist; copy: e0; periodic: the cell one period in).  x and y
 // faces over planes [k0, k1]; the z faces when stencils of those planes
-// reach them.
-// Each value depends on cells of the domain box only (no edge or corner
-// ghost is read or written), so the threads are independent; the launcher
-// requires at least 3 domain cells along every axis with a bit set.
+// reach them.  Each value depends on cells of the domain box only (no edge
+// or corner ghost is read or written), so the threads are independent; the
+// launcher requires at least 3 domain cells along every axis with a bit set.
+// Block b < k1-k0+1 writes the x and y ghosts of plane k0+b (the 6 cells of
+// a row's two ends together, then the 6 rows of the y faces along x); the
+// remaining blocks write the z ghost planes, zchunks blocks per plane.
 template <typename T>
-__global__ void k_face_ghosts(T* phi, Box gb, FillBox dom, unsigned m, int k0, int k1) {
-  const int nx = dom.n(0), ny = dom.n(1), nz = dom.n(2);
+__device__ __forceinline__ T face_ghost_value(const Grid3<T>& g, const FillBox& dom,
+                                              unsigned m, int face, int dist, int c[3]) {
+  const int d = face >> 1;
+  const bool hi = face & 1;
+  if (m & (1u << (16 + face))) {
+    c[d] += hi ? -dom.n(d) : dom.n(d);
+    return *g.ptr(c[0], c[1], c[2]);
+  }
+  c[d] = hi ? dom.hi[d] : dom.lo[d];
+  const T e0 = *g.ptr(c[0], c[1], c[2]);
+  if (m & (1u << (8 + face))) return e0;
+  c[d] += hi ? -1 : 1;
+  const T e1 = *g.ptr(c[0], c[1], c[2]);
+  const T slope = e0 - e1;
+  return e0 + slope * (T)dist;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_face_ghosts(T* phi, Box gb, FillBox dom, unsigned m, int k0, int k1, int zchunks) {
+  const int nx = dom.n(0), ny = dom.n(1);
   const int np = k1 - k0 + 1;
-  const long nxf = 6L * ny * np, nyf = 6L * nx * np;
-  const bool zlo = k0 - 3 < dom.lo[2], zhi = k1 + 3 > dom.hi[2];
-  const long nzf = 3L * nx * ny;
-  const long total = nxf + nyf + (zlo ? nzf : 0) + (zhi ? nzf : 0);
   const Grid3<T> g = make_grid(phi, gb);
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total;
-       q += (long)gridDim.x * blockDim.x) {
-    int face, i, j, k, dist;
-    long r = q;
-    if (r < nxf) {          // x faces: (side, layer, j, k)
-      face = (int)(r % 2); r /= 2;
-      dist = 1 + (int)(r % 3); r /= 3;
-      j = dom.lo[1] + (int)(r % ny); k = k0 + (int)(r / ny);
-      i = face ? dom.hi[0] + dist : dom.lo[0] - dist;
-    } else if ((r -= nxf) < nyf) {   // y faces
-      face = 2 + (int)(r % 2); r /= 2;
-      dist = 1 + (int)(r % 3); r /= 3;
-      i = dom.lo[0] + (int)(r % nx); k = k0 + (int)(r / nx);
-      j = face == 3 ? dom.hi[1] + dist : dom.lo[1] - dist;
-    } else {                // z faces
-      r -= nyf;
-      face = (zlo && r < nzf) ? 4 : 5;
-      if (face == 5 && zlo) r -= nzf;
-      dist = 1 + (int)(r % 3); r /= 3;
-      i = dom.lo[0] + (int)(r % nx); j = dom.lo[1] + (int)(r / nx);
-      k = face == 5 ? dom.hi[2] + dist : dom.lo[2] - dist;
+  const unsigned any_face[6] = {m & 0x10101u, m & 0x20202u, m & 0x40404u,
+                                m & 0x80808u, m & 0x101010u, m & 0x202020u};
+  const int b = (int)blockIdx.x;
+  if (b < np) {
+    const int k = k0 + b;
+    // x faces: item q = 6 j + r, r = side * 3 + layer
+    for (int q = threadIdx.x; q < 6 * ny; q += blockDim.x) {
+      const int j = dom.lo[1] + q / 6, r = q % 6;
+      const int face = r / 3, dist = r % 3 + 1;
+      if (!any_face[face]) continue;
+      const int i = face ? dom.hi[0] + dist : dom.lo[0] - dist;
+      int c[3] = {i, j, k};
+      *g.ptr(i, j, k) = face_ghost_value(g, dom, m, face, dist, c);
     }
-    const int d = face >> 1;
-    const bool hi = face & 1;
+    // y faces: item q = nx r + (i - lo), r = side * 3 + layer
+    for (int q = threadIdx.x; q < 6 * nx; q += blockDim.x) {
+      const int i = dom.lo[0] + q % nx, r = q / nx;
+      const int face = 2 + r / 3, dist = r % 3 + 1;
+      if (!any_face[face]) continue;
+      const int j = face == 3 ? dom.hi[1] + dist : dom.lo[1] - dist;
+      int c[3] = {i, j, k};
+      *g.ptr(i, j, k) = face_ghost_value(g, dom, m, face, dist, c);
+    }
+    return;
+  }
+  // z ghost planes: plane zp = side * 3 + layer, chunk of its nx * ny cells
+  const int zp = (b - np) / zchunks, chunk = (b - np) % zchunks;
+  const int face = 4 + zp / 3, dist = zp % 3 + 1;
+  if (!any_face[face]) return;
+  if (face == 4 ? k0 - 3 >= dom.lo[2] : k1 + 3 <= dom.hi[2]) return;   // not reached
+  const int k = face == 5 ? dom.hi[2] + dist : dom.lo[2] - dist;
+  const int cells = nx * ny, per = (cells + zchunks - 1) / zchunks;
+  const int end = min(cells, (chunk + 1) * per);
+  for (int q = chunk * per + threadIdx.x; q < end; q += blockDim.x) {
+    const int i = dom.lo[0] + q % nx, j = dom.lo[1] + q / nx;
     int c[3] = {i, j, k};
-    const int n = dom.n(d);
-    T v;
-    if (m & (1u << (16 + face))) {
-      c[d] += hi ? -n : n;
-      v = *g.ptr(c[0], c[1], c[2]);
-    } else if (m & (1u << (8 + face))) {
-      c[d] = hi ? dom.hi[d] : dom.lo[d];
-      v = *g.ptr(c[0], c[1], c[2]);
-    } else if (m & (1u << face)) {
-      c[d] = hi ? dom.hi[d] : dom.lo[d];
-      const T e0 = *g.ptr(c[0], c[1], c[2]);
-      c[d] += hi ? -1 : 1;
-      const T e1 = *g.ptr(c[0], c[1], c[2]);
-      const T slope = e0 - e1;
-      v = e0 + slope * (T)dist;
-    } else {
-      continue;
-    }
-    *g.ptr(i, j, k) = v;
+    *g.ptr(i, j, k) = face_ghost_value(g, dom, m, face, dist, c);
   }
 }
 

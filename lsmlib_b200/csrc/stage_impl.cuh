@@ -1,6 +1,8 @@
 // stage_impl.cuh -- instantiation of the fused stage kernels for one
 // arithmetic mode.  Included once by stage_strict.cu (STAGE_FAST = false,
 // built with --fmad=false) and once by stage_fast.cu (STAGE_FAST = true, FMA).
+#include <algorithm>
+
 #include "launch.h"
 #include "stage.cuh"
 #include "stage_launch.h"
@@ -68,8 +70,10 @@ void launch_kind(dim3 grid, const StageArgs& a, const StageParams<T>& p, cudaStr
       StageParams<T> q = p;
       if (a.bc_mask != 0u) {
         // the planes of the fill box, and the z faces its stencils reach
-        k_face_ghosts<T><<<296, 256, 0, st>>>((T*)a.phi_s, a.gb, a.dom, a.bc_mask,
-                                               a.fb.lo[2], a.fb.hi[2]);
+        const int zchunks = (int)std::min<long>(
+            64, ((long)a.dom.n(0) * a.dom.n(1) + 2047) / 2048);
+        k_face_ghosts<T><<<a.fb.n(2) + 6 * zchunks, 256, 0, st>>>(
+            (T*)a.phi_s, a.gb, a.dom, a.bc_mask, a.fb.lo[2], a.fb.hi[2], zchunks);
         ++launch_counter();
         q.bc_mask = 0u;
       }

@@ -34,6 +34,31 @@ __device__ __forceinline__ float rcp_nr(float d) {
   return fmaf(r, e, r);
 }
 
+// 1/sqrt(x) for x > 0: the hardware seed (rsqrt.approx.ftz) refined by
+// Newton-Raphson steps for f(r) = 1/r^2 - x, r <- r + r (1 - x r^2) / 2
+// (each step doubles the correct bits; Markstein, IBM J. Res. Dev. 34(1),
+// 1990): two steps in FP64, one in FP32.  Fast-mode arithmetic only.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double r;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-(x * r), r, 1.0);
+  r = fma(0.5 * r, e, r);
+  e = fma(-(x * r), r, 1.0);
+  return fma(0.5 * r, e, r);
+}
+__device__ __forceinline__ float rsqrt_nr(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  const float e = fmaf(-(x * r), r, 1.0f);
+  return fmaf(0.5f * r, e, r);
+}
+// sqrt(x) for x >= 0 as x / sqrt(x) with rsqrt_nr; x below the normal range
+// (where the ftz seed would be infinite) takes the correctly rounded sqrt
+template <typename T>
+__device__ __forceinline__ T sqrt_nr(T x) {
+  return x >= T(sizeof(T) == 8 ? 1e-300 : 1e-30) ? x * rsqrt_nr(x) : T(sqrt(x));
+}
+
 // 2^-(unbiased exponent of x) for a positive normal x
 __device__ __forceinline__ double inv_pow2_of(double x) {
   const int e = (__double2hiint(x) >> 20) & 0x7ff;
