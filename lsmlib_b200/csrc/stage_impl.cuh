@@ -66,7 +66,8 @@ template <typename T, int KIND>
 void launch_kind(dim3 grid, const StageArgs& a, const StageParams<T>& p, cudaStream_t st) {
   constexpr int TX = kStageTX, TY = kStageTY, TZ = kStageTZ;
   if constexpr (LSMGPU_STAGE_PAIRS && UseFaces<T, KIND, STAGE_FAST, TX>::value) {
-    if (a.bc_mask == 0u || ghosts_storable(a)) {
+    const bool small = a.gb.sz() * (long)a.gb.n[2] < (1L << 31);   // 32-bit offsets
+    if (small && (a.bc_mask == 0u || ghosts_storable(a))) {
       StageParams<T> q = p;
       if (a.bc_mask != 0u) {
         // the planes of the fill box, and the z faces its stencils reach

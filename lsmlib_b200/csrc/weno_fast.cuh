@@ -59,6 +59,15 @@ __device__ __forceinline__ T sqrt_nr(T x) {
   return x >= T(sizeof(T) == 8 ? 1e-300 : 1e-30) ? x * rsqrt_nr(x) : T(sqrt(x));
 }
 
+// max and min for the eps maxima and the kink tests: a plain comparison in
+// FP64 (CUDA's IEEE fmax of doubles, which also sorts out NaN operands, cost
+// a third of the stage kernels' integer instructions; these values are
+// never NaN for finite phi), the native instruction in FP32
+__device__ __forceinline__ double vmax(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double vmin(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ float vmin(float a, float b) { return fminf(a, b); }
+
 // 2^-(unbiased exponent of x) for a positive normal x
 __device__ __forceinline__ double inv_pow2_of(double x) {
   const int e = (__double2hiint(x) >> 20) & 0x7ff;
@@ -79,7 +88,7 @@ __device__ __forceinline__ float inv_pow2_of(float x) {
 // indicators.
 template <typename T>
 __device__ __forceinline__ T weno5_side_fast(T D1, T D2, T D3, T D4, T D5, T inv) {
-  const T amax = fmax(fmax(fmax(fabs(D1), fabs(D2)), fmax(fabs(D3), fabs(D4))), fabs(D5));
+  const T amax = vmax(vmax(vmax(fabs(D1), fabs(D2)), vmax(fabs(D3), fabs(D4))), fabs(D5));
   const T eps = T(1e-6) * (amax * amax) + Consts<T>::tiny;
   const T c13_12 = T(13.0 / 12.0), c14 = T(0.25);
   const T ta = D1 - T(2) * D2 + D3, tb = D2 - T(2) * D3 + D4, tc = D3 - T(2) * D4 + D5;
@@ -131,9 +140,9 @@ __device__ __forceinline__ void weno5_pm_fast(const T* w, T inv, T& vp, T& vm) {
     V[m] = (w[m + 1] - w[m]) * inv;
     s[m] = V[m] * V[m];
   }
-  const T mid = fmax(fmax(s[1], s[2]), fmax(s[3], s[4]));
-  const T eps_m = T(1e-6) * fmax(mid, s[0]) + Consts<T>::tiny;
-  const T eps_p = T(1e-6) * fmax(mid, s[5]) + Consts<T>::tiny;
+  const T mid = vmax(vmax(s[1], s[2]), vmax(s[3], s[4]));
+  const T eps_m = T(1e-6) * vmax(mid, s[0]) + Consts<T>::tiny;
+  const T eps_p = T(1e-6) * vmax(mid, s[5]) + Consts<T>::tiny;
   const T c13_12 = T(13.0 / 12.0), c14 = T(0.25);
   T t;
   t = V[0] - T(2) * V[1] + V[2]; const T cA = t * t;
@@ -165,9 +174,9 @@ __device__ __forceinline__ void weno5_pm_fast(const T* w, T inv, T& vp, T& vm) {
   vm = weno5_weigh(mS1, mS2, mS3, mp1, mp2, mp3, eps_m);
   vp = weno5_weigh(pS1, pS2, pS3, pp1, pp2, pp3, eps_p);
   if (KINK64) {
-    const T scale = fmax(mid, fmax(s[0], s[5]));
-    const bool km = fmax(fmax(mS1, mS2), mS3) > T(1e3) * fmin(fmin(mS1, mS2), mS3) + T(1e-4) * scale;
-    const bool kp = fmax(fmax(pS1, pS2), pS3) > T(1e3) * fmin(fmin(pS1, pS2), pS3) + T(1e-4) * scale;
+    const T scale = vmax(mid, vmax(s[0], s[5]));
+    const bool km = vmax(vmax(mS1, mS2), mS3) > T(1e3) * vmin(vmin(mS1, mS2), mS3) + T(1e-4) * scale;
+    const bool kp = vmax(vmax(pS1, pS2), pS3) > T(1e3) * vmin(vmin(pS1, pS2), pS3) + T(1e-4) * scale;
     if (km || kp) {
       double wd[7];
 #pragma unroll
@@ -218,7 +227,7 @@ template <typename T, bool KINK64>
 __device__ __forceinline__ void weno5_face(const T* u, T inv, T& vp, T& vm) {
   const T V1 = u[1] - u[0], V2 = u[2] - u[1], V3 = u[3] - u[2], V4 = u[4] - u[3],
           V5 = u[5] - u[4];
-  const T amax = fmax(fmax(fmax(fabs(V1), fabs(V2)), fmax(fabs(V3), fabs(V4))), fabs(V5));
+  const T amax = vmax(vmax(vmax(fabs(V1), fabs(V2)), vmax(fabs(V3), fabs(V4))), fabs(V5));
   const T m = amax * amax;
   // the reference's 1e-6 max(v^2) + tiny, in units of the undivided
   // differences (the floor, reached only where every |D| < 1e-46, is kept
@@ -233,7 +242,7 @@ __device__ __forceinline__ void weno5_face(const T* u, T inv, T& vp, T& vm) {
   t = T(3) * V3 - T(4) * V4 + V5;
   const T Sc = c13_12 * (tc * tc) + c14 * (t * t);
   if (KINK64) {
-    const T mx = fmax(fmax(Sa, Sb), Sc), mn = fmin(fmin(Sa, Sb), Sc);
+    const T mx = vmax(vmax(Sa, Sb), Sc), mn = vmin(vmin(Sa, Sb), Sc);
     if (mx > T(1e3) * mn + T(1e-4) * m) {
       if constexpr (sizeof(T) == 4) {
         const float2 r = weno5_face_fp64(u[0], u[1], u[2], u[3], u[4], u[5], inv);
@@ -288,8 +297,8 @@ __device__ __forceinline__ bool weno5_is_kink(T v1, T v2, T v3, T v4, T v5) {
   t = v3 - T(2) * v4 + v5;
   u = T(3) * v3 - T(4) * v4 + v5;
   const T S3 = T(13.0 / 12.0) * (t * t) + T(0.25) * (u * u);
-  const T mx = fmax(fmax(S1, S2), S3), mn = fmin(fmin(S1, S2), S3);
-  const T scale = fmax(fmax(fmax(v1 * v1, v2 * v2), fmax(v3 * v3, v4 * v4)), v5 * v5);
+  const T mx = vmax(vmax(S1, S2), S3), mn = vmin(vmin(S1, S2), S3);
+  const T scale = vmax(vmax(vmax(v1 * v1, v2 * v2), vmax(v3 * v3, v4 * v4)), v5 * v5);
   return mx > T(1e3) * mn + T(1e-4) * scale;
 }
 
