@@ -606,6 +606,19 @@ int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace *ws, void *phi, const void *F,
                               const int fb[6], const double dx[3], double cfl,
                               int nsteps, int step0, int reinit_interval,
                               int reinit_iters, int use_phi0_for_sgn);
+/* Queueing of lsmgpu_normal_tvdrk3_host on this workspace.  on = 0 (the
+ * default): each call returns when phi is back in host memory.  on = 1: a
+ * call returns once its copies and kernels are queued, and successive calls
+ * overlap -- the next call's speed is copied to a second device buffer while
+ * this one computes, and each z-slab of phi is copied in as soon as the
+ * previous call's copy of that slab back to the host has landed.  The host
+ * arrays of a queued call must not be read or written until
+ * lsmgpu_workspace_sync returns (a later host call on the same workspace
+ * with the same arrays is ordered after it).  Switching back to 0 waits. */
+int lsmgpu_workspace_set_host_async(lsmgpu_workspace *ws, int on);
+/* waits until every queued lsmgpu_normal_tvdrk3_host call of the workspace
+ * has finished and its phi is in host memory */
+int lsmgpu_workspace_sync(lsmgpu_workspace *ws);
 /* iters TVD-RK3 reinitialization pseudo-steps of phi (in place) */
 int lsmgpu_reinit_tvdrk3(lsmgpu_workspace *ws, void *phi, const int fb[6],
                          const double dx[3], double cfl, int iters,

@@ -31,13 +31,22 @@ struct lsmgpu_workspace {
   void* phi2 = nullptr;
   void* rhs = nullptr;
   void* phi0 = nullptr;
-  // lsmgpu_normal_tvdrk3_host: device copies of the host level set and
-  // speed, the stream their slabs are copied on, one event per slab and
-  // direction (created on first use)
+  // lsmgpu_normal_tvdrk3_host: device copies of the host level set and of
+  // the speed (two buffers, alternating between queued calls), the streams
+  // of the slab copies to and from the host, and per slab: copied in, final
+  // stage done, copied out; per speed buffer: last read (created on first
+  // use)
   void* dphi = nullptr;
-  void* dF = nullptr;
-  cudaStream_t copy_stream = nullptr;
-  cudaEvent_t slab_ev[8] = {};
+  void* dF[2] = {nullptr, nullptr};
+  cudaStream_t copy_stream = nullptr;       // host -> device
+  cudaStream_t copy_stream_out = nullptr;   // device -> host
+  cudaEvent_t slab_ev[8] = {};              // [q] in, [4 + q] final stage
+  cudaEvent_t out_ev[4] = {};
+  cudaEvent_t F_ev[2] = {};
+  cudaEvent_t start_ev = nullptr;
+  int host_async = 0;       // lsmgpu_workspace_set_host_async
+  int host_pending = 0;     // a queued host call has not been waited for
+  unsigned host_calls = 0;
   double* defo_tab = nullptr;   // deformation sine tables (see stage.cuh)
   size_t defo_len = 0;
   double* scal = nullptr;   // device scalars (kDt, kT, kDtLast, kG0..kG0+2)
@@ -381,14 +390,46 @@ int lsmgpu_workspace_create(lsmgpu_workspace** out, const int gb[6],
 
 int lsmgpu_workspace_destroy(lsmgpu_workspace* ws) {
   if (!ws) return LSMGPU_SUCCESS;
+  if (ws->host_pending) lsmgpu_workspace_sync(ws);
   void* ps[] = {ws->phi1, ws->phi2, ws->rhs, ws->phi0, ws->defo_tab, ws->scal,
-                ws->partials, ws->dphi, ws->dF};
+                ws->partials, ws->dphi, ws->dF[0], ws->dF[1]};
   for (void* p : ps)
     if (p) cudaFree(p);
   for (cudaEvent_t e : ws->slab_ev)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : ws->out_ev)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : ws->F_ev)
+    if (e) cudaEventDestroy(e);
+  if (ws->start_ev) cudaEventDestroy(ws->start_ev);
   if (ws->copy_stream) cudaStreamDestroy(ws->copy_stream);
+  if (ws->copy_stream_out) cudaStreamDestroy(ws->copy_stream_out);
   delete ws;
+  return LSMGPU_SUCCESS;
+}
+
+int lsmgpu_workspace_set_host_async(lsmgpu_workspace* ws, int on) {
+  if (!ws_ok(ws, "lsmgpu_workspace_set_host_async")) return LSMGPU_ERR_NULL_POINTER;
+  if (!on && ws->host_pending) {
+    const int rc = lsmgpu_workspace_sync(ws);
+    if (rc != LSMGPU_SUCCESS) return rc;
+  }
+  ws->host_async = on ? 1 : 0;
+  return LSMGPU_SUCCESS;
+}
+
+int lsmgpu_workspace_sync(lsmgpu_workspace* ws) {
+  const char* R = "lsmgpu_workspace_sync";
+  if (!ws_ok(ws, R)) return LSMGPU_ERR_NULL_POINTER;
+  if (!ws->host_pending) return LSMGPU_SUCCESS;
+  ws->host_pending = 0;
+  // the copies back to the host are the last work of a host call; the
+  // speed buffers' events close its kernels
+  if (!cuda_ok(cudaStreamSynchronize(ws->copy_stream_out), R) ||
+      !cuda_ok(cudaStreamSynchronize(ws->copy_stream), R))
+    return LSMGPU_ERR_CUDA;
+  for (cudaEvent_t e : ws->F_ev)
+    if (!cuda_ok(cudaEventSynchronize(e), R)) return LSMGPU_ERR_CUDA;
   return LSMGPU_SUCCESS;
 }
 
@@ -698,7 +739,12 @@ int lsmgpu_normal_tvdrk3(lsmgpu_workspace* ws, void* phi, const void* F,
 // copied to the workspace's device buffers in kHostSlabs z-slabs while the
 // first step's RHS/CFL pass works through the slabs already there, and the
 // last step's final stage runs slab by slab, each slab copied back while the
-// next is computed.  Returns when phi is back in host memory.
+// next is computed.  By default the call returns when phi is back in host
+// memory.  With lsmgpu_workspace_set_host_async(ws, 1) it returns once its
+// work is queued, and successive calls overlap: the speed goes to the other
+// of two device buffers while the previous call still computes, and each
+// slab of phi is copied in as soon as the previous call's copy of that slab
+// back to the host has landed (copies in and out on two streams).
 namespace {
 constexpr int kHostSlabs = 4;
 }
@@ -718,14 +764,26 @@ int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
   cudaStream_t st = cur_stream();
   if (!ws->dphi) {
     if (!cuda_ok(cudaMalloc(&ws->dphi, ws->bytes), R) ||
-        !cuda_ok(cudaMalloc(&ws->dF, ws->bytes), R) ||
-        !cuda_ok(cudaStreamCreateWithFlags(&ws->copy_stream, cudaStreamNonBlocking), R))
+        !cuda_ok(cudaMalloc(&ws->dF[0], ws->bytes), R) ||
+        !cuda_ok(cudaStreamCreateWithFlags(&ws->copy_stream, cudaStreamNonBlocking), R) ||
+        !cuda_ok(cudaStreamCreateWithFlags(&ws->copy_stream_out, cudaStreamNonBlocking), R) ||
+        !cuda_ok(cudaEventCreateWithFlags(&ws->start_ev, cudaEventDisableTiming), R))
       return LSMGPU_ERR_CUDA;
     for (cudaEvent_t& e : ws->slab_ev)
       if (!cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), R))
         return LSMGPU_ERR_CUDA;
+    for (cudaEvent_t& e : ws->out_ev)
+      if (!cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), R))
+        return LSMGPU_ERR_CUDA;
+    for (cudaEvent_t& e : ws->F_ev)
+      if (!cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), R))
+        return LSMGPU_ERR_CUDA;
   }
-  cudaStream_t cs = ws->copy_stream;
+  // queued calls alternate between the two speed buffers
+  const int fbuf = ws->host_async ? (int)(ws->host_calls & 1u) : 0;
+  if (!ws->dF[fbuf] && !cuda_ok(cudaMalloc(&ws->dF[fbuf], ws->bytes), R)) return LSMGPU_ERR_CUDA;
+  void* dF = ws->dF[fbuf];
+  cudaStream_t ci = ws->copy_stream, co = ws->copy_stream_out;
   const Box& gb = ws->gb;
   const size_t esz = (size_t)ws->prec;
   const size_t plane = (size_t)gb.sz() * esz;
@@ -747,19 +805,29 @@ int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
     s.hi[2] = zlo[q + 1] - 1;
     return s;
   };
-  auto copy = [&](void* dst, const void* src, int q, cudaMemcpyKind kind) {
+  auto copy = [&](void* dst, const void* src, int q, cudaMemcpyKind kind, cudaStream_t cs) {
     const size_t off = (size_t)(zb[q] - gb.lo[2]) * plane;
     return cudaMemcpyAsync((char*)dst + off, (const char*)src + off,
                            (size_t)(zb[q + 1] - zb[q]) * plane, kind, cs);
   };
-  // host -> device, slab by slab, after the work already queued on st
-  if (!cuda_ok(cudaEventRecord(ws->slab_ev[0], st), R) ||
-      !cuda_ok(cudaStreamWaitEvent(cs, ws->slab_ev[0], 0), R))
+  // host -> device.  After a waited-for call: behind all the work queued on
+  // st.  Behind a queued call: the speed behind the last kernels that read
+  // this buffer (two calls back), each phi slab behind that call's copy of
+  // the slab back to the host (which followed every kernel writing it).
+  const bool pending = ws->host_pending != 0;
+  if (!pending) {
+    if (!cuda_ok(cudaEventRecord(ws->start_ev, st), R) ||
+        !cuda_ok(cudaStreamWaitEvent(ci, ws->start_ev, 0), R))
+      return LSMGPU_ERR_CUDA;
+  } else if (ws->host_calls >= 2 && !cuda_ok(cudaStreamWaitEvent(ci, ws->F_ev[fbuf], 0), R)) {
     return LSMGPU_ERR_CUDA;
+  }
+  for (int q = 0; q < ns; q++)
+    if (!cuda_ok(copy(dF, F, q, cudaMemcpyHostToDevice, ci), R)) return LSMGPU_ERR_CUDA;
   for (int q = 0; q < ns; q++) {
-    if (!cuda_ok(copy(ws->dphi, phi, q, cudaMemcpyHostToDevice), R) ||
-        !cuda_ok(copy(ws->dF, F, q, cudaMemcpyHostToDevice), R) ||
-        !cuda_ok(cudaEventRecord(ws->slab_ev[q], cs), R))
+    if ((pending && !cuda_ok(cudaStreamWaitEvent(ci, ws->out_ev[q], 0), R)) ||
+        !cuda_ok(copy(ws->dphi, phi, q, cudaMemcpyHostToDevice, ci), R) ||
+        !cuda_ok(cudaEventRecord(ws->slab_ev[q], ci), R))
       return LSMGPU_ERR_CUDA;
   }
   const double tiny = ws->prec == 8 ? Consts<double>::tiny : (double)Consts<float>::tiny;
@@ -768,7 +836,7 @@ int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
   bool copied_back = false;
   for (int s = 0; s < nsteps; s++) {
     StageArgs a = base_args(ws, f, dx);
-    a.aux[0] = ws->dF;
+    a.aux[0] = dF;
     a.rhs_out = ws->rhs;
     a.phi_s = dphi;
     if (s == 0) {
@@ -805,8 +873,9 @@ int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
         b.fb = slab_fb(q);
         if (!cuda_ok(stage(kStageNormal, ws->prec, b, st, ws), R) ||
             !cuda_ok(cudaEventRecord(ws->slab_ev[kHostSlabs + q], st), R) ||
-            !cuda_ok(cudaStreamWaitEvent(cs, ws->slab_ev[kHostSlabs + q], 0), R) ||
-            !cuda_ok(copy(phi, dphi, q, cudaMemcpyDeviceToHost), R))
+            !cuda_ok(cudaStreamWaitEvent(co, ws->slab_ev[kHostSlabs + q], 0), R) ||
+            !cuda_ok(copy(phi, dphi, q, cudaMemcpyDeviceToHost, co), R) ||
+            !cuda_ok(cudaEventRecord(ws->out_ev[q], co), R))
           return LSMGPU_ERR_CUDA;
       }
       copied_back = true;
@@ -819,14 +888,24 @@ int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
     if (reinit_now && !reinit_run(ws, dphi, f, dx, cfl, reinit_iters, use_phi0_for_sgn, st, R))
       return lsmgpu_peek_last_error();
   }
+  if (!cuda_ok(cudaEventRecord(ws->F_ev[fbuf], st), R)) return LSMGPU_ERR_CUDA;
   if (!copied_back) {
     if (!cuda_ok(cudaEventRecord(ws->slab_ev[kHostSlabs], st), R) ||
-        !cuda_ok(cudaStreamWaitEvent(cs, ws->slab_ev[kHostSlabs], 0), R))
+        !cuda_ok(cudaStreamWaitEvent(co, ws->slab_ev[kHostSlabs], 0), R))
       return LSMGPU_ERR_CUDA;
     for (int q = 0; q < ns; q++)
-      if (!cuda_ok(copy(phi, dphi, q, cudaMemcpyDeviceToHost), R)) return LSMGPU_ERR_CUDA;
+      if (!cuda_ok(copy(phi, dphi, q, cudaMemcpyDeviceToHost, co), R) ||
+          !cuda_ok(cudaEventRecord(ws->out_ev[q], co), R))
+        return LSMGPU_ERR_CUDA;
   }
-  if (!cuda_ok(cudaGetLastError(), R) || !cuda_ok(cudaStreamSynchronize(cs), R) ||
+  ws->host_calls++;
+  if (!cuda_ok(cudaGetLastError(), R)) return LSMGPU_ERR_CUDA;
+  if (ws->host_async) {
+    ws->host_pending = 1;
+    return LSMGPU_SUCCESS;
+  }
+  ws->host_pending = 0;
+  if (!cuda_ok(cudaStreamSynchronize(co), R) || !cuda_ok(cudaStreamSynchronize(ci), R) ||
       !cuda_ok(cudaStreamSynchronize(st), R))
     return LSMGPU_ERR_CUDA;
   return LSMGPU_SUCCESS;

@@ -15,6 +15,8 @@ SIGNATURES = {
     "lsmgpu_workspace_create": (I, [ctypes.POINTER(P), IA, I]),
     "lsmgpu_workspace_destroy": (I, [P]),
     "lsmgpu_workspace_set_bc": (I, [P, U]),
+    "lsmgpu_workspace_set_host_async": (I, [P, I]),
+    "lsmgpu_workspace_sync": (I, [P]),
     "lsmgpu_workspace_set_fp64_policy": (I, [P, I]),
     "lsmgpu_workspace_set_time": (I, [P, D]),
     "lsmgpu_workspace_get_time": (I, [P, DA, DA]),

@@ -59,6 +59,15 @@ class Workspace:
     def set_bc(self, mask):
         gpu.check_rc(gpu.load().lsmgpu_workspace_set_bc(self.h, int(mask)), "set_bc")
 
+    def set_host_async(self, on):
+        """Queue normal_host calls instead of waiting for each (see
+        lsmgpu_workspace_set_host_async); sync() waits for them."""
+        gpu.check_rc(gpu.load().lsmgpu_workspace_set_host_async(self.h, int(bool(on))),
+                     "set_host_async")
+
+    def sync(self):
+        gpu.check_rc(gpu.load().lsmgpu_workspace_sync(self.h), "workspace_sync")
+
     def set_fp64_policy(self, policy):
         """FP32 workspaces: FP64_KINKS | FP64_SIGN | STOCH_ROUND."""
         gpu.check_rc(gpu.load().lsmgpu_workspace_set_fp64_policy(self.h, int(policy)),

@@ -130,6 +130,42 @@ def test_normal_velocity_with_reinitialization(mode, n):
     check(mode, g.interior(g.field(d.download())), g.interior(ref))
 
 
+def test_config2_fast_mode_at_128_cubed():
+    """The benchmark's workload (6 seeded spheres, F = 1 + 0.2 sin sin sin,
+    CFL 0.5) at 128^3 in the benchmark's arithmetic (fast mode): 3 steps, then
+    2 reinitialization pseudo-steps, against the oracle's chain of the
+    reference's routines in the reference integrators' order
+    (LevelSetFunctionIntegrator.cc:1319-1510, ReinitializationAlgorithm.cc:
+    177-330), run over z-slab patches on the host cores."""
+    import os
+
+    from lsmlib_b200 import gpu, integrator, workloads
+    from oracle.driver import PatchedNormalStepper
+    cfg = workloads.config2(128)
+    gb, fb = workloads.boxes(cfg["n"])
+    prev = integrator.get_fp_mode()
+    integrator.set_fp_mode(integrator.FP_FAST)
+    try:
+        ws = integrator.Workspace(gb, 8)
+        d = gpu.DeviceArray.from_host(cfg["phi"])
+        dF = gpu.DeviceArray.from_host(cfg["F"])
+        ws.normal(d, dF, fb, cfg["dx"], cfl=0.5, nsteps=3, reinit_interval=10 ** 9,
+                  reinit_iters=0, use_phi0=0)
+        ws.reinit(d, fb, cfg["dx"], cfl=0.5, iters=2, use_phi0=0)
+        got = d.download()
+    finally:
+        integrator.set_fp_mode(prev)
+    g = Grid(cfg["n"], dx=cfg["dx"])
+    phi = g.field(cfg["phi"])
+    ps = PatchedNormalStepper(oracle.oracle_toolbox(), g, os.cpu_count() or 1)
+    parts, Fs = ps.scatter(phi), ps.scatter(g.field(cfg["F"]))
+    for _ in range(3):
+        ps.normal_step(parts, Fs, 0.5)
+    ps.reinit(parts, 0.5, 2, 0)
+    ps.gather(parts, phi)
+    assert rel_err(g.interior(g.field(got)), g.interior(phi)) <= REL_FAST
+
+
 @pytest.mark.parametrize("use0", [0, 1])
 def test_reinitialization(mode, use0):
     from lsmlib_b200 import gpu, integrator
@@ -330,3 +366,49 @@ def test_normal_host_buffers_match_device_driver(mode, n, steps, interval):
     assert same_bits(host, d.download())
     ws.close()
     ws2.close()
+
+
+def test_queued_host_calls_match_device_driver(mode):
+    """lsmgpu_workspace_set_host_async(ws, 1): one-step host calls queued back
+    to back on pinned phi and F (each call's slabs copied in behind the
+    previous call's copies back, the speed in alternating device buffers),
+    a reinitialization every other step, then lsmgpu_workspace_sync: the
+    device driver's values bit for bit."""
+    import ctypes
+
+    from lsmlib_b200 import gpu, integrator
+    n = (48, 40, 70)
+    g = Grid(n, dx=(2.0 / n[0],) * 3)
+    x_lo = (-1.0, -1.0, -1.0)
+    phi0 = np.asfortranarray(spheres(g, x_lo, seed=9))
+    x, y, z = g.centers(x_lo)
+    F = np.asfortranarray(1.0 + 0.2 * np.sin(4 * np.pi * x) * np.sin(4 * np.pi * y) *
+                          np.sin(4 * np.pi * z))
+    steps = 5
+    ws = integrator.Workspace(g.gb, 8)
+    d = gpu.DeviceArray.from_host(phi0)
+    dF = gpu.DeviceArray.from_host(F)
+    ws.normal(d, dF, g.fb, g.dx, cfl=0.5, nsteps=steps, reinit_interval=2, reinit_iters=2)
+    want = d.download()
+    lib = gpu.load()
+    hp_addr = lib.lsmgpu_host_alloc(phi0.nbytes)
+    hf_addr = lib.lsmgpu_host_alloc(F.nbytes)
+    try:
+        count = phi0.size
+        hp = np.ctypeslib.as_array((ctypes.c_double * count).from_address(hp_addr))
+        hf = np.ctypeslib.as_array((ctypes.c_double * count).from_address(hf_addr))
+        hp[:] = phi0.ravel(order="F")
+        hf[:] = F.ravel(order="F")
+        ws2 = integrator.Workspace(g.gb, 8)
+        ws2.set_host_async(True)
+        for s in range(steps):
+            ws2.normal_host(hp_addr, hf_addr, g.fb, g.dx, cfl=0.5, nsteps=1, step0=s,
+                            reinit_interval=2, reinit_iters=2)
+        ws2.sync()
+        got = hp.reshape(phi0.shape, order="F").copy(order="F")
+        assert same_bits(got, want)
+        ws2.close()
+    finally:
+        lib.lsmgpu_host_free(hp_addr)
+        lib.lsmgpu_host_free(hf_addr)
+    ws.close()
