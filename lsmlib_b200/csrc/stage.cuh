@@ -751,7 +751,9 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
     if (hy1) ny1 = ld(i1, hj, k);
   };
 
-  T w0[7], w1[7];
+  // (a cell outside the fill box keeps zeros: the packed FP32 faces read
+  // both windows)
+  T w0[7] = {}, w1[7] = {};
   if (act0) {
 #pragma unroll
     for (int m = 0; m < 6; m++) w0[m + 1] = ld(i0, j, kb - 3 + m);
@@ -813,8 +815,6 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
       const T2 q2 = *reinterpret_cast<const T2*>(&tile[buf][ty + 3][c0 + 6]);
       u[0] = q0.x; u[1] = q0.y; u[2] = q1.x; u[3] = q1.y; u[4] = q2.x; u[5] = q2.y;
       u[6] = tile[buf][ty + 3][c0 + 8];
-      face_pm_t<T, K64>(u, p.inv[0], xp0, xm1);
-      face_pm_t<T, K64>(u + 1, p.inv[0], xp1, xnext);
       // y: both cells' columns, rows j-2 .. j+3
       T ya[6], yb[6];
 #pragma unroll
@@ -824,11 +824,30 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
         yb[m] = q.y;
       }
       T ym0, ym1;
-      face_pm_t<T, K64>(ya, p.inv[1], yp0, ym0);
-      face_pm_t<T, K64>(yb, p.inv[1], yp1, ym1);
+      if constexpr (sizeof(T) == 4 && !K64) {
+        // FP32: the two faces of each axis in one packed evaluation
+        float2 a[6], vp, vm;
+#pragma unroll
+        for (int m = 0; m < 6; m++) a[m] = make_float2(u[m], u[m + 1]);
+        weno5_face2(a, p.inv[0], vp, vm);
+        xp0 = vp.x; xp1 = vp.y; xm1 = vm.x; xnext = vm.y;
+#pragma unroll
+        for (int m = 0; m < 6; m++) a[m] = make_float2(ya[m], yb[m]);
+        weno5_face2(a, p.inv[1], vp, vm);
+        yp0 = vp.x; yp1 = vp.y; ym0 = vm.x; ym1 = vm.y;
+#pragma unroll
+        for (int m = 0; m < 6; m++) a[m] = make_float2(w0[m + 1], w1[m + 1]);
+        weno5_face2(a, p.inv[2], vp, vm);
+        zp0 = vp.x; zp1 = vp.y; znx0 = vm.x; znx1 = vm.y;
+      } else {
+        face_pm_t<T, K64>(u, p.inv[0], xp0, xm1);
+        face_pm_t<T, K64>(u + 1, p.inv[0], xp1, xnext);
+        face_pm_t<T, K64>(ya, p.inv[1], yp0, ym0);
+        face_pm_t<T, K64>(yb, p.inv[1], yp1, ym1);
+        face_pm_t<T, K64>(w0 + 1, p.inv[2], zp0, znx0);
+        if (act1) face_pm_t<T, K64>(w1 + 1, p.inv[2], zp1, znx1);
+      }
       if (ty + 1 < TY) *reinterpret_cast<T2*>(&fy[ty + 1][c0]) = T2{ym0, ym1};
-      face_pm_t<T, K64>(w0 + 1, p.inv[2], zp0, znx0);
-      if (act1) face_pm_t<T, K64>(w1 + 1, p.inv[2], zp1, znx1);
     }
     const T xm_left = __shfl_up_sync(0xffffffffu, xnext, 1, NP);
     if (xtra) {

@@ -275,6 +275,62 @@ __device__ __forceinline__ void weno5_face(const T* u, T inv, T& vp, T& vm) {
   }
 }
 
+// weno5_face<float> for two independent faces at once, one per lane of a
+// float2 (u[m].x and u[m].y: phi(c-2+m) of each face), on the packed FP32x2
+// arithmetic of sm_100 (__ffma2_rn, __fadd2_rn, __fmul2_rn: two IEEE single
+// operations per instruction).  The same formulas as weno5_face with explicit
+// fused multiply-adds; the eps maximum, the power-of-two scaling and the
+// reciprocal seeds stay per lane.
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b, rounded once (b * -1 is exact)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
+
+__device__ __forceinline__ void weno5_face2(const float2* u, float inv, float2& vp, float2& vm) {
+  const float2 V1 = sub2(u[1], u[0]), V2 = sub2(u[2], u[1]), V3 = sub2(u[3], u[2]),
+               V4 = sub2(u[4], u[3]), V5 = sub2(u[5], u[4]);
+  float2 amax;
+  amax.x = vmax(vmax(vmax(fabsf(V1.x), fabsf(V2.x)), vmax(fabsf(V3.x), fabsf(V4.x))), fabsf(V5.x));
+  amax.y = vmax(vmax(vmax(fabsf(V1.y), fabsf(V2.y)), vmax(fabsf(V3.y), fabsf(V4.y))), fabsf(V5.y));
+  const float2 m = mul2(amax, amax);
+  const float2 eps = fma2(f2(1e-6f), m, f2(Consts<float>::tiny));
+  const float2 c13_12 = f2(13.0f / 12.0f), c14 = f2(0.25f);
+  const float2 ta = add2(fma2(f2(-2.0f), V2, V1), V3);
+  const float2 tb = add2(fma2(f2(-2.0f), V3, V2), V4);
+  const float2 tc = add2(fma2(f2(-2.0f), V4, V3), V5);
+  float2 t = fma2(f2(3.0f), V3, fma2(f2(-4.0f), V2, V1));
+  const float2 Sa = fma2(c13_12, mul2(ta, ta), mul2(c14, mul2(t, t)));
+  t = sub2(V2, V4);
+  const float2 Sb = fma2(c13_12, mul2(tb, tb), mul2(c14, mul2(t, t)));
+  t = add2(fma2(f2(-4.0f), V4, mul2(f2(3.0f), V3)), V5);
+  const float2 Sc = fma2(c13_12, mul2(tc, tc), mul2(c14, mul2(t, t)));
+  const float2 sc = make_float2(inv_pow2_of(eps.x), inv_pow2_of(eps.y));
+  const float2 es = mul2(eps, sc);
+  const float2 qa = fma2(Sa, sc, es), qb = fma2(Sb, sc, es), qc = fma2(Sc, sc, es);
+  const float2 Qa = mul2(qa, qa), Qb = mul2(qb, qb), Qc = mul2(qc, qc);
+  const float2 Pbc = mul2(Qb, Qc), Pac = mul2(Qa, Qc), Pab = mul2(Qa, Qb);
+  const float2 A = mul2(Pbc, sub2(ta, tb)), B = mul2(Pab, sub2(tb, tc));
+  const float2 num_m = fma2(f2(2.0f), A, mul2(f2(3.0f), B));
+  const float2 num_p = fma2(f2(2.0f), B, mul2(f2(3.0f), A));
+  const float2 e3 = mul2(f2(5.0f / 6.0f), V3);
+  const float2 p2m = fma2(f2(1.0f / 3.0f), V4, fma2(f2(-1.0f / 6.0f), V2, e3));
+  const float2 p2p = fma2(f2(1.0f / 3.0f), V2, fma2(f2(-1.0f / 6.0f), V4, e3));
+  const float2 sm = fma2(f2(6.0f), Pbc, fma2(f2(36.0f), Pac, mul2(f2(18.0f), Pab)));
+  const float2 sp = fma2(f2(6.0f), Pab, fma2(f2(36.0f), Pac, mul2(f2(18.0f), Pbc)));
+  // reciprocals: per-lane seeds, one packed Newton-Raphson step (rcp_nr)
+  float2 rm, rp;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rm.x) : "f"(sm.x));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rm.y) : "f"(sm.y));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rp.x) : "f"(sp.x));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rp.y) : "f"(sp.y));
+  rm = fma2(rm, fma2(mul2(f2(-1.0f), sm), rm, f2(1.0f)), rm);
+  rp = fma2(rp, fma2(mul2(f2(-1.0f), sp), rp, f2(1.0f)), rp);
+  vm = mul2(fma2(num_m, rm, p2m), f2(inv));
+  vp = mul2(fma2(mul2(f2(-1.0f), num_p), rp, p2p), f2(inv));
+}
+
 static __device__ __noinline__ float2 weno5_face_fp64(float u0, float u1, float u2,
                                                      float u3, float u4, float u5,
                                                      float inv) {
