@@ -102,6 +102,55 @@ k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ ite
   }
 }
 
+// The face ghost cells of every grid of a packed buffer, written as stored
+// values before a stage (the kinds of fetch_bc, through face_ghost_value), so
+// that the stage reads them from memory: with grids of 32-128 cells per axis
+// nearly every tile touches a face, and generating them on the fly put the
+// boundary branch in nearly every load.  Item (g, k >= 0): the x and y ghost
+// rows of plane k of grid g; item (g, -1 - p): z ghost plane p (side * 3 +
+// layer).  Every value depends on domain cells only.
+template <typename T>
+__global__ void __launch_bounds__(128)
+k_batched_ghosts(const GridMeta* __restrict__ grids, const int2* __restrict__ items,
+                 int nitems, T* buf, unsigned m) {
+  for (int q = blockIdx.x; q < nitems; q += gridDim.x) {
+    const int2 it = items[q];
+    const GridMeta& g = grids[it.x];
+    const FillBox dom = g.fb;
+    const Grid3<T> gr = make_grid(buf + g.offset, g.gb);
+    const int nx = dom.n(0), ny = dom.n(1);
+    auto has = [&](int face) {
+      return ((m >> face) | (m >> (8 + face)) | (m >> (16 + face))) & 1u;
+    };
+    if (it.y >= 0) {
+      const int k = dom.lo[2] + it.y;
+      for (int r = threadIdx.x; r < 6 * ny; r += blockDim.x) {
+        const int j = dom.lo[1] + r / 6, face = (r % 6) / 3, dist = r % 3 + 1;
+        if (!has(face)) continue;
+        const int i = face ? dom.hi[0] + dist : dom.lo[0] - dist;
+        int c[3] = {i, j, k};
+        *gr.ptr(i, j, k) = face_ghost_value(gr, dom, m, face, dist, c);
+      }
+      for (int r = threadIdx.x; r < 6 * nx; r += blockDim.x) {
+        const int i = dom.lo[0] + r % nx, face = 2 + (r / nx) / 3, dist = (r / nx) % 3 + 1;
+        if (!has(face)) continue;
+        const int j = face == 3 ? dom.hi[1] + dist : dom.lo[1] - dist;
+        int c[3] = {i, j, k};
+        *gr.ptr(i, j, k) = face_ghost_value(gr, dom, m, face, dist, c);
+      }
+    } else {
+      const int zp = -1 - it.y, face = 4 + zp / 3, dist = zp % 3 + 1;
+      if (!has(face)) continue;
+      const int k = face == 5 ? dom.hi[2] + dist : dom.lo[2] - dist;
+      for (int r = threadIdx.x; r < nx * ny; r += blockDim.x) {
+        const int i = dom.lo[0] + r % nx, j = dom.lo[1] + r / nx;
+        int c[3] = {i, j, k};
+        *gr.ptr(i, j, k) = face_ghost_value(gr, dom, m, face, dist, c);
+      }
+    }
+  }
+}
+
 // the plain alternative: one launch per grid per stage
 template <typename T, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(TX * TY, 2)
@@ -153,6 +202,11 @@ struct lsmgpu_batch {
   void* phi2 = nullptr;
   int4* d_items[kNumShapes] = {nullptr};
   int nitems[kNumShapes] = {0};
+  // ghost-fill items (see k_batched_ghosts); ghosts_stored: every grid has
+  // at least 3 cells per axis, so the ghosts are written before each stage
+  int2* d_ghost_items = nullptr;
+  int n_ghost_items = 0;
+  bool ghosts_stored = false;
   unsigned* d_counter = nullptr;    // three tile counters (one per stage), step
   int shape = 1;
   int policy = kStochRound;         // FP32: kFp64Kinks | kStochRound
@@ -180,19 +234,28 @@ cudaError_t launch_shape(lsmgpu_batch* b, int shape, bool batched, int rk_kind,
                          T* out, const T* in, const T* base, unsigned* counter,
                          cudaStream_t st) {
   const int grid = b->num_sms * b->blocks_per_sm;
+  // with stored ghosts the stage reads every ghost cell from memory
+  unsigned bcm = b->bc_mask;
+  if (b->ghosts_stored) {
+    const int gblocks = std::min(b->n_ghost_items, b->num_sms * 8);
+    k_batched_ghosts<T><<<gblocks, 128, 0, st>>>(b->d_meta, b->d_ghost_items,
+                                                b->n_ghost_items, (T*)in, b->bc_mask);
+    ++launch_counter();
+    bcm = 0u;
+  }
 #define BATCH_CASE(I, TX, TY, TZ)                                                  \
   case I:                                                                          \
     if (batched) {                                                                 \
       k_batched_stage<T, TX, TY, TZ><<<grid, dim3(TX, TY), 0, st>>>(               \
           b->d_meta, b->d_items[I], b->nitems[I], counter, out, in, base, rk_kind, \
-          b->policy, b->d_counter + 3, b->bc_mask);                                \
+          b->policy, b->d_counter + 3, bcm);                                       \
     } else {                                                                       \
       for (int gi = 0; gi < b->ngrids; gi++) {                                     \
         const FillBox& f = b->meta[gi].fb;                                         \
         dim3 g((f.n(0) + TX - 1) / TX, (f.n(1) + TY - 1) / TY, (f.n(2) + TZ - 1) / TZ); \
         k_grid_stage<T, TX, TY, TZ><<<g, dim3(TX, TY), 0, st>>>(                   \
             b->d_meta, gi, out, in, base, rk_kind, b->policy, b->d_counter + 3,    \
-            b->bc_mask);                                                           \
+            bcm);                                                                  \
       }                                                                            \
     }                                                                              \
     break;
@@ -339,6 +402,22 @@ int lsmgpu_batch_create(lsmgpu_batch** out, int ngrids, const int* n,
          cudaMemcpy(b->d_items[s], sorted.data(), sizeof(int4) * sorted.size(),
                     cudaMemcpyHostToDevice) == cudaSuccess;
   }
+  // ghost-fill items: every plane of every grid, and its 6 z ghost planes
+  b->ghosts_stored = true;
+  for (int g = 0; g < ngrids; g++)
+    for (int d = 0; d < 3; d++)
+      if (b->meta[g].fb.n(d) < 3) b->ghosts_stored = false;
+  if (ok && b->ghosts_stored) {
+    std::vector<int2> gi;
+    for (int g = 0; g < ngrids; g++) {
+      for (int k = 0; k < b->meta[g].fb.n(2); k++) gi.push_back(make_int2(g, k));
+      for (int zp = 0; zp < 6; zp++) gi.push_back(make_int2(g, -1 - zp));
+    }
+    b->n_ghost_items = (int)gi.size();
+    ok = cudaMalloc((void**)&b->d_ghost_items, sizeof(int2) * gi.size()) == cudaSuccess &&
+         cudaMemcpy(b->d_ghost_items, gi.data(), sizeof(int2) * gi.size(),
+                    cudaMemcpyHostToDevice) == cudaSuccess;
+  }
   ok = ok && cudaMemset(b->phi, 0, bytes) == cudaSuccess &&
        cudaMemset(b->phi1, 0, bytes) == cudaSuccess &&
        cudaMemset(b->phi2, 0, bytes) == cudaSuccess &&
@@ -358,7 +437,7 @@ int lsmgpu_batch_create(lsmgpu_batch** out, int ngrids, const int* n,
 int lsmgpu_batch_destroy(lsmgpu_batch* b) {
   if (!b) return LSMGPU_SUCCESS;
   drop_graph(b);
-  void* ps[] = {b->phi, b->phi1, b->phi2, b->d_meta, b->d_counter};
+  void* ps[] = {b->phi, b->phi1, b->phi2, b->d_meta, b->d_counter, b->d_ghost_items};
   for (void* p : ps)
     if (p) cudaFree(p);
   for (int s = 0; s < kNumShapes; s++)
