@@ -1107,6 +1107,22 @@ def run_reference(args, world, rank, budget_s=90.0):
     }
 
 
+def profile_batched(ngrids=64):
+    """Two steps of a batch of the config-4 generator's first `ngrids` grids
+    (FP64, periodic boundaries, the shape the autotuner picks for the full
+    batch: 16x8x32), launched directly (no graph), for an ncu capture of
+    k_batched_stage and k_batched_ghosts."""
+    from lsmlib_b200 import batched, gpu, workloads
+    cfg = workloads.config4(ngrids=ngrids)
+    b = batched.Batch(cfg["sizes"], cfg["dx"], 8)
+    b.upload(workloads.config4_phi(cfg, np.float64))
+    b.set_velocity(cfg["vel"], cfg["cfl"])
+    b.set_bc(batched.BC_PERIODIC)
+    b.set_tile(4)
+    b.advect(2, mode=batched.MODE_PERSISTENT)
+    gpu.check_rc(gpu.load().lsmgpu_stream_synchronize(), "sync")
+
+
 def profile_kernels():
     """Two launches each of the normal-velocity and reinitialization stage
     kernels (TVD-RK3 stage 2, distinct phi_s and phi^n, ghost cells read as
@@ -1187,6 +1203,8 @@ def main():
     ap.add_argument("--config3-full", action="store_true",
                     help="run the config-3 full reversal at 512^3 (minutes) instead of 256^3")
     ap.add_argument("--size", type=int, default=256, help="interior cells per axis")
+    ap.add_argument("--profile-batched", action="store_true",
+                    help="only two steps of a 64-grid batch (for ncu captures) and exit")
     ap.add_argument("--profile-adjoint", action="store_true",
                     help="only run the config-5 forward and reverse sweep twice "
                          "(for ncu captures) and exit")
@@ -1207,6 +1225,9 @@ def main():
         return
     if args.profile_adjoint:
         profile_adjoint()
+        return
+    if args.profile_batched:
+        profile_batched()
         return
     if args.profile_distance:
         profile_distance()

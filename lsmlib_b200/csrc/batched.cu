@@ -59,8 +59,15 @@ __device__ __forceinline__ unsigned batch_sr_seed(int policy, const unsigned* sr
 
 __global__ void k_bump(unsigned* c) { *c += 1u; }
 
+// register budget: 24 warps per SM, as the single-grid stage kernels (the
+// earlier budget of 2 blocks let the compiler take 190 registers and left
+// the SMs at 8 warps: ncu, 12 % warps active, 45 % issue)
+#ifndef LSMGPU_BATCH_WARPS
+#define LSMGPU_BATCH_WARPS 24
+#endif
+
 template <typename T, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX * TY, 2)
+__global__ void __launch_bounds__(TX * TY, LSMGPU_BATCH_WARPS * 32 / (TX * TY))
 k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ items,
                 int nitems, unsigned* counter, T* out, const T* phi_s,
                 const T* phi_n, int rk_kind, int policy, const unsigned* sr_step,
@@ -153,7 +160,7 @@ k_batched_ghosts(const GridMeta* __restrict__ grids, const int2* __restrict__ it
 
 // the plain alternative: one launch per grid per stage
 template <typename T, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(TX * TY, 2)
+__global__ void __launch_bounds__(TX * TY, LSMGPU_BATCH_WARPS * 32 / (TX * TY))
 k_grid_stage(const GridMeta* __restrict__ grids, int gi, T* out, const T* phi_s,
              const T* phi_n, int rk_kind, int policy, const unsigned* sr_step,
              unsigned bc_mask) {
@@ -212,6 +219,7 @@ struct lsmgpu_batch {
   int policy = kStochRound;         // FP32: kFp64Kinks | kStochRound
   unsigned bc_mask = kBcLinear;
   int blocks_per_sm = 2;
+  int resident[kNumShapes] = {0};   // blocks per SM of each shape's kernel
   int num_sms = 148;
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
@@ -233,7 +241,27 @@ template <typename T>
 cudaError_t launch_shape(lsmgpu_batch* b, int shape, bool batched, int rk_kind,
                          T* out, const T* in, const T* base, unsigned* counter,
                          cudaStream_t st) {
-  const int grid = b->num_sms * b->blocks_per_sm;
+  // persistent grid: every SM filled with as many blocks of the shape as fit
+  int per_sm = b->blocks_per_sm;
+  if (b->resident[shape] == 0) {
+    const void* fn = nullptr;
+    switch (shape) {
+      case 0: fn = (const void*)k_batched_stage<T, 32, 8, 16>; break;
+      case 1: fn = (const void*)k_batched_stage<T, 32, 8, 32>; break;
+      case 2: fn = (const void*)k_batched_stage<T, 32, 8, 64>; break;
+      case 3: fn = (const void*)k_batched_stage<T, 16, 8, 16>; break;
+      default: fn = (const void*)k_batched_stage<T, 16, 8, 32>; break;
+    }
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kShapes[shape].tx * kShapes[shape].ty,
+                                                      0) != cudaSuccess || nb < 1) {
+      cudaGetLastError();
+      nb = b->blocks_per_sm;
+    }
+    b->resident[shape] = nb;
+  }
+  per_sm = b->resident[shape];
+  const int grid = b->num_sms * per_sm;
   // with stored ghosts the stage reads every ghost cell from memory
   unsigned bcm = b->bc_mask;
   if (b->ghosts_stored) {
