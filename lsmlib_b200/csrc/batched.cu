@@ -41,11 +41,15 @@ struct GridMeta {
   double vel[3];
 };
 
-// tile shapes the autotuner chooses from
+// tile shapes the autotuner chooses from, each with two halo-staging
+// schedules (stage_tile's STAGING: shared plane, direct loads): configuration
+// c is shape c % kNumShapes with schedule c / kNumShapes
 struct TileShape { int tx, ty, tz; };
 constexpr TileShape kShapes[] = {{32, 8, 16}, {32, 8, 32}, {32, 8, 64}, {16, 8, 16},
                                  {16, 8, 32}};
 constexpr int kNumShapes = 5;
+constexpr int kNumStagings = 2;
+constexpr int kNumConfigs = kNumShapes * kNumStagings;
 
 // seed of the stochastic rounding of one stage: the step number kept on the
 // device (bumped at the end of every step, so that graph replays differ)
@@ -66,7 +70,7 @@ __global__ void k_bump(unsigned* c) { *c += 1u; }
 #define LSMGPU_BATCH_WARPS 24
 #endif
 
-template <typename T, int TX, int TY, int TZ>
+template <typename T, int TX, int TY, int TZ, int STAGING>
 __global__ void __launch_bounds__(TX * TY, LSMGPU_BATCH_WARPS * 32 / (TX * TY))
 k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ items,
                 int nitems, unsigned* counter, T* out, const T* phi_s,
@@ -105,7 +109,7 @@ k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ ite
     p.use_phi0 = 0;
     p.fp64_policy = policy & kFp64Kinks;
     p.sr_seed = batch_sr_seed<T>(policy, sr_step, rk_kind);
-    stage_tile<T, kStageAdvectConst, true, TX, TY, TZ>(p, it.y, it.z, it.w, tile);
+    stage_tile<T, kStageAdvectConst, true, TX, TY, TZ, STAGING>(p, it.y, it.z, it.w, tile);
   }
 }
 
@@ -159,7 +163,7 @@ k_batched_ghosts(const GridMeta* __restrict__ grids, const int2* __restrict__ it
 }
 
 // the plain alternative: one launch per grid per stage
-template <typename T, int TX, int TY, int TZ>
+template <typename T, int TX, int TY, int TZ, int STAGING>
 __global__ void __launch_bounds__(TX * TY, LSMGPU_BATCH_WARPS * 32 / (TX * TY))
 k_grid_stage(const GridMeta* __restrict__ grids, int gi, T* out, const T* phi_s,
              const T* phi_n, int rk_kind, int policy, const unsigned* sr_step,
@@ -188,8 +192,8 @@ k_grid_stage(const GridMeta* __restrict__ grids, int gi, T* out, const T* phi_s,
   p.use_phi0 = 0;
   p.fp64_policy = policy & kFp64Kinks;
   p.sr_seed = batch_sr_seed<T>(policy, sr_step, rk_kind);
-  stage_tile<T, kStageAdvectConst, true, TX, TY, TZ>(p, (int)blockIdx.x, (int)blockIdx.y,
-                                                     (int)blockIdx.z, tile);
+  stage_tile<T, kStageAdvectConst, true, TX, TY, TZ, STAGING>(
+      p, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, tile);
 }
 
 std::mutex g_tune_mutex;
@@ -219,7 +223,7 @@ struct lsmgpu_batch {
   int policy = kStochRound;         // FP32: kFp64Kinks | kStochRound
   unsigned bc_mask = kBcLinear;
   int blocks_per_sm = 2;
-  int resident[kNumShapes] = {0};   // blocks per SM of each shape's kernel
+  int resident[kNumConfigs] = {0};   // blocks per SM of each configuration's kernel
   int num_sms = 148;
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
@@ -241,16 +245,23 @@ template <typename T>
 cudaError_t launch_shape(lsmgpu_batch* b, int shape, bool batched, int rk_kind,
                          T* out, const T* in, const T* base, unsigned* counter,
                          cudaStream_t st) {
-  // persistent grid: every SM filled with as many blocks of the shape as fit
-  int per_sm = b->blocks_per_sm;
-  if (b->resident[shape] == 0) {
+  // persistent grid: every SM filled with as many blocks of the
+  // configuration as fit
+  const int cfg = shape;
+  shape = cfg % kNumShapes;
+  if (b->resident[cfg] == 0) {
     const void* fn = nullptr;
-    switch (shape) {
-      case 0: fn = (const void*)k_batched_stage<T, 32, 8, 16>; break;
-      case 1: fn = (const void*)k_batched_stage<T, 32, 8, 32>; break;
-      case 2: fn = (const void*)k_batched_stage<T, 32, 8, 64>; break;
-      case 3: fn = (const void*)k_batched_stage<T, 16, 8, 16>; break;
-      default: fn = (const void*)k_batched_stage<T, 16, 8, 32>; break;
+    switch (cfg) {
+      case 0: fn = (const void*)k_batched_stage<T, 32, 8, 16, 0>; break;
+      case 1: fn = (const void*)k_batched_stage<T, 32, 8, 32, 0>; break;
+      case 2: fn = (const void*)k_batched_stage<T, 32, 8, 64, 0>; break;
+      case 3: fn = (const void*)k_batched_stage<T, 16, 8, 16, 0>; break;
+      case 4: fn = (const void*)k_batched_stage<T, 16, 8, 32, 0>; break;
+      case 5: fn = (const void*)k_batched_stage<T, 32, 8, 16, 1>; break;
+      case 6: fn = (const void*)k_batched_stage<T, 32, 8, 32, 1>; break;
+      case 7: fn = (const void*)k_batched_stage<T, 32, 8, 64, 1>; break;
+      case 8: fn = (const void*)k_batched_stage<T, 16, 8, 16, 1>; break;
+      default: fn = (const void*)k_batched_stage<T, 16, 8, 32, 1>; break;
     }
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kShapes[shape].tx * kShapes[shape].ty,
@@ -258,10 +269,9 @@ cudaError_t launch_shape(lsmgpu_batch* b, int shape, bool batched, int rk_kind,
       cudaGetLastError();
       nb = b->blocks_per_sm;
     }
-    b->resident[shape] = nb;
+    b->resident[cfg] = nb;
   }
-  per_sm = b->resident[shape];
-  const int grid = b->num_sms * per_sm;
+  const int grid = b->num_sms * b->resident[cfg];
   // with stored ghosts the stage reads every ghost cell from memory
   unsigned bcm = b->bc_mask;
   if (b->ghosts_stored) {
@@ -271,28 +281,33 @@ cudaError_t launch_shape(lsmgpu_batch* b, int shape, bool batched, int rk_kind,
     ++launch_counter();
     bcm = 0u;
   }
-#define BATCH_CASE(I, TX, TY, TZ)                                                  \
+#define BATCH_CASE(I, TX, TY, TZ, SG)                                              \
   case I:                                                                          \
     if (batched) {                                                                 \
-      k_batched_stage<T, TX, TY, TZ><<<grid, dim3(TX, TY), 0, st>>>(               \
-          b->d_meta, b->d_items[I], b->nitems[I], counter, out, in, base, rk_kind, \
-          b->policy, b->d_counter + 3, bcm);                                       \
+      k_batched_stage<T, TX, TY, TZ, SG><<<grid, dim3(TX, TY), 0, st>>>(           \
+          b->d_meta, b->d_items[I % kNumShapes], b->nitems[I % kNumShapes], counter, \
+          out, in, base, rk_kind, b->policy, b->d_counter + 3, bcm);               \
     } else {                                                                       \
       for (int gi = 0; gi < b->ngrids; gi++) {                                     \
         const FillBox& f = b->meta[gi].fb;                                         \
         dim3 g((f.n(0) + TX - 1) / TX, (f.n(1) + TY - 1) / TY, (f.n(2) + TZ - 1) / TZ); \
-        k_grid_stage<T, TX, TY, TZ><<<g, dim3(TX, TY), 0, st>>>(                   \
+        k_grid_stage<T, TX, TY, TZ, SG><<<g, dim3(TX, TY), 0, st>>>(               \
             b->d_meta, gi, out, in, base, rk_kind, b->policy, b->d_counter + 3,    \
             bcm);                                                                  \
       }                                                                            \
     }                                                                              \
     break;
-  switch (shape) {
-    BATCH_CASE(0, 32, 8, 16)
-    BATCH_CASE(1, 32, 8, 32)
-    BATCH_CASE(2, 32, 8, 64)
-    BATCH_CASE(3, 16, 8, 16)
-    BATCH_CASE(4, 16, 8, 32)
+  switch (cfg) {
+    BATCH_CASE(0, 32, 8, 16, 0)
+    BATCH_CASE(1, 32, 8, 32, 0)
+    BATCH_CASE(2, 32, 8, 64, 0)
+    BATCH_CASE(3, 16, 8, 16, 0)
+    BATCH_CASE(4, 16, 8, 32, 0)
+    BATCH_CASE(5, 32, 8, 16, 1)
+    BATCH_CASE(6, 32, 8, 32, 1)
+    BATCH_CASE(7, 32, 8, 64, 1)
+    BATCH_CASE(8, 16, 8, 16, 1)
+    BATCH_CASE(9, 16, 8, 32, 1)
     default: return cudaErrorInvalidValue;
   }
 #undef BATCH_CASE
@@ -545,9 +560,11 @@ int lsmgpu_batch_get_dt(lsmgpu_batch* b, double* dt) {
   return LSMGPU_SUCCESS;
 }
 
+// configuration: tile shape (shape % 5 of the list above) and halo-staging
+// schedule (shape / 5: 0 shared plane, 1 direct loads)
 int lsmgpu_batch_set_tile(lsmgpu_batch* b, int shape) {
   if (!batch_ok(b, "lsmgpu_batch_set_tile")) return LSMGPU_ERR_NULL_POINTER;
-  if (shape < 0 || shape >= kNumShapes) {
+  if (shape < 0 || shape >= kNumConfigs) {
     set_error(LSMGPU_ERR_INVALID_VALUE, "lsmgpu_batch_set_tile: unknown shape");
     return LSMGPU_ERR_INVALID_VALUE;
   }
@@ -559,9 +576,9 @@ int lsmgpu_batch_get_tile(lsmgpu_batch* b, int* shape, int tile[3]) {
   if (!batch_ok(b, "lsmgpu_batch_get_tile")) return LSMGPU_ERR_NULL_POINTER;
   if (shape) *shape = b->shape;
   if (tile) {
-    tile[0] = kShapes[b->shape].tx;
-    tile[1] = kShapes[b->shape].ty;
-    tile[2] = kShapes[b->shape].tz;
+    tile[0] = kShapes[b->shape % kNumShapes].tx;
+    tile[1] = kShapes[b->shape % kNumShapes].ty;
+    tile[2] = kShapes[b->shape % kNumShapes].tz;
   }
   return LSMGPU_SUCCESS;
 }
@@ -601,7 +618,8 @@ int lsmgpu_batch_set_fp64_policy(lsmgpu_batch* b, int policy) {
 
 // Time one step per tile shape (on a scratch copy of phi, so the batch state
 // is unchanged) and keep the fastest; the choice is cached per (precision,
-// size class).  ms_out[kNumShapes] receives the timings when non-null.
+// size class).  ms_out[10] receives the timings of the ten configurations
+// (tile shape x halo-staging schedule) when non-null.
 int lsmgpu_batch_autotune(lsmgpu_batch* b, float* ms_out) {
   const char* R = "lsmgpu_batch_autotune";
   if (!batch_ok(b, R)) return LSMGPU_ERR_NULL_POINTER;
@@ -620,7 +638,7 @@ int lsmgpu_batch_autotune(lsmgpu_batch* b, float* ms_out) {
   cudaEventCreate(&e1);
   int best = b->shape;
   float best_ms = 1e30f;
-  for (int s = 0; s < kNumShapes; s++) {
+  for (int s = 0; s < kNumConfigs; s++) {
     float ms = 0.f;
     bool ok = step(b, s, true, b->stream) == cudaSuccess;  // warm-up
     ok = ok && cudaEventRecord(e0, b->stream) == cudaSuccess;

@@ -310,7 +310,12 @@ __device__ __forceinline__ T weno_upwind_side(const T* w, T inv, bool plus,
 // read by slower threads of the previous plane.  Returns the tile's largest
 // CFL speed for kStageNormalRhs (-1 otherwise).  The caller synchronises the
 // block before reusing ``tile``.
-template <typename T, int KIND, bool FAST, int TX, int TY, int TZ>
+// STAGING is the halo-staging schedule of the x/y stencils: 0 stages each
+// plane with its 3-cell side strips in shared memory (two barriers per
+// plane); 1 reads the x and y neighbours straight from global memory through
+// L1 (no shared plane, no barrier; neighbouring threads share the cache
+// lines).  The batched autotuner picks one per batch.
+template <typename T, int KIND, bool FAST, int TX, int TY, int TZ, int STAGING = 0>
 __device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
                                              int by, int bz,
                                              T (*tile)[TY + 6][TX + 6]) {
@@ -358,9 +363,9 @@ __device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
   T nx_c = T(0), nx_hx = T(0), nx_hy = T(0);
   auto prefetch = [&](int k) {
     if (act) nx_c = ld(i, j, k + 3);
-    else if (ctr_halo) nx_c = ld(i, j, k);
-    if (has_hx) nx_hx = ld(hx, j, k);
-    if (has_hy) nx_hy = ld(i, hj, k);
+    else if (STAGING == 0 && ctr_halo) nx_c = ld(i, j, k);
+    if (STAGING == 0 && has_hx) nx_hx = ld(hx, j, k);
+    if (STAGING == 0 && has_hy) nx_hy = ld(i, hj, k);
   };
 
   T w[7];
@@ -375,13 +380,15 @@ __device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
 #pragma unroll
       for (int m = 0; m < 6; m++) w[m] = w[m + 1];
       w[6] = nx_c;
-      tile[buf][ty + 3][tx + 3] = w[3];
-    } else if (ctr_halo) {
+      if constexpr (STAGING == 0) tile[buf][ty + 3][tx + 3] = w[3];
+    } else if (STAGING == 0 && ctr_halo) {
       tile[buf][ty + 3][tx + 3] = nx_c;
     }
-    if (has_hx) tile[buf][ty + 3][tcol] = nx_hx;
-    if (has_hy) tile[buf][trow][tx + 3] = nx_hy;
-    __syncthreads();
+    if constexpr (STAGING == 0) {
+      if (has_hx) tile[buf][ty + 3][tcol] = nx_hx;
+      if (has_hy) tile[buf][trow][tx + 3] = nx_hy;
+      __syncthreads();
+    }
     if (k < ke) prefetch(k + 1);
     if (act) {
       const long o = base0 + (long)i + sy * j + sz * k;
@@ -408,10 +415,18 @@ __device__ __forceinline__ double stage_tile(const StageParams<T>& p, int bx,
       }
       if (KIND != kStageNormalRhs && p.rk_kind != 1) uc = __ldg(p.phi_n + o);
       T wx[7], wy[7];
+      if constexpr (STAGING == 0) {
 #pragma unroll
-      for (int m = 0; m < 7; m++) {
-        wx[m] = tile[buf][ty + 3][tx + m];
-        wy[m] = tile[buf][ty + m][tx + 3];
+        for (int m = 0; m < 7; m++) {
+          wx[m] = tile[buf][ty + 3][tx + m];
+          wy[m] = tile[buf][ty + m][tx + 3];
+        }
+      } else {
+#pragma unroll
+        for (int m = 0; m < 7; m++) {
+          wx[m] = m == 3 ? w[3] : ld(i - 3 + m, j, k);
+          wy[m] = m == 3 ? w[3] : ld(i, j - 3 + m, k);
+        }
       }
       const T ztol = stage_zero_tol<T>();
       T L;
