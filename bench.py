@@ -53,9 +53,9 @@ WORKLOAD = ("256^3 normal-velocity level set (6 spheres, F = 1 + 0.2 sin sin sin
 
 # DRAM bytes (read + write) per launch and FP64-pipe utilisation of the fused
 # stage kernels on the 256^3 workload, from the ncu capture summarised in
-# profiles/k_stage_fp64_config2_256.md (distinct phi_s and phi^n)
-NCU_TRAFFIC = {"stage_reinit_rk32": 390.8e6, "stage_normal_rk32": 536.0e6}
-NCU_FP64_PIPE = {"stage_reinit_rk32": 46.8, "stage_normal_rk32": 49.7}
+# profiles/k_stage_pairs_config2_256.md (distinct phi_s and phi^n)
+NCU_TRAFFIC = {"stage_reinit_rk32": 394.6e6, "stage_normal_rk32": 539.3e6}
+NCU_FP64_PIPE = {"stage_reinit_rk32": 63.8, "stage_normal_rk32": 70.5}
 
 def env_int(name, default):
     try:
@@ -365,7 +365,7 @@ def run_ours(args, world, rank, local, pg):
     traffic = NCU_TRAFFIC.get(dom) if N_CELLS == 256 else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                "traffic_source": "ncu capture, profiles/k_stage_fp64_config2_256.md",
+                "traffic_source": "ncu capture, profiles/k_stage_pairs_config2_256.md",
                 "fp64_pipe_active_pct_ncu": NCU_FP64_PIPE.get(dom),
                 "kernel": dom, "kernel_ms": round(kern[dom]["ms"], 4),
                 "algorithmic_bytes_per_launch": kern[dom]["bytes"],

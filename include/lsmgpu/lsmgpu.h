@@ -630,7 +630,8 @@ int lsmgpu_reinit_tvdrk3(lsmgpu_workspace *ws, void *phi, const int fb[6],
  * (grid g's ghost box, interior 0..n-1 per axis with 3 ghost cells, starts at
  * the element offset lsmgpu_batch_grid returns).  Every TVD-RK3 stage is one
  * persistent launch that takes tiles from a work-list; a step is captured in
- * a CUDA graph.  The tile shape is chosen by lsmgpu_batch_autotune. */
+ * a CUDA graph.  The configuration (tile shape and halo-staging schedule)
+ * is chosen by lsmgpu_batch_autotune or set by lsmgpu_batch_set_tile. */
 typedef struct lsmgpu_batch lsmgpu_batch;
 /* n[3*g..3*g+2]: interior cells of grid g; dx[3*g..3*g+2]: its spacing */
 int lsmgpu_batch_create(lsmgpu_batch **b, int ngrids, const int *n,
