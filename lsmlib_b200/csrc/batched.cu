@@ -135,29 +135,32 @@ k_batched_ghosts(const GridMeta* __restrict__ grids, const int2* __restrict__ it
     };
     if (it.y >= 0) {
       const int k = dom.lo[2] + it.y;
-      for (int r = threadIdx.x; r < 6 * ny; r += blockDim.x) {
+      ghost_items<4, T>(threadIdx.x, 6 * ny, blockDim.x, [&](int r, T& v) -> T* {
         const int j = dom.lo[1] + r / 6, face = (r % 6) / 3, dist = r % 3 + 1;
-        if (!has(face)) continue;
+        if (!has(face)) return nullptr;
         const int i = face ? dom.hi[0] + dist : dom.lo[0] - dist;
         int c[3] = {i, j, k};
-        *gr.ptr(i, j, k) = face_ghost_value(gr, dom, m, face, dist, c);
-      }
-      for (int r = threadIdx.x; r < 6 * nx; r += blockDim.x) {
+        v = face_ghost_value(gr, dom, m, face, dist, c);
+        return gr.ptr(i, j, k);
+      });
+      ghost_items<4, T>(threadIdx.x, 6 * nx, blockDim.x, [&](int r, T& v) -> T* {
         const int i = dom.lo[0] + r % nx, face = 2 + (r / nx) / 3, dist = (r / nx) % 3 + 1;
-        if (!has(face)) continue;
+        if (!has(face)) return nullptr;
         const int j = face == 3 ? dom.hi[1] + dist : dom.lo[1] - dist;
         int c[3] = {i, j, k};
-        *gr.ptr(i, j, k) = face_ghost_value(gr, dom, m, face, dist, c);
-      }
+        v = face_ghost_value(gr, dom, m, face, dist, c);
+        return gr.ptr(i, j, k);
+      });
     } else {
       const int zp = -1 - it.y, face = 4 + zp / 3, dist = zp % 3 + 1;
       if (!has(face)) continue;
       const int k = face == 5 ? dom.hi[2] + dist : dom.lo[2] - dist;
-      for (int r = threadIdx.x; r < nx * ny; r += blockDim.x) {
+      ghost_items<4, T>(threadIdx.x, nx * ny, blockDim.x, [&](int r, T& v) -> T* {
         const int i = dom.lo[0] + r % nx, j = dom.lo[1] + r / nx;
         int c[3] = {i, j, k};
-        *gr.ptr(i, j, k) = face_ghost_value(gr, dom, m, face, dist, c);
-      }
+        v = face_ghost_value(gr, dom, m, face, dist, c);
+        return gr.ptr(i, j, k);
+      });
     }
   }
 }

@@ -980,9 +980,13 @@ k_stage_pairs(StageParams<T> p) {
 // reach them.  Each value depends on cells of the domain box only (no edge
 // or corner ghost is read or written), so the threads are independent; the
 // launcher requires at least 3 domain cells along every axis with a bit set.
-// Block b < k1-k0+1 writes the x and y ghosts of plane k0+b (the 6 cells of
-// a row's two ends together, then the 6 rows of the y faces along x); the
-// remaining blocks write the z ghost planes, zchunks blocks per plane.
+// One item per thread, so that every load of the launch is in flight at once
+// (a version that looped a block over a plane's items waited on each
+// iteration's loads in turn): per plane k0..k1, face_ghost_xy_blocks(nx, ny)
+// blocks -- the x ghosts (the 6 cells of a row's two ends together, item
+// 6 j + side * 3 + layer), then the y ghosts (6 rows along x, item
+// nx (side * 3 + layer) + i) -- and after them zchunks blocks for each of
+// the 6 z ghost planes.
 template <typename T>
 __device__ __forceinline__ T face_ghost_value(const Grid3<T>& g, const FillBox& dom,
                                               unsigned m, int face, int dist, int c[3]) {
@@ -1001,50 +1005,87 @@ __device__ __forceinline__ T face_ghost_value(const Grid3<T>& g, const FillBox& 
   return e0 + slope * (T)dist;
 }
 
+constexpr int kFaceGhostThreads = 256;
+
+// item(r, v) for r = first, first + stride, ... below end, U items at a time
+// with the loads of all U issued before any of their stores (the ghost
+// fills are bound by load latency).  item returns the cell to write
+// (nullptr: none) and sets v.
+template <int U, typename T, typename F>
+__device__ __forceinline__ void ghost_items(int first, int end, int stride, F item) {
+  for (int r0 = first; r0 < end; r0 += U * stride) {
+    T v[U];
+    T* d[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int r = r0 + u * stride;
+      d[u] = r < end ? item(r, v[u]) : nullptr;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (d[u]) *d[u] = v[u];
+  }
+}
+
+// blocks per plane for the x and y ghosts (one item per thread)
+__host__ __device__ inline int face_ghost_xy_blocks(int nx, int ny, int* bx = nullptr) {
+  const int x = (6 * ny + kFaceGhostThreads - 1) / kFaceGhostThreads;
+  if (bx) *bx = x;
+  return x + (6 * nx + kFaceGhostThreads - 1) / kFaceGhostThreads;
+}
+
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kFaceGhostThreads)
 k_face_ghosts(T* phi, Box gb, FillBox dom, unsigned m, int k0, int k1, int zchunks) {
   const int nx = dom.n(0), ny = dom.n(1);
   const int np = k1 - k0 + 1;
+  int bx;
+  const int bxy = face_ghost_xy_blocks(nx, ny, &bx);
   const Grid3<T> g = make_grid(phi, gb);
   const unsigned any_face[6] = {m & 0x10101u, m & 0x20202u, m & 0x40404u,
                                 m & 0x80808u, m & 0x101010u, m & 0x202020u};
   const int b = (int)blockIdx.x;
-  if (b < np) {
-    const int k = k0 + b;
-    // x faces: item q = 6 j + r, r = side * 3 + layer
-    for (int q = threadIdx.x; q < 6 * ny; q += blockDim.x) {
-      const int j = dom.lo[1] + q / 6, r = q % 6;
-      const int face = r / 3, dist = r % 3 + 1;
-      if (!any_face[face]) continue;
-      const int i = face ? dom.hi[0] + dist : dom.lo[0] - dist;
-      int c[3] = {i, j, k};
-      *g.ptr(i, j, k) = face_ghost_value(g, dom, m, face, dist, c);
+  if (b < np * bxy) {
+    const int k = k0 + b / bxy, sub = b % bxy;
+    int face, dist, i, j;
+    if (sub < bx) {
+      const int q = sub * kFaceGhostThreads + (int)threadIdx.x;
+      if (q >= 6 * ny) return;
+      const int r = q % 6;
+      j = dom.lo[1] + q / 6;
+      face = r / 3;
+      dist = r % 3 + 1;
+      i = face ? dom.hi[0] + dist : dom.lo[0] - dist;
+    } else {
+      const int q = (sub - bx) * kFaceGhostThreads + (int)threadIdx.x;
+      if (q >= 6 * nx) return;
+      const int r = q / nx;
+      i = dom.lo[0] + q % nx;
+      face = 2 + r / 3;
+      dist = r % 3 + 1;
+      j = face == 3 ? dom.hi[1] + dist : dom.lo[1] - dist;
     }
-    // y faces: item q = nx r + (i - lo), r = side * 3 + layer
-    for (int q = threadIdx.x; q < 6 * nx; q += blockDim.x) {
-      const int i = dom.lo[0] + q % nx, r = q / nx;
-      const int face = 2 + r / 3, dist = r % 3 + 1;
-      if (!any_face[face]) continue;
-      const int j = face == 3 ? dom.hi[1] + dist : dom.lo[1] - dist;
-      int c[3] = {i, j, k};
-      *g.ptr(i, j, k) = face_ghost_value(g, dom, m, face, dist, c);
-    }
+    if (!any_face[face]) return;
+    int c[3] = {i, j, k};
+    *g.ptr(i, j, k) = face_ghost_value(g, dom, m, face, dist, c);
     return;
   }
   // z ghost planes: plane zp = side * 3 + layer, chunk of its nx * ny cells
-  const int zp = (b - np) / zchunks, chunk = (b - np) % zchunks;
+  const int zb = b - np * bxy;
+  const int zp = zb / zchunks, chunk = zb % zchunks;
   const int face = 4 + zp / 3, dist = zp % 3 + 1;
   if (!any_face[face]) return;
   if (face == 4 ? k0 - 3 >= dom.lo[2] : k1 + 3 <= dom.hi[2]) return;   // not reached
   const int k = face == 5 ? dom.hi[2] + dist : dom.lo[2] - dist;
   const int cells = nx * ny, per = (cells + zchunks - 1) / zchunks;
   const int end = min(cells, (chunk + 1) * per);
-  for (int q = chunk * per + threadIdx.x; q < end; q += blockDim.x) {
-    const int i = dom.lo[0] + q % nx, j = dom.lo[1] + q / nx;
-    int c[3] = {i, j, k};
-    *g.ptr(i, j, k) = face_ghost_value(g, dom, m, face, dist, c);
-  }
+  ghost_items<4, T>(chunk * per + (int)threadIdx.x, end, kFaceGhostThreads,
+                    [&](int q, T& v) -> T* {
+                      const int i = dom.lo[0] + q % nx, j = dom.lo[1] + q / nx;
+                      int c[3] = {i, j, k};
+                      v = face_ghost_value(g, dom, m, face, dist, c);
+                      return g.ptr(i, j, k);
+                    });
 }
 
 }  // namespace lsmgpu

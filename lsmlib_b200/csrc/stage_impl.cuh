@@ -71,9 +71,13 @@ void launch_kind(dim3 grid, const StageArgs& a, const StageParams<T>& p, cudaStr
       StageParams<T> q = p;
       if (a.bc_mask != 0u) {
         // the planes of the fill box, and the z faces its stencils reach
+        // (about 4 cells per thread of a z ghost plane)
         const int zchunks = (int)std::min<long>(
-            64, ((long)a.dom.n(0) * a.dom.n(1) + 2047) / 2048);
-        k_face_ghosts<T><<<a.fb.n(2) + 6 * zchunks, 256, 0, st>>>(
+            4096, ((long)a.dom.n(0) * a.dom.n(1) + 4 * kFaceGhostThreads - 1) /
+                      (4 * kFaceGhostThreads));
+        const long blocks =
+            (long)a.fb.n(2) * face_ghost_xy_blocks(a.dom.n(0), a.dom.n(1)) + 6L * zchunks;
+        k_face_ghosts<T><<<(unsigned)blocks, kFaceGhostThreads, 0, st>>>(
             (T*)a.phi_s, a.gb, a.dom, a.bc_mask, a.fb.lo[2], a.fb.hi[2], zchunks);
         ++launch_counter();
         q.bc_mask = 0u;
