@@ -544,12 +544,15 @@ def compact_distance(r):
             "bit_exact_all_checked": all(exact) if exact else None}
 
 
-def run_adjoint(n_fd=20, h=1e-6):
+def run_adjoint(n_fd=20, h=2e-5):
     """Config 5: 128^3, B-spline velocity (8^3 x 3 coefficients), 200 steps,
     checkpoints every 15 steps.  Times the forward run (with its
     checkpoints) and the reverse sweep (segment recomputation included), and
     checks dJ/dtheta against central finite differences of the GPU forward
-    model on n_fd seeded coefficients."""
+    model on n_fd seeded coefficients.  The forward map is smooth only
+    piecewise (upwind side, eps argmax and the kinks of H_eps''), so the
+    difference quotients scatter at the 1e-6 level below h ~ 1e-5 and grow
+    as O(h^2) above it; h = 2e-5 sits between the two."""
     from lsmlib_b200 import adjoint, workloads
     cfg = workloads.config5()
     p = adjoint.AdvectionAdjoint(cfg["n"], cfg["dx"], cfg["x_lo"], cfg["lattice"],

@@ -139,17 +139,17 @@ k_batched_ghosts(const GridMeta* __restrict__ grids, const int2* __restrict__ it
         const int j = dom.lo[1] + r / 6, face = (r % 6) / 3, dist = r % 3 + 1;
         if (!has(face)) return nullptr;
         const int i = face ? dom.hi[0] + dist : dom.lo[0] - dist;
-        int c[3] = {i, j, k};
-        v = face_ghost_value(gr, dom, m, face, dist, c);
-        return gr.ptr(i, j, k);
+        T* const cell = gr.ptr(i, j, k);
+        v = face_ghost_value(gr, dom, m, face, dist, cell);
+        return cell;
       });
       ghost_items<4, T>(threadIdx.x, 6 * nx, blockDim.x, [&](int r, T& v) -> T* {
         const int i = dom.lo[0] + r % nx, face = 2 + (r / nx) / 3, dist = (r / nx) % 3 + 1;
         if (!has(face)) return nullptr;
         const int j = face == 3 ? dom.hi[1] + dist : dom.lo[1] - dist;
-        int c[3] = {i, j, k};
-        v = face_ghost_value(gr, dom, m, face, dist, c);
-        return gr.ptr(i, j, k);
+        T* const cell = gr.ptr(i, j, k);
+        v = face_ghost_value(gr, dom, m, face, dist, cell);
+        return cell;
       });
     } else {
       const int zp = -1 - it.y, face = 4 + zp / 3, dist = zp % 3 + 1;
@@ -157,9 +157,9 @@ k_batched_ghosts(const GridMeta* __restrict__ grids, const int2* __restrict__ it
       const int k = face == 5 ? dom.hi[2] + dist : dom.lo[2] - dist;
       ghost_items<4, T>(threadIdx.x, nx * ny, blockDim.x, [&](int r, T& v) -> T* {
         const int i = dom.lo[0] + r % nx, j = dom.lo[1] + r / nx;
-        int c[3] = {i, j, k};
-        v = face_ghost_value(gr, dom, m, face, dist, c);
-        return gr.ptr(i, j, k);
+        T* const cell = gr.ptr(i, j, k);
+        v = face_ghost_value(gr, dom, m, face, dist, cell);
+        return cell;
       });
     }
   }

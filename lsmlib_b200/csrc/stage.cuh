@@ -980,27 +980,25 @@ k_stage_pairs(StageParams<T> p) {
 // reach them.  Each value depends on cells of the domain box only (no edge
 // or corner ghost is read or written), so the threads are independent; the
 // launcher requires at least 3 domain cells along every axis with a bit set.
-// One item per thread, so that every load of the launch is in flight at once
-// (a version that looped a block over a plane's items waited on each
-// iteration's loads in turn): per plane k0..k1, face_ghost_xy_blocks(nx, ny)
-// blocks -- the x ghosts (the 6 cells of a row's two ends together, item
-// 6 j + side * 3 + layer), then the y ghosts (6 rows along x, item
-// nx (side * 3 + layer) + i) -- and after them zchunks blocks for each of
-// the 6 z ghost planes.
+// The grid is about one wave, each thread with the loads of several cells
+// in flight (a version that looped a block over a plane's items waited on
+// each iteration's loads in turn): per group of kGhostPlanes planes from
+// k0, face_ghost_xy_blocks(nx, ny) blocks -- the x ghosts (the 6 cells of a
+// row's two ends together, item 6 j + side * 3 + layer), then the y ghosts
+// (6 rows along x, item nx (side * 3 + layer) + i), the same cell of each
+// plane of the group per thread -- and after them zchunks blocks for each
+// of the 6 z ghost planes.
 template <typename T>
 __device__ __forceinline__ T face_ghost_value(const Grid3<T>& g, const FillBox& dom,
-                                              unsigned m, int face, int dist, int c[3]) {
+                                              unsigned m, int face, int dist, T* cell) {
   const int d = face >> 1;
   const bool hi = face & 1;
-  if (m & (1u << (16 + face))) {
-    c[d] += hi ? -dom.n(d) : dom.n(d);
-    return *g.ptr(c[0], c[1], c[2]);
-  }
-  c[d] = hi ? dom.hi[d] : dom.lo[d];
-  const T e0 = *g.ptr(c[0], c[1], c[2]);
+  const long st = g.stride(d);
+  if (m & (1u << (16 + face))) return *(cell + (hi ? -st : st) * dom.n(d));
+  const T* e = cell + (hi ? -st : st) * dist;   // the domain's cell on the face
+  const T e0 = *e;
   if (m & (1u << (8 + face))) return e0;
-  c[d] += hi ? -1 : 1;
-  const T e1 = *g.ptr(c[0], c[1], c[2]);
+  const T e1 = *(e + (hi ? -st : st));
   const T slope = e0 - e1;
   return e0 + slope * (T)dist;
 }
@@ -1027,7 +1025,11 @@ __device__ __forceinline__ void ghost_items(int first, int end, int stride, F it
   }
 }
 
-// blocks per plane for the x and y ghosts (one item per thread)
+// planes per block of the x and y ghosts (one cell of each plane per thread,
+// all their loads issued before the stores)
+constexpr int kGhostPlanes = 4;
+
+// blocks per group of kGhostPlanes planes for the x and y ghosts
 __host__ __device__ inline int face_ghost_xy_blocks(int nx, int ny, int* bx = nullptr) {
   const int x = (6 * ny + kFaceGhostThreads - 1) / kFaceGhostThreads;
   if (bx) *bx = x;
@@ -1038,15 +1040,15 @@ template <typename T>
 __global__ void __launch_bounds__(kFaceGhostThreads)
 k_face_ghosts(T* phi, Box gb, FillBox dom, unsigned m, int k0, int k1, int zchunks) {
   const int nx = dom.n(0), ny = dom.n(1);
-  const int np = k1 - k0 + 1;
+  const int ngroups = (k1 - k0 + kGhostPlanes) / kGhostPlanes;
   int bx;
   const int bxy = face_ghost_xy_blocks(nx, ny, &bx);
   const Grid3<T> g = make_grid(phi, gb);
   const unsigned any_face[6] = {m & 0x10101u, m & 0x20202u, m & 0x40404u,
                                 m & 0x80808u, m & 0x101010u, m & 0x202020u};
   const int b = (int)blockIdx.x;
-  if (b < np * bxy) {
-    const int k = k0 + b / bxy, sub = b % bxy;
+  if (b < ngroups * bxy) {
+    const int ka = k0 + (b / bxy) * kGhostPlanes, sub = b % bxy;
     int face, dist, i, j;
     if (sub < bx) {
       const int q = sub * kFaceGhostThreads + (int)threadIdx.x;
@@ -1060,18 +1062,24 @@ k_face_ghosts(T* phi, Box gb, FillBox dom, unsigned m, int k0, int k1, int zchun
       const int q = (sub - bx) * kFaceGhostThreads + (int)threadIdx.x;
       if (q >= 6 * nx) return;
       const int r = q / nx;
-      i = dom.lo[0] + q % nx;
+      i = dom.lo[0] + (q - r * nx);
       face = 2 + r / 3;
       dist = r % 3 + 1;
       j = face == 3 ? dom.hi[1] + dist : dom.lo[1] - dist;
     }
     if (!any_face[face]) return;
-    int c[3] = {i, j, k};
-    *g.ptr(i, j, k) = face_ghost_value(g, dom, m, face, dist, c);
+    T* const cell = g.ptr(i, j, ka);
+    T v[kGhostPlanes];
+#pragma unroll
+    for (int u = 0; u < kGhostPlanes; u++)
+      if (ka + u <= k1) v[u] = face_ghost_value(g, dom, m, face, dist, cell + u * g.sz);
+#pragma unroll
+    for (int u = 0; u < kGhostPlanes; u++)
+      if (ka + u <= k1) cell[u * g.sz] = v[u];
     return;
   }
   // z ghost planes: plane zp = side * 3 + layer, chunk of its nx * ny cells
-  const int zb = b - np * bxy;
+  const int zb = b - ngroups * bxy;
   const int zp = zb / zchunks, chunk = zb % zchunks;
   const int face = 4 + zp / 3, dist = zp % 3 + 1;
   if (!any_face[face]) return;
@@ -1082,9 +1090,9 @@ k_face_ghosts(T* phi, Box gb, FillBox dom, unsigned m, int k0, int k1, int zchun
   ghost_items<4, T>(chunk * per + (int)threadIdx.x, end, kFaceGhostThreads,
                     [&](int q, T& v) -> T* {
                       const int i = dom.lo[0] + q % nx, j = dom.lo[1] + q / nx;
-                      int c[3] = {i, j, k};
-                      v = face_ghost_value(g, dom, m, face, dist, c);
-                      return g.ptr(i, j, k);
+                      T* const cell = g.ptr(i, j, k);
+                      v = face_ghost_value(g, dom, m, face, dist, cell);
+                      return cell;
                     });
 }
 

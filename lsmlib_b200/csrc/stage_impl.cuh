@@ -75,8 +75,8 @@ void launch_kind(dim3 grid, const StageArgs& a, const StageParams<T>& p, cudaStr
         const int zchunks = (int)std::min<long>(
             4096, ((long)a.dom.n(0) * a.dom.n(1) + 4 * kFaceGhostThreads - 1) /
                       (4 * kFaceGhostThreads));
-        const long blocks =
-            (long)a.fb.n(2) * face_ghost_xy_blocks(a.dom.n(0), a.dom.n(1)) + 6L * zchunks;
+        const long groups = (a.fb.n(2) + kGhostPlanes - 1) / kGhostPlanes;
+        const long blocks = groups * face_ghost_xy_blocks(a.dom.n(0), a.dom.n(1)) + 6L * zchunks;
         k_face_ghosts<T><<<(unsigned)blocks, kFaceGhostThreads, 0, st>>>(
             (T*)a.phi_s, a.gb, a.dom, a.bc_mask, a.fb.lo[2], a.fb.hi[2], zchunks);
         ++launch_counter();
