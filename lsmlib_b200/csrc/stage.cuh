@@ -214,20 +214,26 @@ __device__ __forceinline__ T weno_side(const T* w, T inv, bool plus,
   return plus ? weno_plus7<T, FAST>(w, inv) : weno_minus7<T, FAST>(w, inv);
 }
 
+// Godunov |grad phi|^2 of the normal-speed term
+// (lsm_level_set_evolution3d.f.in:209-231): per axis, for vn > 0,
+// max(max(phi^-, 0)^2, min(phi^+, 0)^2).  Both operands are squares of
+// non-negative numbers (max(phi^-, 0) and -min(phi^+, 0)), and rounding is
+// monotone, so the larger square is the square of the larger of the two:
+// max(phi^-, -phi^+, 0)^2, the same value in two comparisons and one product
+// instead of three and two (a zero's sign, the only difference, squares away).
 template <typename T>
 __device__ __forceinline__ T godunov_sq2(T vn, T xp, T yp, T zp, T xm, T ym,
                                          T zm) {
-  T a, b, s;
   const T z = T(0);
+  T ax, ay, az;
   if (vn > z) {
-    a = fmax2(xm, z); b = fmin2(xp, z); s = fmax2(a * a, b * b);
-    a = fmax2(ym, z); b = fmin2(yp, z); s = s + fmax2(a * a, b * b);
-    a = fmax2(zm, z); b = fmin2(zp, z); s = s + fmax2(a * a, b * b);
+    ax = fmax2(fmax2(xm, -xp), z); ay = fmax2(fmax2(ym, -yp), z); az = fmax2(fmax2(zm, -zp), z);
   } else {
-    a = fmin2(xm, z); b = fmax2(xp, z); s = fmax2(a * a, b * b);
-    a = fmin2(ym, z); b = fmax2(yp, z); s = s + fmax2(a * a, b * b);
-    a = fmin2(zm, z); b = fmax2(zp, z); s = s + fmax2(a * a, b * b);
+    ax = fmax2(fmax2(-xm, xp), z); ay = fmax2(fmax2(-ym, yp), z); az = fmax2(fmax2(-zm, zp), z);
   }
+  T s = ax * ax;
+  s = s + ay * ay;
+  s = s + az * az;
   return s;
 }
 
@@ -242,17 +248,12 @@ __device__ __forceinline__ T reinit_cell(T pc, T xp, T yp, T zp, T xm, T ym,
                                          bool fp64_sign) {
   const T z = T(0);
   T gp[3] = {xp, yp, zp}, gm[3] = {xm, ym, zm}, gs[3];
+  // per axis max(max(-+phi^+, 0), max(+-phi^-, 0)) as max(-+phi^+, +-phi^-, 0):
+  // the same value (but for a zero's sign, which squares away) in two
+  // comparisons instead of three
 #pragma unroll
-  for (int d = 0; d < 3; d++) {
-    if (pc > z) {
-      gp[d] = fmax2(-gp[d], z);
-      gm[d] = fmax2(gm[d], z);
-    } else {
-      gp[d] = fmax2(gp[d], z);
-      gm[d] = fmax2(-gm[d], z);
-    }
-    gs[d] = fmax2(gp[d], gm[d]);
-  }
+  for (int d = 0; d < 3; d++)
+    gs[d] = pc > z ? fmax2(fmax2(-gp[d], gm[d]), z) : fmax2(fmax2(gp[d], -gm[d]), z);
   // FP64 build's zero_tol for both precisions (see stage_zero_tol)
   if (!(fabsT(pc) >= T(1.0e-11))) return z;
   const T nsq = gs[0] * gs[0] + gs[1] * gs[1] + gs[2] * gs[2];
