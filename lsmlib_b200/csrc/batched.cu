@@ -100,6 +100,7 @@ k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ ite
     p.bc_mask = bc_mask;
     for (int d = 0; d < 3; d++) {
       p.inv[d] = (T)g.inv[d];
+      p.fk[d] = face_const<T>(p.inv[d]);
       p.vel_const[d] = (T)g.vel[d];
     }
     p.dx_sq = (T)g.dx_sq;
@@ -186,6 +187,7 @@ k_grid_stage(const GridMeta* __restrict__ grids, int gi, T* out, const T* phi_s,
   p.bc_mask = bc_mask;
   for (int d = 0; d < 3; d++) {
     p.inv[d] = (T)g.inv[d];
+      p.fk[d] = face_const<T>(p.inv[d]);
     p.vel_const[d] = (T)g.vel[d];
   }
   p.dx_sq = (T)g.dx_sq;

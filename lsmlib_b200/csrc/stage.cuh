@@ -51,6 +51,7 @@ struct StageParams {
   FillBox dom;         // domain box for on-the-fly ghost extrapolation
   unsigned bc_mask;    // bit f set: extrapolate beyond face f (0..5)
   T inv[3];            // 1/dx, 1/dy, 1/dz
+  FaceConst<T> fk[3];  // face_const(inv[d]): the face-shared kernels' WENO5 constants
   T dx_sq;             // max(dx,dy,dz)^2 (reinit sign, CFL)
   const double* dt_dev;
   double dt;
@@ -683,8 +684,8 @@ template <> struct Pair2<float> { using type = float2; };
 constexpr int kPairPX = 4;
 
 template <typename T, bool K64>
-__device__ __forceinline__ void face_pm_t(const T* u, T inv, T& vp, T& vm) {
-  weno5_face<T, sizeof(T) == 4 && K64>(u, inv, vp, vm);
+__device__ __forceinline__ void face_pm_t(const T* u, const FaceConst<T>& k, T& vp, T& vm) {
+  weno5_face<T, sizeof(T) == 4 && K64>(u, k, vp, vm);
 }
 
 template <typename T, int KIND, bool K64, int TX, int TY, int TZ>
@@ -745,7 +746,6 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
   const int xoff = row_start ? (t + 3) * (TX + 8) + PX - 3 : col_c + PX;
   const int xstride = row_start ? 1 : TX + 8;
   T* const xout = row_start ? &fx[t] : &fy[0][col_c];
-  const T xinv = row_start ? p.inv[0] : p.inv[1];
 
   // 32-bit element offsets from the index-space origin (the launcher takes
   // this kernel only for arrays of fewer than 2^31 elements): the 64-bit
@@ -783,8 +783,8 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
   T zrun0 = T(0), zrun1 = T(0);
   if (act0) {
     T unused;
-    face_pm_t<T, K64>(w0 + 1, p.inv[2], unused, zrun0);
-    if (act1) face_pm_t<T, K64>(w1 + 1, p.inv[2], unused, zrun1);
+    face_pm_t<T, K64>(w0 + 1, p.fk[2], unused, zrun0);
+    if (act1) face_pm_t<T, K64>(w1 + 1, p.fk[2], unused, zrun1);
   }
   prefetch(kb);
   for (int k = kb; k <= ke; ++k) {
@@ -856,12 +856,12 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
         weno5_face2(a, p.inv[2], vp, vm);
         zp0 = vp.x; zp1 = vp.y; znx0 = vm.x; znx1 = vm.y;
       } else {
-        face_pm_t<T, K64>(u, p.inv[0], xp0, xm1);
-        face_pm_t<T, K64>(u + 1, p.inv[0], xp1, xnext);
-        face_pm_t<T, K64>(ya, p.inv[1], yp0, ym0);
-        face_pm_t<T, K64>(yb, p.inv[1], yp1, ym1);
-        face_pm_t<T, K64>(w0 + 1, p.inv[2], zp0, znx0);
-        if (act1) face_pm_t<T, K64>(w1 + 1, p.inv[2], zp1, znx1);
+        face_pm_t<T, K64>(u, p.fk[0], xp0, xm1);
+        face_pm_t<T, K64>(u + 1, p.fk[0], xp1, xnext);
+        face_pm_t<T, K64>(ya, p.fk[1], yp0, ym0);
+        face_pm_t<T, K64>(yb, p.fk[1], yp1, ym1);
+        face_pm_t<T, K64>(w0 + 1, p.fk[2], zp0, znx0);
+        if (act1) face_pm_t<T, K64>(w1 + 1, p.fk[2], zp1, znx1);
       }
       if (ty + 1 < TY) *reinterpret_cast<T2*>(&fy[ty + 1][c0]) = T2{ym0, ym1};
     }
@@ -871,7 +871,7 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
       T u[6], unused;
 #pragma unroll
       for (int m = 0; m < 6; m++) u[m] = xb[m * xstride];
-      face_pm_t<T, K64>(u, xinv, unused, *xout);
+      face_pm_t<T, K64>(u, face_const(row_start ? p.inv[0] : p.inv[1]), unused, *xout);
     }
     __syncthreads();
     if (act0) {

@@ -25,7 +25,10 @@ StageParams<T> to_params(const StageArgs& a) {
   p.fb = a.fb;
   p.dom = a.dom;
   p.bc_mask = a.bc_mask;
-  for (int d = 0; d < 3; d++) p.inv[d] = (T)a.inv[d];
+  for (int d = 0; d < 3; d++) {
+    p.inv[d] = (T)a.inv[d];
+    p.fk[d] = face_const<T>(p.inv[d]);
+  }
   p.dx_sq = (T)a.dx_sq;
   p.dt_dev = a.dt_dev;
   p.dt = a.dt;

@@ -196,6 +196,17 @@ static __device__ __noinline__ float2 weno5_face_fp64(float u0, float u1, float 
                                                      float u3, float u4, float u5,
                                                      float inv);
 
+// Per-axis constants of weno5_face: 1/dx and the weights of the middle
+// candidate scaled by it.
+template <typename T>
+struct FaceConst {
+  T inv, c3, c56, c16;   // 1/dx, 1/(3dx), 5/(6dx), 1/(6dx)
+};
+template <typename T>
+__host__ __device__ inline FaceConst<T> face_const(T inv) {
+  return {inv, inv * T(1.0 / 3.0), inv * T(5.0 / 6.0), inv * T(1.0 / 6.0)};
+}
+
 // The two HJ-WENO5 values that share the face between cells c and c+1, from
 // u[0..5] = phi(c-2..c+3): vp = phi^+(c) and vm = phi^-(c+1).  Both read the
 // same five differences V1..V5 (faces c-3/2..c+5/2), minus in the order
@@ -220,33 +231,43 @@ static __device__ __noinline__ float2 weno5_face_fp64(float u0, float u1, float 
 //    once;
 //  * the eps maximum is max|D| squared (rounding is monotone, so this is
 //    exactly the largest square);
-//  * in FP64 one reciprocal of 60 sm sp serves both sides (the products stay
-//    below 2^210; in FP32 they would overflow, so FP32 takes two).
+//  * in FP64 one reciprocal of the product of the two weight sums serves
+//    both sides (the products stay below 2^230; in FP32 they would overflow,
+//    so FP32 takes two).
 // When KINK64 is set (FP32 form) a face whose indicators differ by more than
-// a factor 1e3 is recomputed in FP64.
+// a factor 1e3 is recomputed in FP64.  Three further rearrangements, again
+// only rounding:
+//  * the S_k and eps enter the weights only through ratios of the q_k, so
+//    all four are taken four times over: S_k = 13/3 t1^2 + t2^2 (the
+//    reference's 13/12 t1^2 + 1/4 t2^2) and eps = 4e-6 max D^2 + 4 tiny;
+//  * numerators and weight sums are halved: vm = p2m + (A + 3/2 B) / (3 Pbc +
+//    18 Pac + 9 Pab), vp = p2p - (B + 3/2 A) / (3 Pab + 18 Pac + 9 Pbc), the
+//    18 Pac shared;
+//  * 1/dx is folded into the middle candidate's weights (FaceConst) and
+//    into the one reciprocal.
 template <typename T, bool KINK64>
-__device__ __forceinline__ void weno5_face(const T* u, T inv, T& vp, T& vm) {
+__device__ __forceinline__ void weno5_face(const T* u, const FaceConst<T>& k, T& vp, T& vm) {
   const T V1 = u[1] - u[0], V2 = u[2] - u[1], V3 = u[3] - u[2], V4 = u[4] - u[3],
           V5 = u[5] - u[4];
   const T amax = vmax(vmax(vmax(fabs(V1), fabs(V2)), vmax(fabs(V3), fabs(V4))), fabs(V5));
   const T m = amax * amax;
-  // the reference's 1e-6 max(v^2) + tiny, in units of the undivided
-  // differences (the floor, reached only where every |D| < 1e-46, is kept
-  // in these units)
-  const T eps = T(1e-6) * m + Consts<T>::tiny;
-  const T c13_12 = T(13.0 / 12.0), c14 = T(0.25);
+  // four times the reference's 1e-6 max(v^2) + tiny, in units of the
+  // undivided differences (the floor, reached only where every |D| < 1e-46,
+  // is kept in these units)
+  const T eps = T(4e-6) * m + T(4) * Consts<T>::tiny;
+  const T c13_3 = T(13.0 / 3.0);
   const T ta = V1 - T(2) * V2 + V3, tb = V2 - T(2) * V3 + V4, tc = V3 - T(2) * V4 + V5;
   T t = V1 - T(4) * V2 + T(3) * V3;
-  const T Sa = c13_12 * (ta * ta) + c14 * (t * t);
+  const T Sa = (c13_3 * ta) * ta + t * t;
   t = V2 - V4;
-  const T Sb = c13_12 * (tb * tb) + c14 * (t * t);
+  const T Sb = (c13_3 * tb) * tb + t * t;
   t = T(3) * V3 - T(4) * V4 + V5;
-  const T Sc = c13_12 * (tc * tc) + c14 * (t * t);
+  const T Sc = (c13_3 * tc) * tc + t * t;
   if (KINK64) {
     const T mx = vmax(vmax(Sa, Sb), Sc), mn = vmin(vmin(Sa, Sb), Sc);
-    if (mx > T(1e3) * mn + T(1e-4) * m) {
+    if (mx > T(1e3) * mn + T(4e-4) * m) {
       if constexpr (sizeof(T) == 4) {
-        const float2 r = weno5_face_fp64(u[0], u[1], u[2], u[3], u[4], u[5], inv);
+        const float2 r = weno5_face_fp64(u[0], u[1], u[2], u[3], u[4], u[5], k.inv);
         vp = r.x;
         vm = r.y;
         return;
@@ -259,21 +280,26 @@ __device__ __forceinline__ void weno5_face(const T* u, T inv, T& vp, T& vm) {
   const T Qa = qa * qa, Qb = qb * qb, Qc = qc * qc;
   const T Pbc = Qb * Qc, Pac = Qa * Qc, Pab = Qa * Qb;
   const T A = Pbc * (ta - tb), B = Pab * (tb - tc);
-  const T num_m = T(2) * A + T(3) * B, num_p = T(2) * B + T(3) * A;
-  const T e3 = T(5.0 / 6.0) * V3;
-  const T p2m = T(1.0 / 3.0) * V4 + (e3 - T(1.0 / 6.0) * V2);
-  const T p2p = T(1.0 / 3.0) * V2 + (e3 - T(1.0 / 6.0) * V4);
-  // 60 sm and 60 sp
-  const T sm = T(6) * Pbc + T(36) * Pac + T(18) * Pab;
-  const T sp = T(6) * Pab + T(36) * Pac + T(18) * Pbc;
+  const T num_m = T(1.5) * B + A, num_p = T(1.5) * A + B;
+  const T e3 = k.c56 * V3;
+  const T p2m = k.c3 * V4 + (e3 - k.c16 * V2);
+  const T p2p = k.c3 * V2 + (e3 - k.c16 * V4);
+  // 30 sm and 30 sp
+  const T p18 = T(18) * Pac;
+  const T sm = T(3) * Pbc + (T(9) * Pab + p18);
+  const T sp = T(3) * Pab + (T(9) * Pbc + p18);
   if constexpr (sizeof(T) == 8) {
-    const T r = rcp_nr(sm * sp);
-    vm = (p2m + num_m * (sp * r)) * inv;
-    vp = (p2p - num_p * (sm * r)) * inv;
+    const T r = rcp_nr(sm * sp) * k.inv;
+    vm = p2m + num_m * (sp * r);
+    vp = p2p - num_p * (sm * r);
   } else {
-    vm = (p2m + num_m * rcp_nr(sm)) * inv;
-    vp = (p2p - num_p * rcp_nr(sp)) * inv;
+    vm = p2m + num_m * (rcp_nr(sm) * k.inv);
+    vp = p2p - num_p * (rcp_nr(sp) * k.inv);
   }
+}
+template <typename T, bool KINK64>
+__device__ __forceinline__ void weno5_face(const T* u, T inv, T& vp, T& vm) {
+  weno5_face<T, KINK64>(u, face_const(inv), vp, vm);
 }
 
 // weno5_face<float> for two independent faces at once, one per lane of a
