@@ -683,9 +683,9 @@ template <> struct Pair2<float> { using type = float2; };
 // stage_tile_faces.
 constexpr int kPairPX = 4;
 
-template <typename T, bool K64>
+template <typename T, bool K64, bool LMAX = false>
 __device__ __forceinline__ void face_pm_t(const T* u, const FaceConst<T>& k, T& vp, T& vm) {
-  weno5_face<T, sizeof(T) == 4 && K64>(u, k, vp, vm);
+  weno5_face<T, sizeof(T) == 4 && K64, LMAX>(u, k, vp, vm);
 }
 
 template <typename T, int KIND, bool K64, int TX, int TY, int TZ>
@@ -856,7 +856,8 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
         weno5_face2(a, p.inv[2], vp, vm);
         zp0 = vp.x; zp1 = vp.y; znx0 = vm.x; znx1 = vm.y;
       } else {
-        face_pm_t<T, K64>(u, p.fk[0], xp0, xm1);
+        face_pm_t<T, K64, true>(u, p.fk[0], xp0, xm1);   // shares its eps maximum's
+                                                          // inner part with the next
         face_pm_t<T, K64>(u + 1, p.fk[0], xp1, xnext);
         face_pm_t<T, K64>(ya, p.fk[1], yp0, ym0);
         face_pm_t<T, K64>(yb, p.fk[1], yp1, ym1);

@@ -245,11 +245,15 @@ __host__ __device__ inline FaceConst<T> face_const(T inv) {
 //    18 Pac shared;
 //  * 1/dx is folded into the middle candidate's weights (FaceConst) and
 //    into the one reciprocal.
-template <typename T, bool KINK64>
+// LMAX: the eps maximum grouped as max(|D1|, max(|D2|..|D5|)) instead of
+// max(max(|D1|..|D4|), |D5|) -- the same value; a face evaluated with LMAX
+// beside the face one cell on (without) shares the inner four-way maximum.
+template <typename T, bool KINK64, bool LMAX = false>
 __device__ __forceinline__ void weno5_face(const T* u, const FaceConst<T>& k, T& vp, T& vm) {
   const T V1 = u[1] - u[0], V2 = u[2] - u[1], V3 = u[3] - u[2], V4 = u[4] - u[3],
           V5 = u[5] - u[4];
-  const T amax = vmax(vmax(vmax(fabs(V1), fabs(V2)), vmax(fabs(V3), fabs(V4))), fabs(V5));
+  const T amax = LMAX ? vmax(fabs(V1), vmax(vmax(fabs(V2), fabs(V3)), vmax(fabs(V4), fabs(V5))))
+                      : vmax(vmax(vmax(fabs(V1), fabs(V2)), vmax(fabs(V3), fabs(V4))), fabs(V5));
   const T m = amax * amax;
   // four times the reference's 1e-6 max(v^2) + tiny, in units of the
   // undivided differences (the floor, reached only where every |D| < 1e-46,
@@ -322,30 +326,33 @@ __device__ __forceinline__ void weno5_face2(const float2* u, float inv, float2& 
   amax.x = vmax(vmax(vmax(fabsf(V1.x), fabsf(V2.x)), vmax(fabsf(V3.x), fabsf(V4.x))), fabsf(V5.x));
   amax.y = vmax(vmax(vmax(fabsf(V1.y), fabsf(V2.y)), vmax(fabsf(V3.y), fabsf(V4.y))), fabsf(V5.y));
   const float2 m = mul2(amax, amax);
-  const float2 eps = fma2(f2(1e-6f), m, f2(Consts<float>::tiny));
-  const float2 c13_12 = f2(13.0f / 12.0f), c14 = f2(0.25f);
+  // S_k and eps four times over, as in weno5_face
+  const float2 eps = fma2(f2(4e-6f), m, f2(4.0f * Consts<float>::tiny));
+  const float2 c13_3 = f2(13.0f / 3.0f);
   const float2 ta = add2(fma2(f2(-2.0f), V2, V1), V3);
   const float2 tb = add2(fma2(f2(-2.0f), V3, V2), V4);
   const float2 tc = add2(fma2(f2(-2.0f), V4, V3), V5);
   float2 t = fma2(f2(3.0f), V3, fma2(f2(-4.0f), V2, V1));
-  const float2 Sa = fma2(c13_12, mul2(ta, ta), mul2(c14, mul2(t, t)));
+  const float2 Sa = fma2(mul2(c13_3, ta), ta, mul2(t, t));
   t = sub2(V2, V4);
-  const float2 Sb = fma2(c13_12, mul2(tb, tb), mul2(c14, mul2(t, t)));
+  const float2 Sb = fma2(mul2(c13_3, tb), tb, mul2(t, t));
   t = add2(fma2(f2(-4.0f), V4, mul2(f2(3.0f), V3)), V5);
-  const float2 Sc = fma2(c13_12, mul2(tc, tc), mul2(c14, mul2(t, t)));
+  const float2 Sc = fma2(mul2(c13_3, tc), tc, mul2(t, t));
   const float2 sc = make_float2(inv_pow2_of(eps.x), inv_pow2_of(eps.y));
   const float2 es = mul2(eps, sc);
   const float2 qa = fma2(Sa, sc, es), qb = fma2(Sb, sc, es), qc = fma2(Sc, sc, es);
   const float2 Qa = mul2(qa, qa), Qb = mul2(qb, qb), Qc = mul2(qc, qc);
   const float2 Pbc = mul2(Qb, Qc), Pac = mul2(Qa, Qc), Pab = mul2(Qa, Qb);
   const float2 A = mul2(Pbc, sub2(ta, tb)), B = mul2(Pab, sub2(tb, tc));
-  const float2 num_m = fma2(f2(2.0f), A, mul2(f2(3.0f), B));
-  const float2 num_p = fma2(f2(2.0f), B, mul2(f2(3.0f), A));
+  // halved numerators and weight sums, as in weno5_face
+  const float2 num_m = fma2(f2(1.5f), B, A);
+  const float2 num_p = fma2(f2(1.5f), A, B);
   const float2 e3 = mul2(f2(5.0f / 6.0f), V3);
   const float2 p2m = fma2(f2(1.0f / 3.0f), V4, fma2(f2(-1.0f / 6.0f), V2, e3));
   const float2 p2p = fma2(f2(1.0f / 3.0f), V2, fma2(f2(-1.0f / 6.0f), V4, e3));
-  const float2 sm = fma2(f2(6.0f), Pbc, fma2(f2(36.0f), Pac, mul2(f2(18.0f), Pab)));
-  const float2 sp = fma2(f2(6.0f), Pab, fma2(f2(36.0f), Pac, mul2(f2(18.0f), Pbc)));
+  const float2 p18 = mul2(f2(18.0f), Pac);
+  const float2 sm = fma2(f2(3.0f), Pbc, fma2(f2(9.0f), Pab, p18));
+  const float2 sp = fma2(f2(3.0f), Pab, fma2(f2(9.0f), Pbc, p18));
   // reciprocals: per-lane seeds, one packed Newton-Raphson step (rcp_nr)
   float2 rm, rp;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rm.x) : "f"(sm.x));
