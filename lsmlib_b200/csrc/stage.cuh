@@ -895,11 +895,187 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
   return hmax;
 }
 
+// The one-sided (upwind) kinds -- external velocity arrays, LeVeque's
+// deformation field, a constant velocity -- with two cells per thread, in
+// the layout of stage_tile_pairs: thread (t, ty) of a TX/2 x TY block owns
+// cells x0+2t and x0+2t+1 of row j0+ty and marches them along z, reading
+// every ghost cell as stored.  Each cell takes one WENO5 side per axis, chosen
+// by the sign of its velocity component (no face is shared between cells),
+// so one barrier per plane suffices: plane k goes to buffer (k-kb)&1, and a
+// thread writing that buffer again two planes on has passed the barrier of
+// the plane between, which every reader of plane k has reached.  The pair
+// reads its x stencils (cells x0+2t-4 .. x0+2t+5) as five and its y
+// columns as seven 16-byte shared loads.  Per cell the arithmetic is that
+// of stage_tile (weno_upwind_side and the same RHS and RK update).
+template <typename T, int KIND, bool K64, int TX, int TY, int TZ>
+__device__ __forceinline__ void stage_tile_pairs_up(const StageParams<T>& p, int bx, int by,
+                                                    int bz, T (*tile)[TY + 6][TX + 8]) {
+  using T2 = typename Pair2<T>::type;
+  static_assert(TX == 32, "a tile row is one half-warp of pairs");
+  constexpr int NP = TX / 2;
+  constexpr int PX = kPairPX;
+  const int t = threadIdx.x, ty = threadIdx.y;
+  const int x0 = p.fb.lo[0] + bx * TX, j0 = p.fb.lo[1] + by * TY;
+  const int c0 = 2 * t;
+  const int i0 = x0 + c0, i1 = i0 + 1;
+  const int j = j0 + ty;
+  const int kb = p.fb.lo[2] + bz * TZ;
+  const int ke = min(kb + TZ - 1, p.fb.hi[2]);
+  const int hi0 = p.fb.hi[0], hi1 = p.fb.hi[1];
+  const bool rowin = j <= hi1;
+  const bool act0 = rowin && i0 <= hi0, act1 = rowin && i1 <= hi0;
+  const bool halo0 = !act0 && i0 <= hi0 + 3 && j <= hi1 + 3 && !(i0 > hi0 && j > hi1);
+  const bool halo1 = !act1 && i1 <= hi0 + 3 && j <= hi1 + 3 && !(i1 > hi0 && j > hi1);
+  const long sy = p.gb.sy(), sz = p.gb.sz();
+  const long base0 = -((long)p.gb.lo[0] + sy * p.gb.lo[1] + sz * p.gb.lo[2]);
+  const T dt = p.dt_dev ? (T)(*p.dt_dev) : (T)p.dt;
+  const T ztol = stage_zero_tol<T>();
+
+  // side strips and halo roles as in stage_tile_pairs
+  int hxa = 0, hxb = 0;
+  bool has_a = false, has_b = false;
+  if (rowin) {
+    if (t == 0) { hxa = x0 - 3; hxb = x0 - 2; has_a = has_b = true; }
+    else if (t == 1) { hxa = x0 - 1; has_a = true; }
+    else if (t == NP - 1) {
+      hxa = x0 + TX; hxb = x0 + TX + 1;
+      has_a = hxa <= hi0 + 3; has_b = hxb <= hi0 + 3;
+    } else if (t == NP - 2) { hxa = x0 + TX + 2; has_a = hxa <= hi0 + 3; }
+  }
+  const int cola = hxa - x0 + PX, colb = hxb - x0 + PX;
+  const int hj = ty < 3 ? j0 - 3 + ty : j + 3;
+  const bool has_hy = (ty < 3) || (ty >= TY - 3 && rowin);
+  const bool hy0 = has_hy && i0 <= hi0, hy1 = has_hy && i1 <= hi0;
+  const int trow = ty < 3 ? ty : ty + 6;
+
+  const T* P0 = p.phi_s + base0;
+  const int isy = (int)sy, isz = (int)sz;
+  auto ld = [&](int a, int b, int c) -> T { return __ldg(P0 + (a + isy * b + isz * c)); };
+  T n0 = T(0), n1 = T(0), na = T(0), nb = T(0), ny0 = T(0), ny1 = T(0);
+  auto prefetch = [&](int k) {
+    if (act0) n0 = ld(i0, j, k + 3);
+    else if (halo0) n0 = ld(i0, j, k);
+    if (act1) n1 = ld(i1, j, k + 3);
+    else if (halo1) n1 = ld(i1, j, k);
+    if (has_a) na = ld(hxa, j, k);
+    if (has_b) nb = ld(hxb, j, k);
+    if (hy0) ny0 = ld(i0, hj, k);
+    if (hy1) ny1 = ld(i1, hj, k);
+  };
+
+  T w0[7] = {}, w1[7] = {};
+  if (act0) {
+#pragma unroll
+    for (int m = 0; m < 6; m++) w0[m + 1] = ld(i0, j, kb - 3 + m);
+  }
+  if (act1) {
+#pragma unroll
+    for (int m = 0; m < 6; m++) w1[m + 1] = ld(i1, j, kb - 3 + m);
+  }
+  prefetch(kb);
+  for (int k = kb; k <= ke; ++k) {
+    const int buf = (k - kb) & 1;
+    T v0 = n0, v1 = n1;
+    if (act0) {
+#pragma unroll
+      for (int m = 0; m < 6; m++) w0[m] = w0[m + 1];
+      w0[6] = n0;
+      v0 = w0[3];
+    }
+    if (act1) {
+#pragma unroll
+      for (int m = 0; m < 6; m++) w1[m] = w1[m + 1];
+      w1[6] = n1;
+      v1 = w1[3];
+    }
+    *reinterpret_cast<T2*>(&tile[buf][ty + 3][c0 + PX]) = T2{v0, v1};
+    if (has_a) tile[buf][ty + 3][cola] = na;
+    if (has_b) tile[buf][ty + 3][colb] = nb;
+    if (hy0 || hy1) *reinterpret_cast<T2*>(&tile[buf][trow][c0 + PX]) = T2{ny0, ny1};
+    __syncthreads();
+    if (k < ke) prefetch(k + 1);
+    if (!act0) continue;
+    const long o0 = base0 + (i0 + isy * j + isz * k);
+    // velocities and the RK input of both cells, loaded before the stencils
+    T a[2][3] = {}, uc[2] = {};
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      if (c == 1 && !act1) break;
+      const long o = o0 + c;
+      if (KIND == kStageAdvect) {
+        a[c][0] = __ldg(p.aux0 + o); a[c][1] = __ldg(p.aux1 + o); a[c][2] = __ldg(p.aux2 + o);
+      } else if (KIND == kStageDeformation) {
+        const int nx = p.fb.hi[0] - p.fb.lo[0] + 1, ny = p.fb.hi[1] - p.fb.lo[1] + 1,
+                  nz = p.fb.hi[2] - p.fb.lo[2] + 1;
+        const double* tx_ = p.defo_tab + p.defo_off[0] + (i0 + c - p.fb.lo[0]);
+        const double* ty_ = p.defo_tab + p.defo_off[1] + (j - p.fb.lo[1]);
+        const double* tz_ = p.defo_tab + p.defo_off[2] + (k - p.fb.lo[2]);
+        DeformSines sn;
+        sn.sx = __ldg(tx_); sn.s2x = __ldg(tx_ + nx);
+        sn.sy = __ldg(ty_); sn.s2y = __ldg(ty_ + ny);
+        sn.sz = __ldg(tz_); sn.s2z = __ldg(tz_ + nz);
+        deformation_velocity(sn, __ldg(p.g_dev), a[c][0], a[c][1], a[c][2]);
+      } else {
+        a[c][0] = p.vel_const[0]; a[c][1] = p.vel_const[1]; a[c][2] = p.vel_const[2];
+      }
+      if (p.rk_kind != 1) uc[c] = __ldg(p.phi_n + o);
+    }
+    // one axis at a time for both cells, so that only one axis's stencils
+    // are live: x from tile columns c0 .. c0+9 (phi(x0+2t-4 .. x0+2t+5)),
+    // y from rows j-3 .. j+3 of the pair's two columns, z from the windows
+    const bool kink64 = K64;
+    T g[2][3] = {};
+    {
+      T q[10];
+#pragma unroll
+      for (int m = 0; m < 5; m++) {
+        const T2 v = *reinterpret_cast<const T2*>(&tile[buf][ty + 3][c0 + 2 * m]);
+        q[2 * m] = v.x;
+        q[2 * m + 1] = v.y;
+      }
+#pragma unroll
+      for (int c = 0; c < 2; c++)
+        if ((c == 0 || act1) && !(fabsT(a[c][0]) < ztol))
+          g[c][0] = weno_upwind_side<T, true>(q + 1 + c, p.inv[0], !(a[c][0] > T(0)), kink64);
+    }
+    {
+      T ya[7], yb[7];
+#pragma unroll
+      for (int m = 0; m < 7; m++) {
+        const T2 v = *reinterpret_cast<const T2*>(&tile[buf][ty + m][c0 + PX]);
+        ya[m] = v.x;
+        yb[m] = v.y;
+      }
+      if (!(fabsT(a[0][1]) < ztol))
+        g[0][1] = weno_upwind_side<T, true>(ya, p.inv[1], !(a[0][1] > T(0)), kink64);
+      if (act1 && !(fabsT(a[1][1]) < ztol))
+        g[1][1] = weno_upwind_side<T, true>(yb, p.inv[1], !(a[1][1] > T(0)), kink64);
+    }
+    if (!(fabsT(a[0][2]) < ztol))
+      g[0][2] = weno_upwind_side<T, true>(w0, p.inv[2], !(a[0][2] > T(0)), kink64);
+    if (act1 && !(fabsT(a[1][2]) < ztol))
+      g[1][2] = weno_upwind_side<T, true>(w1, p.inv[2], !(a[1][2] > T(0)), kink64);
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      if (c == 1 && !act1) break;
+      const T L = T(0) - (a[c][0] * g[c][0] + a[c][1] * g[c][1] + a[c][2] * g[c][2]);
+      p.out[o0 + c] = stage_out(p, o0 + c, uc[c], c ? w1[3] : w0[3], L, dt);
+    }
+  }
+}
+
 template <typename T, int KIND, bool FAST, int TX>
 struct UseFaces {
   static constexpr bool value =
       (FAST || sizeof(T) == 4) && TX == 32 &&
       (KIND == kStageNormal || KIND == kStageReinit || KIND == kStageNormalRhs);
+};
+// the one-sided kinds of stage_tile_pairs_up
+template <typename T, int KIND, bool FAST, int TX>
+struct UsePairsUp {
+  static constexpr bool value =
+      (FAST || sizeof(T) == 4) && TX == 32 &&
+      (KIND == kStageAdvect || KIND == kStageDeformation || KIND == kStageAdvectConst);
 };
 
 // kStageNormalRhs: the block's largest CFL speed into its partials slot,
@@ -971,6 +1147,16 @@ k_stage_pairs(StageParams<T> p) {
   const double hmax = stage_tile_pairs<T, KIND, K64, TX, TY, TZ>(
       p, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, tile, fy, fx);
   block_max_partial<KIND, TX / 2 * TY>(p, hmax);
+}
+
+// The one-sided kinds, two cells per thread (stage_tile_pairs_up); every
+// ghost cell the stencils reach is read as stored.
+template <typename T, int KIND, bool K64, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(TX / 2 * TY, LSMGPU_PAIR_MIN_BLOCKS)
+k_stage_pairs_up(StageParams<T> p) {
+  __shared__ __align__(16) T tile[2][TY + 6][TX + 8];
+  stage_tile_pairs_up<T, KIND, K64, TX, TY, TZ>(p, (int)blockIdx.x, (int)blockIdx.y,
+                                               (int)blockIdx.z, tile);
 }
 
 // The face ghost cells of phi that the stencils of fill-box cells in planes

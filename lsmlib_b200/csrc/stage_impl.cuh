@@ -59,30 +59,42 @@ bool ghosts_storable(const StageArgs& a) {
   return true;
 }
 
-// One kind: the face-shared two-cells-per-thread kernel where it applies
-// (FMA or FP32 arithmetic, two-sided kinds) and the ghost cells are stored
-// (no boundary kind, or k_face_ghosts writes them first); else one cell per
-// thread with the boundary values generated on the fly.  Both cover TX x TY
-// x TZ cells per block, so the grid (and the per-block CFL partials) are the
-// same.
+// The boundary values of a.bc_mask into phi_s's ghost cells: the planes of
+// the fill box, and the z faces its stencils reach (about 4 cells per
+// thread of a z ghost plane).
+template <typename T>
+void launch_face_ghosts(const StageArgs& a, cudaStream_t st) {
+  const int zchunks = (int)std::min<long>(
+      4096, ((long)a.dom.n(0) * a.dom.n(1) + 4 * kFaceGhostThreads - 1) /
+                (4 * kFaceGhostThreads));
+  const long groups = (a.fb.n(2) + kGhostPlanes - 1) / kGhostPlanes;
+  const long blocks = groups * face_ghost_xy_blocks(a.dom.n(0), a.dom.n(1)) + 6L * zchunks;
+  k_face_ghosts<T><<<(unsigned)blocks, kFaceGhostThreads, 0, st>>>(
+      (T*)a.phi_s, a.gb, a.dom, a.bc_mask, a.fb.lo[2], a.fb.hi[2], zchunks);
+  ++launch_counter();
+}
+
+// The pair kernels take the stage: offsets fit 32 bits, and the ghost cells
+// are stored (no boundary kind, or k_face_ghosts can write them first).
+bool pairs_apply(const StageArgs& a) {
+  const bool small = a.gb.sz() * (long)a.gb.n[2] < (1L << 31);   // 32-bit offsets
+  return small && (a.bc_mask == 0u || ghosts_storable(a));
+}
+
+// One kind: a two-cells-per-thread kernel where it applies (FMA or FP32
+// arithmetic; the face-shared kernel for the two-sided kinds, the one-sided
+// pair kernel for the upwind kinds) and pairs_apply; else one cell per
+// thread with the boundary values generated on the fly.  All cover TX x TY
+// x TZ cells per block, so the grid (and the per-block CFL partials) are
+// the same.
 template <typename T, int KIND>
 void launch_kind(dim3 grid, const StageArgs& a, const StageParams<T>& p, cudaStream_t st) {
   constexpr int TX = kStageTX, TY = kStageTY, TZ = kStageTZ;
   if constexpr (LSMGPU_STAGE_PAIRS && UseFaces<T, KIND, STAGE_FAST, TX>::value) {
-    const bool small = a.gb.sz() * (long)a.gb.n[2] < (1L << 31);   // 32-bit offsets
-    if (small && (a.bc_mask == 0u || ghosts_storable(a))) {
+    if (pairs_apply(a)) {
       StageParams<T> q = p;
       if (a.bc_mask != 0u) {
-        // the planes of the fill box, and the z faces its stencils reach
-        // (about 4 cells per thread of a z ghost plane)
-        const int zchunks = (int)std::min<long>(
-            4096, ((long)a.dom.n(0) * a.dom.n(1) + 4 * kFaceGhostThreads - 1) /
-                      (4 * kFaceGhostThreads));
-        const long groups = (a.fb.n(2) + kGhostPlanes - 1) / kGhostPlanes;
-        const long blocks = groups * face_ghost_xy_blocks(a.dom.n(0), a.dom.n(1)) + 6L * zchunks;
-        k_face_ghosts<T><<<(unsigned)blocks, kFaceGhostThreads, 0, st>>>(
-            (T*)a.phi_s, a.gb, a.dom, a.bc_mask, a.fb.lo[2], a.fb.hi[2], zchunks);
-        ++launch_counter();
+        launch_face_ghosts<T>(a, st);
         q.bc_mask = 0u;
       }
       const dim3 blk(TX / 2, TY, 1);
@@ -93,6 +105,24 @@ void launch_kind(dim3 grid, const StageArgs& a, const StageParams<T>& p, cudaStr
         }
       }
       k_stage_pairs<T, KIND, false, TX, TY, TZ><<<grid, blk, 0, st>>>(q);
+      return;
+    }
+  }
+  if constexpr (LSMGPU_STAGE_PAIRS && UsePairsUp<T, KIND, STAGE_FAST, TX>::value) {
+    if (pairs_apply(a)) {
+      StageParams<T> q = p;
+      if (a.bc_mask != 0u) {
+        launch_face_ghosts<T>(a, st);
+        q.bc_mask = 0u;
+      }
+      const dim3 blk(TX / 2, TY, 1);
+      if constexpr (sizeof(T) == 4) {
+        if (p.fp64_policy & kFp64Kinks) {
+          k_stage_pairs_up<T, KIND, true, TX, TY, TZ><<<grid, blk, 0, st>>>(q);
+          return;
+        }
+      }
+      k_stage_pairs_up<T, KIND, false, TX, TY, TZ><<<grid, blk, 0, st>>>(q);
       return;
     }
   }
