@@ -645,10 +645,12 @@ int lsmgpu_batch_download(lsmgpu_batch *b, void *host);
 /* vel[3*g..3*g+2]: constant velocity of grid g; sets every grid's CFL dt */
 int lsmgpu_batch_set_velocity(lsmgpu_batch *b, const double *vel, double cfl);
 int lsmgpu_batch_get_dt(lsmgpu_batch *b, double *dt);
-/* configuration 0..9: tile shape (shape % 5: 32x8x16, 32x8x32, 32x8x64,
+/* configuration 0..14: tile shape (shape % 5: 32x8x16, 32x8x32, 32x8x64,
  * 16x8x16, 16x8x32 cells) and halo-staging schedule (shape / 5: 0 the x/y
  * stencils through a shared plane with its side strips, 1 straight from
- * global memory); get_tile returns the configuration and its tile */
+ * global memory, 2 two cells per thread through the shared plane, ghost
+ * cells stored first -- schedule 0 where a grid is too thin for that);
+ * get_tile returns the configuration and its tile */
 int lsmgpu_batch_set_tile(lsmgpu_batch *b, int shape);
 int lsmgpu_batch_get_tile(lsmgpu_batch *b, int *shape, int tile[3]);
 int lsmgpu_batch_set_fp64_kinks(lsmgpu_batch *b, int on);
@@ -659,8 +661,8 @@ int lsmgpu_batch_set_fp64_policy(lsmgpu_batch *b, int policy);
 /* boundary of every grid: 0 linear extrapolation (default), 1 copy
  * (homogeneous Neumann), 2 periodic */
 int lsmgpu_batch_set_bc(lsmgpu_batch *b, int kind);
-/* times each of the 10 configurations (tile shape x halo-staging schedule)
- * on the batch (state preserved), keeps the fastest; ms_out (optional, 10
+/* times each of the 15 configurations (tile shape x halo-staging schedule)
+ * on the batch (state preserved), keeps the fastest; ms_out (optional, 15
  * floats) receives one time per configuration */
 int lsmgpu_batch_autotune(lsmgpu_batch *b, float *ms_out);
 /* mode 0: graph replay of persistent work-list launches; 1: the same without

@@ -13,6 +13,10 @@ from . import gpu
 from .ext_abi import dbls, ints
 
 MODE_GRAPH, MODE_PERSISTENT, MODE_PER_GRID = 0, 1, 2
+# batch configurations: tile shape c % 5 (32x8x16, 32x8x32, 32x8x64, 16x8x16,
+# 16x8x32 cells) with halo-staging schedule c // 5 (0 shared plane, 1 direct
+# loads, 2 two cells per thread)
+N_CONFIGS = 15
 BC_LINEAR, BC_COPY, BC_PERIODIC = 0, 1, 2
 
 
@@ -112,9 +116,9 @@ class Batch:
                      "batch_set_fp64_kinks")
 
     def autotune(self, report=True):
-        """Times the 10 configurations (5 tile shapes x 2 halo-staging
+        """Times the N_CONFIGS configurations (5 tile shapes x 3 halo-staging
         schedules) and keeps the fastest; returns their ms per step."""
-        ms = (ctypes.c_float * 10)() if report else None
+        ms = (ctypes.c_float * N_CONFIGS)() if report else None
         gpu.check_rc(gpu.load().lsmgpu_batch_autotune(self.h, ms), "batch_autotune")
         return list(ms) if report else None
 

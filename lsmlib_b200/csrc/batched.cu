@@ -41,15 +41,26 @@ struct GridMeta {
   double vel[3];
 };
 
-// tile shapes the autotuner chooses from, each with two halo-staging
-// schedules (stage_tile's STAGING: shared plane, direct loads): configuration
-// c is shape c % kNumShapes with schedule c / kNumShapes
+// tile shapes the autotuner chooses from, each with three halo-staging
+// schedules: 0 and 1 are stage_tile's STAGING (one cell per thread; x/y
+// stencils through a shared plane with its side strips, or straight from
+// global memory), 2 is stage_tile_pairs_up (two cells per thread, shared
+// plane, one barrier per plane; needs the ghost cells stored).
+// Configuration c is shape c % kNumShapes with schedule c / kNumShapes.
 struct TileShape { int tx, ty, tz; };
 constexpr TileShape kShapes[] = {{32, 8, 16}, {32, 8, 32}, {32, 8, 64}, {16, 8, 16},
                                  {16, 8, 32}};
 constexpr int kNumShapes = 5;
-constexpr int kNumStagings = 2;
+constexpr int kNumStagings = 3;
 constexpr int kNumConfigs = kNumShapes * kNumStagings;
+constexpr int kPairStaging = 2;
+
+// threads per block of a schedule, and the blocks per SM its register
+// budget allows (one cell per thread: LSMGPU_BATCH_WARPS warps per SM; two
+// cells per thread: 16 warps, the budget of the single-grid pair kernels)
+#define BATCH_THREADS(TX, TY, SG) ((SG) == kPairStaging ? (TX) / 2 * (TY) : (TX) * (TY))
+#define BATCH_MIN_BLOCKS(TX, TY, SG) \
+  ((SG) == kPairStaging ? 512 / ((TX) / 2 * (TY)) : LSMGPU_BATCH_WARPS * 32 / ((TX) * (TY)))
 
 // seed of the stochastic rounding of one stage: the step number kept on the
 // device (bumped at the end of every step, so that graph replays differ)
@@ -70,13 +81,29 @@ __global__ void k_bump(unsigned* c) { *c += 1u; }
 #define LSMGPU_BATCH_WARPS 24
 #endif
 
+// one tile of the batch with a schedule's stage routine
 template <typename T, int TX, int TY, int TZ, int STAGING>
-__global__ void __launch_bounds__(TX * TY, LSMGPU_BATCH_WARPS * 32 / (TX * TY))
+__device__ __forceinline__ void batch_tile(const StageParams<T>& p, int bx, int by, int bz,
+                                           int policy) {
+  if constexpr (STAGING == kPairStaging) {
+    __shared__ __align__(16) T tile[2][TY + 6][TX + 8];
+    if (sizeof(T) == 4 && (policy & kFp64Kinks))
+      stage_tile_pairs_up<T, kStageAdvectConst, sizeof(T) == 4, TX, TY, TZ>(p, bx, by, bz, tile);
+    else
+      stage_tile_pairs_up<T, kStageAdvectConst, false, TX, TY, TZ>(p, bx, by, bz, tile);
+  } else {
+    __shared__ T tile[2][TY + 6][TX + 6];
+    stage_tile<T, kStageAdvectConst, true, TX, TY, TZ, STAGING>(p, bx, by, bz, tile);
+  }
+}
+
+template <typename T, int TX, int TY, int TZ, int STAGING>
+__global__ void __launch_bounds__(BATCH_THREADS(TX, TY, STAGING),
+                                  BATCH_MIN_BLOCKS(TX, TY, STAGING))
 k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ items,
                 int nitems, unsigned* counter, T* out, const T* phi_s,
                 const T* phi_n, int rk_kind, int policy, const unsigned* sr_step,
                 unsigned bc_mask) {
-  __shared__ T tile[2][TY + 6][TX + 6];
   __shared__ int s_item;
   for (;;) {
     if (threadIdx.x == 0 && threadIdx.y == 0) s_item = (int)atomicAdd(counter, 1u);
@@ -110,7 +137,7 @@ k_batched_stage(const GridMeta* __restrict__ grids, const int4* __restrict__ ite
     p.use_phi0 = 0;
     p.fp64_policy = policy & kFp64Kinks;
     p.sr_seed = batch_sr_seed<T>(policy, sr_step, rk_kind);
-    stage_tile<T, kStageAdvectConst, true, TX, TY, TZ, STAGING>(p, it.y, it.z, it.w, tile);
+    batch_tile<T, TX, TY, TZ, STAGING>(p, it.y, it.z, it.w, policy);
   }
 }
 
@@ -168,11 +195,11 @@ k_batched_ghosts(const GridMeta* __restrict__ grids, const int2* __restrict__ it
 
 // the plain alternative: one launch per grid per stage
 template <typename T, int TX, int TY, int TZ, int STAGING>
-__global__ void __launch_bounds__(TX * TY, LSMGPU_BATCH_WARPS * 32 / (TX * TY))
+__global__ void __launch_bounds__(BATCH_THREADS(TX, TY, STAGING),
+                                  BATCH_MIN_BLOCKS(TX, TY, STAGING))
 k_grid_stage(const GridMeta* __restrict__ grids, int gi, T* out, const T* phi_s,
              const T* phi_n, int rk_kind, int policy, const unsigned* sr_step,
              unsigned bc_mask) {
-  __shared__ T tile[2][TY + 6][TX + 6];
   const GridMeta& g = grids[gi];
   StageParams<T> p;
   p.out = out + g.offset;
@@ -197,8 +224,7 @@ k_grid_stage(const GridMeta* __restrict__ grids, int gi, T* out, const T* phi_s,
   p.use_phi0 = 0;
   p.fp64_policy = policy & kFp64Kinks;
   p.sr_seed = batch_sr_seed<T>(policy, sr_step, rk_kind);
-  stage_tile<T, kStageAdvectConst, true, TX, TY, TZ, STAGING>(
-      p, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, tile);
+  batch_tile<T, TX, TY, TZ, STAGING>(p, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, policy);
 }
 
 std::mutex g_tune_mutex;
@@ -251,26 +277,32 @@ cudaError_t launch_shape(lsmgpu_batch* b, int shape, bool batched, int rk_kind,
                          T* out, const T* in, const T* base, unsigned* counter,
                          cudaStream_t st) {
   // persistent grid: every SM filled with as many blocks of the
-  // configuration as fit
-  const int cfg = shape;
+  // configuration as fit.  The two-cells-per-thread schedule reads the ghost
+  // cells as stored; without them (a grid with fewer than 3 cells along an
+  // axis) its shape runs with schedule 0.
+  int cfg = shape;
+  if (cfg / kNumShapes == kPairStaging && !b->ghosts_stored) cfg %= kNumShapes;
   shape = cfg % kNumShapes;
+  const int sg = cfg / kNumShapes;
+  const int threads = sg == kPairStaging ? kShapes[shape].tx / 2 * kShapes[shape].ty
+                                         : kShapes[shape].tx * kShapes[shape].ty;
+#define BATCH_CONFIGS(X)                                                           \
+  X(0, 32, 8, 16, 0) X(1, 32, 8, 32, 0) X(2, 32, 8, 64, 0) X(3, 16, 8, 16, 0)      \
+  X(4, 16, 8, 32, 0) X(5, 32, 8, 16, 1) X(6, 32, 8, 32, 1) X(7, 32, 8, 64, 1)      \
+  X(8, 16, 8, 16, 1) X(9, 16, 8, 32, 1) X(10, 32, 8, 16, 2) X(11, 32, 8, 32, 2)    \
+  X(12, 32, 8, 64, 2) X(13, 16, 8, 16, 2) X(14, 16, 8, 32, 2)
   if (b->resident[cfg] == 0) {
     const void* fn = nullptr;
+#define BATCH_FN(I, TX, TY, TZ, SG) \
+  case I: fn = (const void*)k_batched_stage<T, TX, TY, TZ, SG>; break;
     switch (cfg) {
-      case 0: fn = (const void*)k_batched_stage<T, 32, 8, 16, 0>; break;
-      case 1: fn = (const void*)k_batched_stage<T, 32, 8, 32, 0>; break;
-      case 2: fn = (const void*)k_batched_stage<T, 32, 8, 64, 0>; break;
-      case 3: fn = (const void*)k_batched_stage<T, 16, 8, 16, 0>; break;
-      case 4: fn = (const void*)k_batched_stage<T, 16, 8, 32, 0>; break;
-      case 5: fn = (const void*)k_batched_stage<T, 32, 8, 16, 1>; break;
-      case 6: fn = (const void*)k_batched_stage<T, 32, 8, 32, 1>; break;
-      case 7: fn = (const void*)k_batched_stage<T, 32, 8, 64, 1>; break;
-      case 8: fn = (const void*)k_batched_stage<T, 16, 8, 16, 1>; break;
-      default: fn = (const void*)k_batched_stage<T, 16, 8, 32, 1>; break;
+      BATCH_CONFIGS(BATCH_FN)
+      default: return cudaErrorInvalidValue;
     }
+#undef BATCH_FN
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kShapes[shape].tx * kShapes[shape].ty,
-                                                      0) != cudaSuccess || nb < 1) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, 0) != cudaSuccess ||
+        nb < 1) {
       cudaGetLastError();
       nb = b->blocks_per_sm;
     }
@@ -289,33 +321,25 @@ cudaError_t launch_shape(lsmgpu_batch* b, int shape, bool batched, int rk_kind,
 #define BATCH_CASE(I, TX, TY, TZ, SG)                                              \
   case I:                                                                          \
     if (batched) {                                                                 \
-      k_batched_stage<T, TX, TY, TZ, SG><<<grid, dim3(TX, TY), 0, st>>>(           \
+      k_batched_stage<T, TX, TY, TZ, SG><<<grid, dim3(BATCH_THREADS(TX, TY, SG) / (TY), TY), 0, st>>>( \
           b->d_meta, b->d_items[I % kNumShapes], b->nitems[I % kNumShapes], counter, \
           out, in, base, rk_kind, b->policy, b->d_counter + 3, bcm);               \
     } else {                                                                       \
       for (int gi = 0; gi < b->ngrids; gi++) {                                     \
         const FillBox& f = b->meta[gi].fb;                                         \
         dim3 g((f.n(0) + TX - 1) / TX, (f.n(1) + TY - 1) / TY, (f.n(2) + TZ - 1) / TZ); \
-        k_grid_stage<T, TX, TY, TZ, SG><<<g, dim3(TX, TY), 0, st>>>(               \
+        k_grid_stage<T, TX, TY, TZ, SG><<<g, dim3(BATCH_THREADS(TX, TY, SG) / (TY), TY), 0, st>>>( \
             b->d_meta, gi, out, in, base, rk_kind, b->policy, b->d_counter + 3,    \
             bcm);                                                                  \
       }                                                                            \
     }                                                                              \
     break;
   switch (cfg) {
-    BATCH_CASE(0, 32, 8, 16, 0)
-    BATCH_CASE(1, 32, 8, 32, 0)
-    BATCH_CASE(2, 32, 8, 64, 0)
-    BATCH_CASE(3, 16, 8, 16, 0)
-    BATCH_CASE(4, 16, 8, 32, 0)
-    BATCH_CASE(5, 32, 8, 16, 1)
-    BATCH_CASE(6, 32, 8, 32, 1)
-    BATCH_CASE(7, 32, 8, 64, 1)
-    BATCH_CASE(8, 16, 8, 16, 1)
-    BATCH_CASE(9, 16, 8, 32, 1)
+    BATCH_CONFIGS(BATCH_CASE)
     default: return cudaErrorInvalidValue;
   }
 #undef BATCH_CASE
+#undef BATCH_CONFIGS
   launch_counter() += batched ? 1 : b->ngrids;
   return cudaGetLastError();
 }
@@ -566,7 +590,8 @@ int lsmgpu_batch_get_dt(lsmgpu_batch* b, double* dt) {
 }
 
 // configuration: tile shape (shape % 5 of the list above) and halo-staging
-// schedule (shape / 5: 0 shared plane, 1 direct loads)
+// schedule (shape / 5: 0 shared plane, 1 direct loads, 2 two cells per
+// thread)
 int lsmgpu_batch_set_tile(lsmgpu_batch* b, int shape) {
   if (!batch_ok(b, "lsmgpu_batch_set_tile")) return LSMGPU_ERR_NULL_POINTER;
   if (shape < 0 || shape >= kNumConfigs) {

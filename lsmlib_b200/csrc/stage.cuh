@@ -911,7 +911,9 @@ template <typename T, int KIND, bool K64, int TX, int TY, int TZ>
 __device__ __forceinline__ void stage_tile_pairs_up(const StageParams<T>& p, int bx, int by,
                                                     int bz, T (*tile)[TY + 6][TX + 8]) {
   using T2 = typename Pair2<T>::type;
-  static_assert(TX == 32, "a tile row is one half-warp of pairs");
+  // (no lane exchange: a row of TX/2 >= 4 threads of any width works)
+  static_assert(TX % 2 == 0 && TX / 2 >= 4, "strip roles need four threads per row");
+  static_assert(TY >= 3, "the y strips need three rows at each end");
   constexpr int NP = TX / 2;
   constexpr int PX = kPairPX;
   const int t = threadIdx.x, ty = threadIdx.y;

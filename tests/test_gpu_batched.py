@@ -59,7 +59,7 @@ def test_launch_modes_agree_bitwise():
     assert np.array_equal(outs[0].view(np.uint64), outs[2].view(np.uint64))
 
 
-@pytest.mark.parametrize("shape", range(10))
+@pytest.mark.parametrize("shape", range(15))
 def test_every_tile_shape_gives_the_same_result(shape):
     from lsmlib_b200 import batched, workloads
     cfg = small_batch(seed=8, ngrids=5)
@@ -88,7 +88,7 @@ def test_autotune_keeps_state_and_picks_a_shape():
     after = np.concatenate([a.ravel() for a in b.download()])
     assert np.array_equal(before, after)
     s, tile = b.tile()
-    assert 0 <= s < 10 and tile[1] == 8
+    assert 0 <= s < 15 and tile[1] == 8
 
 
 def test_fp32_batch_error_against_fp64():
