@@ -1112,16 +1112,16 @@ def run_reference(args, world, rank, budget_s=90.0):
 
 def profile_batched(ngrids=64):
     """Two steps of a batch of the config-4 generator's first `ngrids` grids
-    (FP64, periodic boundaries, the shape the autotuner picks for the full
-    batch: 16x8x32), launched directly (no graph), for an ncu capture of
-    k_batched_stage and k_batched_ghosts."""
+    (FP64, periodic boundaries, the configuration the autotuner picks for the
+    full batch: 16x8x32 tiles, two cells per thread), launched directly (no
+    graph), for an ncu capture of k_batched_stage and k_batched_ghosts."""
     from lsmlib_b200 import batched, gpu, workloads
     cfg = workloads.config4(ngrids=ngrids)
     b = batched.Batch(cfg["sizes"], cfg["dx"], 8)
     b.upload(workloads.config4_phi(cfg, np.float64))
     b.set_velocity(cfg["vel"], cfg["cfl"])
     b.set_bc(batched.BC_PERIODIC)
-    b.set_tile(4)
+    b.set_tile(14)
     b.advect(2, mode=batched.MODE_PERSISTENT)
     gpu.check_rc(gpu.load().lsmgpu_stream_synchronize(), "sync")
 

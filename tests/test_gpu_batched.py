@@ -60,19 +60,27 @@ def test_launch_modes_agree_bitwise():
 
 
 @pytest.mark.parametrize("shape", range(15))
-def test_every_tile_shape_gives_the_same_result(shape):
+@pytest.mark.parametrize("prec", [8, 4])
+def test_every_tile_shape_gives_the_same_result(shape, prec):
+    """Every tile shape and halo-staging schedule (one cell per thread with a
+    shared plane or direct loads, two cells per thread) gives the same bits,
+    in FP64 and in FP32 with stochastic rounding and FP64 kinks."""
     from lsmlib_b200 import batched, workloads
     cfg = small_batch(seed=8, ngrids=5)
-    phis = workloads.config4_phi(cfg)
+    dtype = np.float64 if prec == 8 else np.float32
+    phis = workloads.config4_phi(cfg, dtype)
     res = []
     for s in (1, shape):
-        b = batched.Batch(cfg["sizes"], cfg["dx"], 8)
+        b = batched.Batch(cfg["sizes"], cfg["dx"], prec)
         b.upload(phis)
         b.set_velocity(cfg["vel"], 0.5)
+        if prec == 4:
+            b.set_fp64_policy(5)
         b.set_tile(s)
         b.advect(2, batched.MODE_PERSISTENT)
         res.append(np.concatenate([a.ravel() for a in b.download()]))
-    assert np.array_equal(res[0].view(np.uint64), res[1].view(np.uint64))
+    u = np.uint64 if prec == 8 else np.uint32
+    assert np.array_equal(res[0].view(u), res[1].view(u))
 
 
 def test_autotune_keeps_state_and_picks_a_shape():
