@@ -23,6 +23,12 @@
 
 using namespace lsmgpu;
 
+// z-slabs of the host-array driver's copies (see lsmgpu_normal_tvdrk3_host)
+#ifndef LSMGPU_HOST_SLABS
+#define LSMGPU_HOST_SLABS 4
+#endif
+constexpr int kHostSlabs = LSMGPU_HOST_SLABS;
+
 struct lsmgpu_workspace {
   Box gb;
   int prec;
@@ -40,8 +46,8 @@ struct lsmgpu_workspace {
   void* dF[2] = {nullptr, nullptr};
   cudaStream_t copy_stream = nullptr;       // host -> device
   cudaStream_t copy_stream_out = nullptr;   // device -> host
-  cudaEvent_t slab_ev[8] = {};              // [q] in, [4 + q] final stage
-  cudaEvent_t out_ev[4] = {};
+  cudaEvent_t slab_ev[2 * kHostSlabs] = {};  // [q] in, [kHostSlabs + q] final stage
+  cudaEvent_t out_ev[kHostSlabs] = {};
   cudaEvent_t F_ev[2] = {};
   cudaEvent_t start_ev = nullptr;
   int host_async = 0;       // lsmgpu_workspace_set_host_async
@@ -745,10 +751,6 @@ int lsmgpu_normal_tvdrk3(lsmgpu_workspace* ws, void* phi, const void* F,
 // of two device buffers while the previous call still computes, and each
 // slab of phi is copied in as soon as the previous call's copy of that slab
 // back to the host has landed (copies in and out on two streams).
-namespace {
-constexpr int kHostSlabs = 4;
-}
-
 int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
                               const int fb[6], const double dx[3], double cfl, int nsteps,
                               int step0, int reinit_interval, int reinit_iters,
