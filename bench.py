@@ -56,6 +56,11 @@ WORKLOAD = ("256^3 normal-velocity level set (6 spheres, F = 1 + 0.2 sin sin sin
 # profiles/k_stage_pairs_config2_256.md (distinct phi_s and phi^n)
 NCU_TRAFFIC = {"stage_reinit_rk32": 395.0e6, "stage_normal_rk32": 541.1e6}
 NCU_FP64_PIPE = {"stage_reinit_rk32": 63.2, "stage_normal_rk32": 64.0}
+# FP64 thread instructions per cell of the same kernels (ncu op counters
+# smsp__sass_thread_inst_executed_op_fp64_pred_on, the same capture's
+# profile command) and the B200's FP64 lanes per SM
+NCU_FP64_OPS_PER_CELL = {"stage_reinit_rk32": 266.8, "stage_normal_rk32": 254.8}
+FP64_LANES_PER_SM = 64
 
 def env_int(name, default):
     try:
@@ -363,10 +368,22 @@ def run_ours(args, world, rank, local, pg):
     dom = "stage_reinit_rk32" if share_re >= share_no else "stage_normal_rk32"
     achieved = kern[dom]["bytes"] / (kern[dom]["ms"] / 1e3) / 1e9
     traffic = NCU_TRAFFIC.get(dom) if N_CELLS == 256 else None
+    # the FP64 pipe's share: the kernel's FP64 instructions per second over
+    # the SMs' FP64 lanes at the SM clock sampled under load
+    import torch
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+    fp64_peak = n_sm * FP64_LANES_PER_SM * mhz * 1e6
+    fp64_ach = NCU_FP64_OPS_PER_CELL[dom] * cells / (kern[dom]["ms"] / 1e3)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                 "traffic_source": "ncu capture, profiles/k_stage_pairs_config2_256.md",
                 "fp64_pipe_active_pct_ncu": NCU_FP64_PIPE.get(dom),
+                "fp64_frac": round(fp64_ach / fp64_peak, 3),
+                "fp64": {"achieved_Tops": round(fp64_ach / 1e12, 2),
+                         "peak_Tops": round(fp64_peak / 1e12, 2),
+                         "ops_per_cell_ncu": NCU_FP64_OPS_PER_CELL[dom], "sms": n_sm,
+                         "sm_mhz": mhz},
                 "kernel": dom, "kernel_ms": round(kern[dom]["ms"], 4),
                 "algorithmic_bytes_per_launch": kern[dom]["bytes"],
                 "peak_source": peak_kind,
@@ -482,7 +499,7 @@ def run_ours(args, world, rank, local, pg):
         "distance": sig(compact_distance(distance_res)),
         "roofline": sig(pick(roofline, "bound", "achieved", "peak", "unit", "frac",
                              "traffic", "kernel", "kernel_ms", "peak_source",
-                             "fp64_pipe_active_pct_ncu")),
+                             "fp64_pipe_active_pct_ncu", "fp64_frac")),
         "e2e": sig(pick(e2e, "value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step",
                         "ms_per_step", "blocking_ms_per_step")),
         "gpu_launches": int(launches),
