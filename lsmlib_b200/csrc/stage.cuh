@@ -906,7 +906,9 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
 // the plane between, which every reader of plane k has reached.  The pair
 // reads its x stencils (cells x0+2t-4 .. x0+2t+5) as five and its y
 // columns as seven 16-byte shared loads.  Per cell the arithmetic is that
-// of stage_tile (weno_upwind_side and the same RHS and RK update).
+// of stage_tile (weno_upwind_side and the same RHS and RK update), but for
+// FP32 without the FP64 kink recomputation, where the two cells' sides of
+// an axis are one packed FP32x2 evaluation (weno5_side2).
 template <typename T, int KIND, bool K64, int TX, int TY, int TZ>
 __device__ __forceinline__ void stage_tile_pairs_up(const StageParams<T>& p, int bx, int by,
                                                     int bz, T (*tile)[TY + 6][TX + 8]) {
@@ -1027,6 +1029,26 @@ __device__ __forceinline__ void stage_tile_pairs_up(const StageParams<T>& p, int
     // y from rows j-3 .. j+3 of the pair's two columns, z from the windows
     const bool kink64 = K64;
     T g[2][3] = {};
+    // one axis for both cells: scalar sides, or (FP32 without the FP64 kink
+    // recomputation) both cells' sides in one packed evaluation, each lane
+    // with the differences of its own window in its own side's order
+    auto axis = [&](int d, const T* wa, const T* wb) {
+      const bool up0 = !(fabsT(a[0][d]) < ztol), up1 = act1 && !(fabsT(a[1][d]) < ztol);
+      if constexpr (sizeof(T) == 4 && !K64) {
+        const bool pl0 = !(a[0][d] > T(0)), pl1 = !(a[1][d] > T(0));
+        float2 D[5];
+#pragma unroll
+        for (int m = 0; m < 5; m++)
+          D[m] = make_float2(pl0 ? wa[6 - m] - wa[5 - m] : wa[m + 1] - wa[m],
+                             pl1 ? wb[6 - m] - wb[5 - m] : wb[m + 1] - wb[m]);
+        const float2 r = weno5_side2(D, p.inv[d]);
+        if (up0) g[0][d] = r.x;
+        if (up1) g[1][d] = r.y;
+      } else {
+        if (up0) g[0][d] = weno_upwind_side<T, true>(wa, p.inv[d], !(a[0][d] > T(0)), kink64);
+        if (up1) g[1][d] = weno_upwind_side<T, true>(wb, p.inv[d], !(a[1][d] > T(0)), kink64);
+      }
+    };
     {
       T q[10];
 #pragma unroll
@@ -1035,10 +1057,7 @@ __device__ __forceinline__ void stage_tile_pairs_up(const StageParams<T>& p, int
         q[2 * m] = v.x;
         q[2 * m + 1] = v.y;
       }
-#pragma unroll
-      for (int c = 0; c < 2; c++)
-        if ((c == 0 || act1) && !(fabsT(a[c][0]) < ztol))
-          g[c][0] = weno_upwind_side<T, true>(q + 1 + c, p.inv[0], !(a[c][0] > T(0)), kink64);
+      axis(0, q + 1, q + 2);
     }
     {
       T ya[7], yb[7];
@@ -1048,15 +1067,9 @@ __device__ __forceinline__ void stage_tile_pairs_up(const StageParams<T>& p, int
         ya[m] = v.x;
         yb[m] = v.y;
       }
-      if (!(fabsT(a[0][1]) < ztol))
-        g[0][1] = weno_upwind_side<T, true>(ya, p.inv[1], !(a[0][1] > T(0)), kink64);
-      if (act1 && !(fabsT(a[1][1]) < ztol))
-        g[1][1] = weno_upwind_side<T, true>(yb, p.inv[1], !(a[1][1] > T(0)), kink64);
+      axis(1, ya, yb);
     }
-    if (!(fabsT(a[0][2]) < ztol))
-      g[0][2] = weno_upwind_side<T, true>(w0, p.inv[2], !(a[0][2] > T(0)), kink64);
-    if (act1 && !(fabsT(a[1][2]) < ztol))
-      g[1][2] = weno_upwind_side<T, true>(w1, p.inv[2], !(a[1][2] > T(0)), kink64);
+    axis(2, w0, w1);
 #pragma unroll
     for (int c = 0; c < 2; c++) {
       if (c == 1 && !act1) break;

@@ -60,6 +60,12 @@ __device__ __forceinline__ T sqrt_nr(T x) {
   return x >= T(sizeof(T) == 8 ? 1e-300 : 1e-30) ? x * rsqrt_nr(x) : T(sqrt(x));
 }
 
+// a * b + c with one rounding, written out where an expression has two
+// products, so that every instantiation fuses the same one (the contraction
+// the compiler picks can differ between inlining contexts)
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
+
 // max and min for the eps maxima and the kink tests: a plain comparison in
 // FP64 (CUDA's IEEE fmax of doubles, which also sorts out NaN operands, cost
 // a third of the stage kernels' integer instructions; these values are
@@ -81,33 +87,35 @@ __device__ __forceinline__ float inv_pow2_of(float x) {
 
 // One side of HJ-WENO5 from the five undivided differences D1..D5 in the
 // reference's ordering (v_k = D_k / dx); returns the reconstruction of the
-// scaled differences.  The same rearrangement as weno5_face below: the
-// weights see only ratios of D (scaling by 1/dx is applied once at the end),
-// eps is taken from max|D|, and with w2 = 1 - w1 - w3
-//   phi = p2 + (2 P23 (ta - tb) + 3 P12 (tb - tc)) / (6 P23 + 36 P13 + 18 P12),
+// scaled differences.  The same rearrangements as weno5_face below (rounding
+// only): the weights see only ratios of D (scaling by 1/dx is applied once
+// at the end), eps is taken from max|D|, the S_k and eps are taken four
+// times over, and with w2 = 1 - w1 - w3 and numerator and weight sum halved
+//   phi = p2 + (P23 (ta - tb) + 3/2 P12 (tb - tc)) / (3 P23 + 18 P13 + 9 P12),
 // P_xy = (q_x q_y)^2, ta, tb, tc the second differences of the smoothness
 // indicators.
 template <typename T>
 __device__ __forceinline__ T weno5_side_fast(T D1, T D2, T D3, T D4, T D5, T inv) {
   const T amax = vmax(vmax(vmax(fabs(D1), fabs(D2)), vmax(fabs(D3), fabs(D4))), fabs(D5));
-  const T eps = T(1e-6) * (amax * amax) + Consts<T>::tiny;
-  const T c13_12 = T(13.0 / 12.0), c14 = T(0.25);
-  const T ta = D1 - T(2) * D2 + D3, tb = D2 - T(2) * D3 + D4, tc = D3 - T(2) * D4 + D5;
-  T t = D1 - T(4) * D2 + T(3) * D3;
-  const T S1 = c13_12 * (ta * ta) + c14 * (t * t);
+  const T eps = fmaT(T(4e-6), amax * amax, T(4) * Consts<T>::tiny);
+  const T c13_3 = T(13.0 / 3.0);
+  const T ta = fmaT(T(-2), D2, D1) + D3, tb = fmaT(T(-2), D3, D2) + D4,
+          tc = fmaT(T(-2), D4, D3) + D5;
+  T t = fmaT(T(3), D3, fmaT(T(-4), D2, D1));
+  const T S1 = fmaT(c13_3 * ta, ta, t * t);
   t = D2 - D4;
-  const T S2 = c13_12 * (tb * tb) + c14 * (t * t);
-  t = T(3) * D3 - T(4) * D4 + D5;
-  const T S3 = c13_12 * (tc * tc) + c14 * (t * t);
+  const T S2 = fmaT(c13_3 * tb, tb, t * t);
+  t = fmaT(T(-4), D4, T(3) * D3) + D5;
+  const T S3 = fmaT(c13_3 * tc, tc, t * t);
   const T sc = inv_pow2_of(eps);
   const T es = eps * sc;
-  const T q1 = S1 * sc + es, q2 = S2 * sc + es, q3 = S3 * sc + es;
+  const T q1 = fmaT(S1, sc, es), q2 = fmaT(S2, sc, es), q3 = fmaT(S3, sc, es);
   const T Q1 = q1 * q1, Q2 = q2 * q2, Q3 = q3 * q3;
   const T P23 = Q2 * Q3, P13 = Q1 * Q3, P12 = Q1 * Q2;
-  const T num = T(2) * (P23 * (ta - tb)) + T(3) * (P12 * (tb - tc));
-  const T den = T(6) * P23 + T(36) * P13 + T(18) * P12;
-  const T p2 = T(1.0 / 3.0) * D4 + (T(5.0 / 6.0) * D3 - T(1.0 / 6.0) * D2);
-  return (p2 + num * rcp_nr(den)) * inv;
+  const T num = fmaT(T(1.5), P12 * (tb - tc), P23 * (ta - tb));
+  const T den = fmaT(T(3), P23, fmaT(T(18), P13, T(9) * P12));
+  const T p2 = fmaT(T(1.0 / 3.0), D4, fmaT(T(-1.0 / 6.0), D2, T(5.0 / 6.0) * D3));
+  return fmaT(num, rcp_nr(den), p2) * inv;
 }
 
 // Weights and combination of one side from its smoothness indicators,
@@ -258,15 +266,16 @@ __device__ __forceinline__ void weno5_face(const T* u, const FaceConst<T>& k, T&
   // four times the reference's 1e-6 max(v^2) + tiny, in units of the
   // undivided differences (the floor, reached only where every |D| < 1e-46,
   // is kept in these units)
-  const T eps = T(4e-6) * m + T(4) * Consts<T>::tiny;
+  const T eps = fmaT(T(4e-6), m, T(4) * Consts<T>::tiny);
   const T c13_3 = T(13.0 / 3.0);
-  const T ta = V1 - T(2) * V2 + V3, tb = V2 - T(2) * V3 + V4, tc = V3 - T(2) * V4 + V5;
-  T t = V1 - T(4) * V2 + T(3) * V3;
-  const T Sa = (c13_3 * ta) * ta + t * t;
+  const T ta = fmaT(T(-2), V2, V1) + V3, tb = fmaT(T(-2), V3, V2) + V4,
+          tc = fmaT(T(-2), V4, V3) + V5;
+  T t = fmaT(T(3), V3, fmaT(T(-4), V2, V1));
+  const T Sa = fmaT(c13_3 * ta, ta, t * t);
   t = V2 - V4;
-  const T Sb = (c13_3 * tb) * tb + t * t;
-  t = T(3) * V3 - T(4) * V4 + V5;
-  const T Sc = (c13_3 * tc) * tc + t * t;
+  const T Sb = fmaT(c13_3 * tb, tb, t * t);
+  t = fmaT(T(-4), V4, T(3) * V3) + V5;
+  const T Sc = fmaT(c13_3 * tc, tc, t * t);
   if (KINK64) {
     const T mx = vmax(vmax(Sa, Sb), Sc), mn = vmin(vmin(Sa, Sb), Sc);
     if (mx > T(1e3) * mn + T(4e-4) * m) {
@@ -280,25 +289,25 @@ __device__ __forceinline__ void weno5_face(const T* u, const FaceConst<T>& k, T&
   }
   const T sc = inv_pow2_of(eps);
   const T es = eps * sc;
-  const T qa = Sa * sc + es, qb = Sb * sc + es, qc = Sc * sc + es;
+  const T qa = fmaT(Sa, sc, es), qb = fmaT(Sb, sc, es), qc = fmaT(Sc, sc, es);
   const T Qa = qa * qa, Qb = qb * qb, Qc = qc * qc;
   const T Pbc = Qb * Qc, Pac = Qa * Qc, Pab = Qa * Qb;
   const T A = Pbc * (ta - tb), B = Pab * (tb - tc);
-  const T num_m = T(1.5) * B + A, num_p = T(1.5) * A + B;
+  const T num_m = fmaT(T(1.5), B, A), num_p = fmaT(T(1.5), A, B);
   const T e3 = k.c56 * V3;
-  const T p2m = k.c3 * V4 + (e3 - k.c16 * V2);
-  const T p2p = k.c3 * V2 + (e3 - k.c16 * V4);
+  const T p2m = fmaT(k.c3, V4, fmaT(-k.c16, V2, e3));
+  const T p2p = fmaT(k.c3, V2, fmaT(-k.c16, V4, e3));
   // 30 sm and 30 sp
   const T p18 = T(18) * Pac;
-  const T sm = T(3) * Pbc + (T(9) * Pab + p18);
-  const T sp = T(3) * Pab + (T(9) * Pbc + p18);
+  const T sm = fmaT(T(3), Pbc, fmaT(T(9), Pab, p18));
+  const T sp = fmaT(T(3), Pab, fmaT(T(9), Pbc, p18));
   if constexpr (sizeof(T) == 8) {
     const T r = rcp_nr(sm * sp) * k.inv;
-    vm = p2m + num_m * (sp * r);
-    vp = p2p - num_p * (sm * r);
+    vm = fmaT(num_m, sp * r, p2m);
+    vp = fmaT(-num_p, sm * r, p2p);
   } else {
-    vm = p2m + num_m * (rcp_nr(sm) * k.inv);
-    vp = p2p - num_p * (rcp_nr(sp) * k.inv);
+    vm = fmaT(num_m, rcp_nr(sm) * k.inv, p2m);
+    vp = fmaT(-num_p, rcp_nr(sp) * k.inv, p2p);
   }
 }
 template <typename T, bool KINK64>
@@ -363,6 +372,42 @@ __device__ __forceinline__ void weno5_face2(const float2* u, float inv, float2& 
   rp = fma2(rp, fma2(mul2(f2(-1.0f), sp), rp, f2(1.0f)), rp);
   vm = mul2(fma2(num_m, rm, p2m), f2(inv));
   vp = mul2(fma2(mul2(f2(-1.0f), num_p), rp, p2p), f2(inv));
+}
+
+// weno5_side_fast<float> for two independent sides at once, one per lane of
+// a float2 (D[m].x and D[m].y: the five undivided differences of each side
+// in its own order), with the packed FP32x2 operations of weno5_face2; the
+// eps maxima, the power-of-two scalings and the reciprocal seeds stay per
+// lane.
+__device__ __forceinline__ float2 weno5_side2(const float2* D, float inv) {
+  const float2 D1 = D[0], D2 = D[1], D3 = D[2], D4 = D[3], D5 = D[4];
+  float2 amax;
+  amax.x = vmax(vmax(vmax(fabsf(D1.x), fabsf(D2.x)), vmax(fabsf(D3.x), fabsf(D4.x))), fabsf(D5.x));
+  amax.y = vmax(vmax(vmax(fabsf(D1.y), fabsf(D2.y)), vmax(fabsf(D3.y), fabsf(D4.y))), fabsf(D5.y));
+  const float2 eps = fma2(f2(4e-6f), mul2(amax, amax), f2(4.0f * Consts<float>::tiny));
+  const float2 c13_3 = f2(13.0f / 3.0f);
+  const float2 ta = add2(fma2(f2(-2.0f), D2, D1), D3);
+  const float2 tb = add2(fma2(f2(-2.0f), D3, D2), D4);
+  const float2 tc = add2(fma2(f2(-2.0f), D4, D3), D5);
+  float2 t = fma2(f2(3.0f), D3, fma2(f2(-4.0f), D2, D1));
+  const float2 S1 = fma2(mul2(c13_3, ta), ta, mul2(t, t));
+  t = sub2(D2, D4);
+  const float2 S2 = fma2(mul2(c13_3, tb), tb, mul2(t, t));
+  t = add2(fma2(f2(-4.0f), D4, mul2(f2(3.0f), D3)), D5);
+  const float2 S3 = fma2(mul2(c13_3, tc), tc, mul2(t, t));
+  const float2 sc = make_float2(inv_pow2_of(eps.x), inv_pow2_of(eps.y));
+  const float2 es = mul2(eps, sc);
+  const float2 q1 = fma2(S1, sc, es), q2 = fma2(S2, sc, es), q3 = fma2(S3, sc, es);
+  const float2 Q1 = mul2(q1, q1), Q2 = mul2(q2, q2), Q3 = mul2(q3, q3);
+  const float2 P23 = mul2(Q2, Q3), P13 = mul2(Q1, Q3), P12 = mul2(Q1, Q2);
+  const float2 num = fma2(f2(1.5f), mul2(P12, sub2(tb, tc)), mul2(P23, sub2(ta, tb)));
+  const float2 den = fma2(f2(3.0f), P23, fma2(f2(18.0f), P13, mul2(f2(9.0f), P12)));
+  const float2 p2 = fma2(f2(1.0f / 3.0f), D4, fma2(f2(-1.0f / 6.0f), D2, mul2(f2(5.0f / 6.0f), D3)));
+  float2 r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.x) : "f"(den.x));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.y) : "f"(den.y));
+  r = fma2(r, fma2(mul2(f2(-1.0f), den), r, f2(1.0f)), r);
+  return mul2(fma2(num, r, p2), f2(inv));
 }
 
 static __device__ __noinline__ float2 weno5_face_fp64(float u0, float u1, float u2,

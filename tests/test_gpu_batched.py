@@ -83,6 +83,28 @@ def test_every_tile_shape_gives_the_same_result(shape, prec):
     assert np.array_equal(res[0].view(u), res[1].view(u))
 
 
+@pytest.mark.parametrize("shape", [10, 11, 12, 13, 14])
+def test_fp32_packed_schedule_matches_one_cell_per_thread(shape):
+    """FP32 without the FP64 kink recomputation: the two-cells-per-thread
+    schedule evaluates both cells' WENO5 sides as one packed FP32x2
+    computation, which rounds differently from the scalar one-cell schedule;
+    the two stay within a few FP32 ulps of the level set's scale."""
+    from lsmlib_b200 import batched, workloads
+    cfg = small_batch(seed=8, ngrids=5)
+    phis = workloads.config4_phi(cfg, np.float32)
+    res = []
+    for s in (0, shape):
+        b = batched.Batch(cfg["sizes"], cfg["dx"], 4)
+        b.upload(phis)
+        b.set_velocity(cfg["vel"], 0.5)
+        b.set_fp64_policy(0)
+        b.set_tile(s)
+        b.advect(2, batched.MODE_PERSISTENT)
+        res.append(np.concatenate([a.ravel() for a in b.download()]).astype(np.float64))
+    scale = np.max(np.abs(res[0]))
+    assert np.max(np.abs(res[0] - res[1])) <= 1e-5 * scale
+
+
 def test_autotune_keeps_state_and_picks_a_shape():
     from lsmlib_b200 import batched, workloads
     cfg = small_batch(seed=11, ngrids=6)
