@@ -877,12 +877,17 @@ def run_config3(lib, pg, world, n_window=512, window=100, n_full=256):
     timer = gpu.Timer()
     res = {"workload": "LeVeque deformation of a sphere, period 3, WENO5 + TVD-RK3, "
                        "CFL 0.5, velocity in-kernel (no velocity arrays)"}
+    # the FP32 form as it is, and with the tiles near the interface in FP64
+    # (FP64_BAND: |phi| < 16 dx, widened by one tile)
+    forms = ((8, "fp64", 0), (4, "fp32", 0), (4, "fp32band", integrator.FP64_BAND))
     cfg = workloads.config3(n_window)
     gb, fb = workloads.boxes(cfg["n"])
     cells = cfg["n"][0] * cfg["n"][1] * cfg["n"][2]
-    for prec, key in ((8, "fp64"), (4, "fp32")):
+    for prec, key, extra in forms:
         dtype = np.float64 if prec == 8 else np.float32
         ws = integrator.Workspace(gb, prec)
+        if extra:
+            ws.set_fp64_policy(integrator.FP64_SIGN | integrator.STOCH_ROUND | extra)
         d = gpu.DeviceArray.from_host(cfg["phi"].astype(dtype))
         ws.deformation(d, fb, cfg["dx"], cfg["x_lo"], period=cfg["period"], cfl=cfg["cfl"],
                        t_end=cfg["t_end"], nsteps=3)
@@ -901,9 +906,11 @@ def run_config3(lib, pg, world, n_window=512, window=100, n_full=256):
     inner = tuple(slice(3, 3 + v) for v in cfg["n"])
     phi0 = cfg["phi"][inner]
     finals = {}
-    for prec, key in ((8, "fp64"), (4, "fp32")):
+    for prec, key, extra in forms:
         dtype = np.float64 if prec == 8 else np.float32
         ws = integrator.Workspace(gb, prec)
+        if extra:
+            ws.set_fp64_policy(integrator.FP64_SIGN | integrator.STOCH_ROUND | extra)
         d = gpu.DeviceArray.from_host(cfg["phi"].astype(dtype))
         ms, steps, t = deformation_run(ws, d, fb, cfg, timer)
         finals[key] = d.download()[inner].astype(np.float64)
@@ -912,11 +919,12 @@ def run_config3(lib, pg, world, n_window=512, window=100, n_full=256):
              "value": n_full ** 3 * steps / (ms / 1e3), "unit": UNIT},
             vs_initial=interface_errors(finals[key], phi0, cfg["dx"][0]))
         del d, ws
-    diff = np.abs(finals["fp32"] - finals["fp64"])
     band = np.abs(finals["fp64"]) < 5 * cfg["dx"][0]
-    res["reversal_%d_fp32" % n_full]["error_vs_fp64"] = {
-        "max_abs": float(diff.max()), "l1_mean": float(diff.mean()),
-        "max_abs_band_5dx": float(diff[band].max())}
+    for key in ("fp32", "fp32band"):
+        diff = np.abs(finals[key] - finals["fp64"])
+        res["reversal_%d_%s" % (n_full, key)]["error_vs_fp64"] = {
+            "max_abs": float(diff.max()), "l1_mean": float(diff.mean()),
+            "max_abs_band_5dx": float(diff[band].max())}
     return res
 
 

@@ -562,10 +562,25 @@ int lsmgpu_workspace_set_bc(lsmgpu_workspace *ws, unsigned linear_faces_mask);
  * factor 1e3 (kinks), bit 1 evaluates the smoothed sign of the
  * reinitialization RHS in FP64, bit 2 forms each Runge-Kutta combination in
  * FP64 and rounds it to FP32 stochastically (unbiased; seeded per launch
- * from a per-workspace counter, so a run is reproducible).  Default 6.  No
- * reference counterpart: the reference's single-precision build is FP32
+ * from a per-workspace counter, so a run is reproducible), bit 3 computes
+ * the tiles near the interface in FP64 (the band form below).  Default 6.
+ * No reference counterpart: the reference's single-precision build is FP32
  * throughout. */
 int lsmgpu_workspace_set_fp64_policy(lsmgpu_workspace *ws, int policy);
+/* The band form (policy bit 3; lsmgpu_deformation_tvdrk3 in fast mode; no
+ * effect elsewhere): the workspace keeps FP64 copies of phi and of its stage
+ * buffers.  Before each step the stage tiles (32 x 8 x 16 cells) that hold a
+ * cell with |phi| < cells * min(dx), and their 26 neighbours, are flagged;
+ * each stage computes the flagged tiles in FP64 from the FP64 copies (on a
+ * second, high-priority stream, beside the FP32 launch) and the others in
+ * FP32, and writes every cell in both precisions, so phi stays the
+ * FP32 array the caller owns (the FP64 results rounded to nearest there).
+ * dt is that of the FP64 velocity.  The copy of phi persists between calls:
+ * a cell whose copy no longer rounds to the caller's value (first call, or
+ * phi changed by the caller) is reloaded from phi.  Default 16 cells; a large
+ * value puts every tile in FP64 (the result is then the FP64 run's, rounded
+ * to FP32).  No reference counterpart. */
+int lsmgpu_workspace_set_fp64_band(lsmgpu_workspace *ws, double cells);
 int lsmgpu_workspace_set_time(lsmgpu_workspace *ws, double t);
 /* waits for the stream; t and the dt of the last step */
 int lsmgpu_workspace_get_time(lsmgpu_workspace *ws, double *t,

@@ -60,6 +60,18 @@ struct lsmgpu_workspace {
   int npart = 0;
   unsigned bc_mask = 0x3fu;
   int fp64_policy = kFp64Sign | kStochRound;  // FP32 workspaces only
+  // FP64 band form (kFp64Band): FP64 copies of phi, phi^(1) and phi^(2)
+  // (created on first use), the per-tile flags (those within band_cells
+  // cells of the interface, then the same widened by one tile), and the
+  // band half-width in cells
+  double* band64[3] = {nullptr, nullptr, nullptr};
+  unsigned char* band_flags = nullptr;
+  int band_tiles = 0;
+  double band_cells = 16.0;
+  // the stream of the FP64 tiles' launches (high priority, so that their
+  // blocks are placed before the FP32 launch's), and its fork/join events
+  cudaStream_t band_stream = nullptr;
+  cudaEvent_t band_ev[2] = {nullptr, nullptr};
   unsigned sr_launches = 0;  // stochastic-rounding seeds drawn so far
   unsigned long long steps = 0;
 };
@@ -202,6 +214,55 @@ __global__ void k_adv_partials(const T* vx, const T* vy, const T* vz, Box gb,
 
 constexpr int kAdvRedBlocks = 1184;
 
+// FP64 band form.  The FP64 copy of the caller's FP32 level set is kept
+// between calls; a cell whose copy no longer rounds to the caller's value
+// (first use, or phi changed by the caller) is reloaded from phi.
+__global__ void k_band_sync(const float* phi, double* copy, long n) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+       t += (long)gridDim.x * blockDim.x) {
+    const float v = phi[t];
+    if (!((float)copy[t] == v)) copy[t] = (double)v;
+  }
+}
+
+// flag[tile] = 1 when some cell of the tile (stage tiles of kStageTX x
+// kStageTY x kStageTZ cells, numbered x fastest) has |phi| < thr
+__global__ void __launch_bounds__(256) k_band_tiles(const float* phi, Box gb, FillBox fb,
+                                                    float thr, unsigned char* flag) {
+  const int x0 = fb.lo[0] + blockIdx.x * kStageTX, y0 = fb.lo[1] + blockIdx.y * kStageTY,
+            z0 = fb.lo[2] + blockIdx.z * kStageTZ;
+  const int x = x0 + (threadIdx.x & (kStageTX - 1));
+  int near = 0;
+  if (x <= fb.hi[0]) {
+    for (int r = threadIdx.x / kStageTX; r < kStageTY * kStageTZ; r += blockDim.x / kStageTX) {
+      const int y = y0 + r % kStageTY, z = z0 + r / kStageTY;
+      if (y > fb.hi[1] || z > fb.hi[2]) continue;
+      const long o = (long)(x - gb.lo[0]) + gb.sy() * (y - gb.lo[1]) + gb.sz() * (z - gb.lo[2]);
+      near |= fabsf(phi[o]) < thr;
+    }
+  }
+  near = __syncthreads_or(near);
+  if (threadIdx.x == 0)
+    flag[blockIdx.x + gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z)] =
+        (unsigned char)(near != 0);
+}
+
+// out[tile] = 1 when the tile or one of its 26 neighbours has in[] = 1
+__global__ void k_band_widen(const unsigned char* in, unsigned char* out, int gx, int gy,
+                             int gz) {
+  const long n = (long)gx * gy * gz;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n;
+       t += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(t % gx), y = (int)((t / gx) % gy), z = (int)(t / ((long)gx * gy));
+    unsigned char f = 0;
+    for (int c = max(z - 1, 0); c <= min(z + 1, gz - 1); c++)
+      for (int b = max(y - 1, 0); b <= min(y + 1, gy - 1); b++)
+        for (int a = max(x - 1, 0); a <= min(x + 1, gx - 1); a++)
+          f |= in[a + (long)gx * (b + (long)gy * c)];
+    out[t] = f;
+  }
+}
+
 // A boundary mask (stage.cuh: bit f linear, 8+f copy, 16+f periodic) is
 // usable by the multi-step drivers when every face has exactly one kind and
 // periodic faces come in lo/hi pairs.
@@ -249,6 +310,76 @@ cudaError_t stage(int kind, int prec, StageArgs a, cudaStream_t st,
   a.sr_seed = next_sr_seed(ws);
   return fp_mode() == LSMGPU_FP_FAST ? launch_stage_fast(kind, prec, a, st)
                                      : launch_stage_strict(kind, prec, a, st);
+}
+
+// FP64 band form: the FP64 copies and flag arrays for fill box f, and the
+// FP64 copy of phi brought in line with the caller's phi
+bool band_setup(lsmgpu_workspace* ws, const void* phi, const FillBox& f, cudaStream_t st,
+                const char* R) {
+  const size_t bytes64 = (size_t)ws->gb.count() * sizeof(double);
+  for (int q = 0; q < 3; q++) {
+    if (ws->band64[q]) continue;
+    if (!(ws->band64[q] = (double*)ws_alloc(bytes64, R))) return false;
+    // the copy of phi starts as NaN, so that k_band_sync loads every cell
+    if (!cuda_ok(cudaMemsetAsync(ws->band64[q], q == 0 ? 0xff : 0, bytes64, st), R))
+      return false;
+  }
+  if (!ws->band_stream) {
+    int lo = 0, hi = 0;
+    if (!cuda_ok(cudaDeviceGetStreamPriorityRange(&lo, &hi), R) ||
+        !cuda_ok(cudaStreamCreateWithPriority(&ws->band_stream, cudaStreamNonBlocking, hi), R) ||
+        !cuda_ok(cudaEventCreateWithFlags(&ws->band_ev[0], cudaEventDisableTiming), R) ||
+        !cuda_ok(cudaEventCreateWithFlags(&ws->band_ev[1], cudaEventDisableTiming), R))
+      return false;
+  }
+  const int tiles = stage_blocks(f);
+  if (ws->band_tiles < tiles) {
+    if (ws->band_flags) cudaFree(ws->band_flags);
+    ws->band_tiles = 0;
+    if (!(ws->band_flags = (unsigned char*)ws_alloc(2 * (size_t)tiles, R))) return false;
+    ws->band_tiles = tiles;
+  }
+  k_band_sync<<<4 * 148, 256, 0, st>>>((const float*)phi, ws->band64[0], ws->gb.count());
+  ++launch_counter();
+  return cuda_ok(cudaGetLastError(), R);
+}
+
+// the tiles of fill box f computed in FP64 this step: within band_cells cells
+// (|phi| < band_cells * min dx) of the interface, widened by one tile
+void band_flags(lsmgpu_workspace* ws, const void* phi, const FillBox& f, const double dx[3],
+                cudaStream_t st) {
+  const dim3 tg((f.n(0) + kStageTX - 1) / kStageTX, (f.n(1) + kStageTY - 1) / kStageTY,
+                (f.n(2) + kStageTZ - 1) / kStageTZ);
+  const int tiles = (int)(tg.x * tg.y * tg.z);
+  double mn = dx[0] < dx[1] ? dx[0] : dx[1];
+  mn = mn < dx[2] ? mn : dx[2];
+  k_band_tiles<<<tg, 256, 0, st>>>((const float*)phi, ws->gb, f, (float)(ws->band_cells * mn),
+                                   ws->band_flags);
+  k_band_widen<<<(tiles + 255) / 256, 256, 0, st>>>(ws->band_flags, ws->band_flags + tiles,
+                                                     (int)tg.x, (int)tg.y, (int)tg.z);
+  launch_counter() += 2;
+}
+
+// one stage in the FP64 band form: a names the FP32 arrays (phi or the
+// workspace's), the FP64 launch takes their copies
+cudaError_t band_stage(int kind, lsmgpu_workspace* ws, const void* phi, StageArgs a,
+                       cudaStream_t st) {
+  auto copy_of = [&](const void* p) -> double* {
+    if (p == phi) return ws->band64[0];
+    if (p == ws->phi1) return ws->band64[1];
+    if (p == ws->phi2) return ws->band64[2];
+    return nullptr;
+  };
+  a.sr_seed = next_sr_seed(ws);
+  StageArgs b = a;
+  b.out = copy_of(a.out);
+  b.phi_s = copy_of(a.phi_s);
+  b.phi_n = copy_of(a.phi_n);
+  b.fp64_policy = 0;
+  b.sr_seed = 0u;
+  if (!b.out || !b.phi_s || !b.phi_n) return cudaErrorInvalidValue;
+  return launch_stage_band(kind, a, b, ws->band_flags + stage_blocks(a.fb), st,
+                           ws->band_stream, ws->band_ev);
 }
 
 StageArgs base_args(lsmgpu_workspace* ws, const FillBox& fb, const double dx[3]) {
@@ -397,8 +528,9 @@ int lsmgpu_workspace_create(lsmgpu_workspace** out, const int gb[6],
 int lsmgpu_workspace_destroy(lsmgpu_workspace* ws) {
   if (!ws) return LSMGPU_SUCCESS;
   if (ws->host_pending) lsmgpu_workspace_sync(ws);
-  void* ps[] = {ws->phi1, ws->phi2, ws->rhs, ws->phi0, ws->defo_tab, ws->scal,
-                ws->partials, ws->dphi, ws->dF[0], ws->dF[1]};
+  void* ps[] = {ws->phi1,      ws->phi2,      ws->rhs,       ws->phi0,      ws->defo_tab,
+                ws->scal,      ws->partials,  ws->dphi,      ws->dF[0],     ws->dF[1],
+                ws->band64[0], ws->band64[1], ws->band64[2], ws->band_flags};
   for (void* p : ps)
     if (p) cudaFree(p);
   for (cudaEvent_t e : ws->slab_ev)
@@ -408,6 +540,9 @@ int lsmgpu_workspace_destroy(lsmgpu_workspace* ws) {
   for (cudaEvent_t e : ws->F_ev)
     if (e) cudaEventDestroy(e);
   if (ws->start_ev) cudaEventDestroy(ws->start_ev);
+  for (cudaEvent_t e : ws->band_ev)
+    if (e) cudaEventDestroy(e);
+  if (ws->band_stream) cudaStreamDestroy(ws->band_stream);
   if (ws->copy_stream) cudaStreamDestroy(ws->copy_stream);
   if (ws->copy_stream_out) cudaStreamDestroy(ws->copy_stream_out);
   delete ws;
@@ -448,13 +583,25 @@ int lsmgpu_workspace_set_bc(lsmgpu_workspace* ws, unsigned linear_faces_mask) {
 
 int lsmgpu_workspace_set_fp64_policy(lsmgpu_workspace* ws, int policy) {
   // bit 0: WENO5 kink stencils in FP64; bit 1: reinitialization sign in FP64;
-  // bit 2: stochastic rounding of the FP32 stage outputs
+  // bit 2: stochastic rounding of the FP32 stage outputs; bit 3: the tiles
+  // near the interface in FP64 (deformation driver, fast mode)
   if (!ws_ok(ws, "lsmgpu_workspace_set_fp64_policy")) return LSMGPU_ERR_NULL_POINTER;
-  if (policy & ~(kFp64Kinks | kFp64Sign | kStochRound)) {
+  if (policy & ~(kFp64Kinks | kFp64Sign | kStochRound | kFp64Band)) {
     set_error(LSMGPU_ERR_INVALID_VALUE, "lsmgpu_workspace_set_fp64_policy: unknown bits");
     return LSMGPU_ERR_INVALID_VALUE;
   }
   ws->fp64_policy = policy;
+  return LSMGPU_SUCCESS;
+}
+
+int lsmgpu_workspace_set_fp64_band(lsmgpu_workspace* ws, double cells) {
+  if (!ws_ok(ws, "lsmgpu_workspace_set_fp64_band")) return LSMGPU_ERR_NULL_POINTER;
+  if (!(cells >= 0.0)) {
+    set_error(LSMGPU_ERR_INVALID_VALUE,
+              "lsmgpu_workspace_set_fp64_band: the band half-width is a number of cells >= 0");
+    return LSMGPU_ERR_INVALID_VALUE;
+  }
+  ws->band_cells = cells;
   return LSMGPU_SUCCESS;
 }
 
@@ -655,11 +802,21 @@ int lsmgpu_deformation_tvdrk3(lsmgpu_workspace* ws, void* phi, const int fb[6],
   k_deform_tables<<<(nt + 127) / 128, 128, 0, st>>>(ws->defo_tab, f, x_lo[0], x_lo[1],
                                                     x_lo[2], dx[0], dx[1], dx[2]);
   ++launch_counter();
-  const double tiny = ws->prec == 8 ? Consts<double>::tiny : (double)Consts<float>::tiny;
+  // FP64 band form: the tiles near the interface in FP64, with the dt of the
+  // FP64 velocity, as an FP64 workspace computes them
+  const bool band = ws->prec == 4 && (ws->fp64_policy & kFp64Band) &&
+                    fp_mode() == LSMGPU_FP_FAST;
+  if (band && !band_setup(ws, phi, f, st, R)) return lsmgpu_peek_last_error();
+  const double tiny =
+      ws->prec == 8 || band ? Consts<double>::tiny : (double)Consts<float>::tiny;
   const double inv[3] = {1.0 / dx[0], 1.0 / dx[1], 1.0 / dx[2]};
+  auto run = [&](StageArgs& a) {
+    return band ? band_stage(kStageDeformation, ws, phi, a, st)
+                : stage(kStageDeformation, ws->prec, a, st, ws);
+  };
   for (int s = 0; s < nsteps; s++) {
     // dt from the field at t (the stage-1 field)
-    if (ws->prec == 8)
+    if (ws->prec == 8 || band)
       k_deform_partials<double><<<kAdvRedBlocks, 256, 0, st>>>(
           ws->defo_tab, f, ws->scal, period, inv[0], inv[1], inv[2], ws->partials);
     else
@@ -674,16 +831,17 @@ int lsmgpu_deformation_tvdrk3(lsmgpu_workspace* ws, void* phi, const int fb[6],
     a.defo_off[0] = 0;
     a.defo_off[1] = 2 * f.n(0);
     a.defo_off[2] = 2 * (f.n(0) + f.n(1));
+    if (band) band_flags(ws, phi, f, dx, st);
     // velocity at t, t + dt, t + dt/2 for the three stages
     a.g_dev = ws->scal + kG0;
     a.out = ws->phi1; a.phi_s = phi; a.phi_n = phi; a.rk_kind = 1;
-    if (!cuda_ok(stage(kStageDeformation, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(run(a), R)) return LSMGPU_ERR_CUDA;
     a.g_dev = ws->scal + kG0 + 1;
     a.out = ws->phi2; a.phi_s = ws->phi1; a.rk_kind = 32;
-    if (!cuda_ok(stage(kStageDeformation, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(run(a), R)) return LSMGPU_ERR_CUDA;
     a.g_dev = ws->scal + kG0 + 2;
     a.out = phi; a.phi_s = ws->phi2; a.rk_kind = 33;
-    if (!cuda_ok(stage(kStageDeformation, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(run(a), R)) return LSMGPU_ERR_CUDA;
     k_advance_t<<<1, 1, 0, st>>>(ws->scal);
     ++launch_counter();
     ws->steps++;

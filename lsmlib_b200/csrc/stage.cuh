@@ -66,6 +66,14 @@ struct StageParams {
   const double* defo_tab;
   int defo_off[3];
   const double* g_dev;
+  // FP64 band of an FP32 workspace (k_stage_pairs_up): tile_fp64[tile], tiles
+  // numbered in launch order, says which precision computes a tile; such a
+  // launch computes only the tiles whose flag equals tile_want, and writes
+  // each output cell also into out_alt, the same stage output in the other
+  // precision (FP32 rounded to nearest, or FP64 widened exactly)
+  const unsigned char* tile_fp64 = nullptr;
+  unsigned tile_want = 0u;
+  void* out_alt = nullptr;
 };
 
 // LeVeque's 3D deformation velocity of a cell from its sine values and g,
@@ -89,7 +97,17 @@ __device__ __forceinline__ void deformation_velocity(const DeformSines& s, doubl
 // kFp64Sign evaluates the smoothed sign of the reinitialization RHS in FP64;
 // kStochRound forms the Runge-Kutta combination in FP64 and rounds it to
 // FP32 stochastically (sr_float).
-constexpr int kFp64Kinks = 1, kFp64Sign = 2, kStochRound = 4;
+// kFp64Band (drivers of an FP32 workspace in fast mode) computes the tiles
+// near the interface in FP64 from FP64 copies of the stage arrays.
+constexpr int kFp64Kinks = 1, kFp64Sign = 2, kStochRound = 4, kFp64Band = 8;
+
+// the other precision's copy of a stage output (FP64 band form)
+__device__ __forceinline__ void store_alt(void* alt, long o, double v) {
+  static_cast<float*>(alt)[o] = (float)v;
+}
+__device__ __forceinline__ void store_alt(void* alt, long o, float v) {
+  static_cast<double*>(alt)[o] = (double)v;
+}
 
 template <typename T>
 __device__ __forceinline__ T rk_combine(int kind, T uc, T us, T r, T dt) {
@@ -909,7 +927,8 @@ __device__ __forceinline__ double stage_tile_pairs(const StageParams<T>& p, int 
 // of stage_tile (weno_upwind_side and the same RHS and RK update), but for
 // FP32 without the FP64 kink recomputation, where the two cells' sides of
 // an axis are one packed FP32x2 evaluation (weno5_side2).
-template <typename T, int KIND, bool K64, int TX, int TY, int TZ>
+// BAND: the FP64 band form (out_alt written as well).
+template <typename T, int KIND, bool K64, int TX, int TY, int TZ, bool BAND = false>
 __device__ __forceinline__ void stage_tile_pairs_up(const StageParams<T>& p, int bx, int by,
                                                     int bz, T (*tile)[TY + 6][TX + 8]) {
   using T2 = typename Pair2<T>::type;
@@ -1074,7 +1093,9 @@ __device__ __forceinline__ void stage_tile_pairs_up(const StageParams<T>& p, int
     for (int c = 0; c < 2; c++) {
       if (c == 1 && !act1) break;
       const T L = T(0) - (a[c][0] * g[c][0] + a[c][1] * g[c][1] + a[c][2] * g[c][2]);
-      p.out[o0 + c] = stage_out(p, o0 + c, uc[c], c ? w1[3] : w0[3], L, dt);
+      const T v = stage_out(p, o0 + c, uc[c], c ? w1[3] : w0[3], L, dt);
+      p.out[o0 + c] = v;
+      if constexpr (BAND) store_alt(p.out_alt, o0 + c, v);
     }
   }
 }
@@ -1165,13 +1186,19 @@ k_stage_pairs(StageParams<T> p) {
 }
 
 // The one-sided kinds, two cells per thread (stage_tile_pairs_up); every
-// ghost cell the stencils reach is read as stored.
-template <typename T, int KIND, bool K64, int TX, int TY, int TZ>
+// ghost cell the stencils reach is read as stored.  BAND: the FP64 band form
+// (the tiles whose tile_fp64 flag is tile_want, out_alt written as well).
+template <typename T, int KIND, bool K64, int TX, int TY, int TZ, bool BAND = false>
 __global__ void __launch_bounds__(TX / 2 * TY, LSMGPU_PAIR_MIN_BLOCKS)
 k_stage_pairs_up(StageParams<T> p) {
   __shared__ __align__(16) T tile[2][TY + 6][TX + 8];
-  stage_tile_pairs_up<T, KIND, K64, TX, TY, TZ>(p, (int)blockIdx.x, (int)blockIdx.y,
-                                               (int)blockIdx.z, tile);
+  if constexpr (BAND) {
+    if (p.tile_fp64[blockIdx.x + gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z)] !=
+        p.tile_want)
+      return;
+  }
+  stage_tile_pairs_up<T, KIND, K64, TX, TY, TZ, BAND>(p, (int)blockIdx.x, (int)blockIdx.y,
+                                                     (int)blockIdx.z, tile);
 }
 
 // The face ghost cells of phi that the stencils of fill-box cells in planes

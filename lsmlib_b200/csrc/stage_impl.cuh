@@ -149,7 +149,66 @@ cudaError_t launch_t(int kind, const StageArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+#ifdef STAGE_BAND_FN
+// the FP64 band form of one upwind kind: FP32 launch for the tiles flagged 0,
+// FP64 launch for those flagged 1, each also writing the other precision
+template <int KIND>
+cudaError_t band_kind(dim3 grid, const StageArgs& a32, const StageArgs& a64,
+                      const unsigned char* tile_fp64, cudaStream_t st, cudaStream_t side,
+                      cudaEvent_t ev[2]) {
+  constexpr int TX = kStageTX, TY = kStageTY, TZ = kStageTZ;
+  static_assert(UsePairsUp<float, KIND, STAGE_FAST, TX>::value &&
+                    UsePairsUp<double, KIND, STAGE_FAST, TX>::value,
+                "the band form runs the two-cells-per-thread upwind kernels");
+  if (!pairs_apply(a32) || !pairs_apply(a64)) return cudaErrorNotSupported;
+  StageParams<float> q32 = to_params<float>(a32);
+  StageParams<double> q64 = to_params<double>(a64);
+  if (a32.bc_mask != 0u) {
+    launch_face_ghosts<float>(a32, st);
+    launch_face_ghosts<double>(a64, st);
+    q32.bc_mask = q64.bc_mask = 0u;
+  }
+  q32.tile_fp64 = q64.tile_fp64 = tile_fp64;
+  q32.tile_want = 0u;
+  q64.tile_want = 1u;
+  q32.out_alt = a64.out;
+  q64.out_alt = a32.out;
+  const dim3 blk(TX / 2, TY, 1);
+  cudaError_t e;
+  if ((e = cudaEventRecord(ev[0], st)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(side, ev[0], 0)) != cudaSuccess)
+    return e;
+  k_stage_pairs_up<double, KIND, false, TX, TY, TZ, true><<<grid, blk, 0, side>>>(q64);
+  if (q32.fp64_policy & kFp64Kinks)
+    k_stage_pairs_up<float, KIND, true, TX, TY, TZ, true><<<grid, blk, 0, st>>>(q32);
+  else
+    k_stage_pairs_up<float, KIND, false, TX, TY, TZ, true><<<grid, blk, 0, st>>>(q32);
+  launch_counter() += 2;
+  if ((e = cudaEventRecord(ev[1], side)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(st, ev[1], 0)) != cudaSuccess)
+    return e;
+  return cudaGetLastError();
+}
+#endif
+
 }  // namespace
+
+#ifdef STAGE_BAND_FN
+cudaError_t STAGE_BAND_FN(int kind, const StageArgs& a32, const StageArgs& a64,
+                          const unsigned char* tile_fp64, cudaStream_t st, cudaStream_t side,
+                          cudaEvent_t ev[2]) {
+  constexpr int TX = kStageTX, TY = kStageTY, TZ = kStageTZ;
+  const FillBox& fb = a32.fb;
+  if (fb.n(0) < 1 || fb.n(1) < 1 || fb.n(2) < 1) return cudaSuccess;
+  const dim3 grid((fb.n(0) + TX - 1) / TX, (fb.n(1) + TY - 1) / TY,
+                  (fb.n(2) + TZ - 1) / TZ);
+  switch (kind) {
+    case kStageDeformation:
+      return band_kind<kStageDeformation>(grid, a32, a64, tile_fp64, st, side, ev);
+    default: return cudaErrorInvalidValue;
+  }
+}
+#endif
 
 cudaError_t STAGE_LAUNCH_FN(int kind, int prec, const StageArgs& a,
                             cudaStream_t st) {

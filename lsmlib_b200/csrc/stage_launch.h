@@ -56,5 +56,18 @@ cudaError_t launch_stage_strict(int kind, int prec, const StageArgs& a,
                                 cudaStream_t st);
 cudaError_t launch_stage_fast(int kind, int prec, const StageArgs& a,
                               cudaStream_t st);
+// One stage of kStageDeformation (velocity evaluated in the kernel, so both
+// precisions have it) in the FP64 band form, fast arithmetic: a32 and a64 name the same stage over the FP32
+// arrays and their FP64 copies; tile_fp64[tile] (tiles as in stage_blocks,
+// x fastest) = 1 computes the tile in FP64, 0 in FP32.  Both launches write
+// every output cell in both precisions.  cudaErrorNotSupported when the
+// two-cells-per-thread kernels do not apply (arrays of 2^31 or more cells,
+// or boundary values that cannot be stored in the ghost cells).
+// The FP64 launch runs on `side` (forked from st after the ghost fills by
+// event ev[0], joined back by ev[1]), so that the FP64 tiles run beside the
+// FP32 launch instead of after it.
+cudaError_t launch_stage_band(int kind, const StageArgs& a32, const StageArgs& a64,
+                              const unsigned char* tile_fp64, cudaStream_t st,
+                              cudaStream_t side, cudaEvent_t ev[2]);
 
 }  // namespace lsmgpu

@@ -23,8 +23,9 @@ FP_STRICT, FP_FAST = 0, 1
 # boundary masks (per face f = x-lo .. z-hi): linear, copy, periodic
 BC_LINEAR, BC_COPY, BC_PERIODIC = 0x3F, 0x3F << 8, 0x3F << 16
 # FP64 parts of the FP32 form (Workspace.set_fp64_policy): kink stencils in
-# FP64, reinitialization sign in FP64, stochastic rounding of stage outputs
-FP64_KINKS, FP64_SIGN, STOCH_ROUND = 1, 2, 4
+# FP64, reinitialization sign in FP64, stochastic rounding of stage outputs,
+# the tiles near the interface in FP64 (deformation driver, fast mode)
+FP64_KINKS, FP64_SIGN, STOCH_ROUND, FP64_BAND = 1, 2, 4, 8
 
 
 def set_fp_mode(mode):
@@ -69,9 +70,15 @@ class Workspace:
         gpu.check_rc(gpu.load().lsmgpu_workspace_sync(self.h), "workspace_sync")
 
     def set_fp64_policy(self, policy):
-        """FP32 workspaces: FP64_KINKS | FP64_SIGN | STOCH_ROUND."""
+        """FP32 workspaces: FP64_KINKS | FP64_SIGN | STOCH_ROUND | FP64_BAND."""
         gpu.check_rc(gpu.load().lsmgpu_workspace_set_fp64_policy(self.h, int(policy)),
                      "set_fp64_policy")
+
+    def set_fp64_band(self, cells):
+        """Half-width in cells of the FP64 band (FP64_BAND): tiles holding a
+        cell with |phi| < cells * min(dx), and their neighbours, run in FP64."""
+        gpu.check_rc(gpu.load().lsmgpu_workspace_set_fp64_band(self.h, float(cells)),
+                     "set_fp64_band")
 
     def set_time(self, t):
         gpu.check_rc(gpu.load().lsmgpu_workspace_set_time(self.h, float(t)), "set_time")
