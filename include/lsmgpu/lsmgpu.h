@@ -570,7 +570,8 @@ int lsmgpu_workspace_set_fp64_policy(lsmgpu_workspace *ws, int policy);
 /* The band form (policy bit 3; lsmgpu_deformation_tvdrk3 in fast mode; no
  * effect elsewhere): the workspace keeps FP64 copies of phi and of its stage
  * buffers.  Before each step the stage tiles (32 x 8 x 16 cells) that hold a
- * cell with |phi| < cells * min(dx), and their 26 neighbours, are flagged;
+ * cell with |phi| < cells * min(dx) are flagged, with their 26 neighbours
+ * when widen is 1;
  * each stage computes the flagged tiles in FP64 from the FP64 copies (on a
  * second, high-priority stream, beside the FP32 launch) and the others in
  * FP32, and writes every cell in both precisions, so phi stays the
@@ -580,7 +581,7 @@ int lsmgpu_workspace_set_fp64_policy(lsmgpu_workspace *ws, int policy);
  * phi changed by the caller) is reloaded from phi.  Default 16 cells; a large
  * value puts every tile in FP64 (the result is then the FP64 run's, rounded
  * to FP32).  No reference counterpart. */
-int lsmgpu_workspace_set_fp64_band(lsmgpu_workspace *ws, double cells);
+int lsmgpu_workspace_set_fp64_band(lsmgpu_workspace *ws, double cells, int widen);
 int lsmgpu_workspace_set_time(lsmgpu_workspace *ws, double t);
 /* waits for the stream; t and the dt of the last step */
 int lsmgpu_workspace_get_time(lsmgpu_workspace *ws, double *t,

@@ -68,6 +68,7 @@ struct lsmgpu_workspace {
   unsigned char* band_flags = nullptr;
   int band_tiles = 0;
   double band_cells = 16.0;
+  int band_widen = 1;   // tiles added around the flagged ones (0 or 1)
   // the stream of the FP64 tiles' launches (high priority, so that their
   // blocks are placed before the FP32 launch's), and its fork/join events
   cudaStream_t band_stream = nullptr;
@@ -353,11 +354,15 @@ void band_flags(lsmgpu_workspace* ws, const void* phi, const FillBox& f, const d
   const int tiles = (int)(tg.x * tg.y * tg.z);
   double mn = dx[0] < dx[1] ? dx[0] : dx[1];
   mn = mn < dx[2] ? mn : dx[2];
+  // without widening the tiles are flagged straight into the second half
   k_band_tiles<<<tg, 256, 0, st>>>((const float*)phi, ws->gb, f, (float)(ws->band_cells * mn),
-                                   ws->band_flags);
-  k_band_widen<<<(tiles + 255) / 256, 256, 0, st>>>(ws->band_flags, ws->band_flags + tiles,
-                                                     (int)tg.x, (int)tg.y, (int)tg.z);
-  launch_counter() += 2;
+                                   ws->band_flags + (ws->band_widen ? 0 : tiles));
+  ++launch_counter();
+  if (ws->band_widen) {
+    k_band_widen<<<(tiles + 255) / 256, 256, 0, st>>>(ws->band_flags, ws->band_flags + tiles,
+                                                       (int)tg.x, (int)tg.y, (int)tg.z);
+    ++launch_counter();
+  }
 }
 
 // one stage in the FP64 band form: a names the FP32 arrays (phi or the
@@ -594,14 +599,15 @@ int lsmgpu_workspace_set_fp64_policy(lsmgpu_workspace* ws, int policy) {
   return LSMGPU_SUCCESS;
 }
 
-int lsmgpu_workspace_set_fp64_band(lsmgpu_workspace* ws, double cells) {
+int lsmgpu_workspace_set_fp64_band(lsmgpu_workspace* ws, double cells, int widen) {
   if (!ws_ok(ws, "lsmgpu_workspace_set_fp64_band")) return LSMGPU_ERR_NULL_POINTER;
-  if (!(cells >= 0.0)) {
+  if (!(cells >= 0.0) || (widen != 0 && widen != 1)) {
     set_error(LSMGPU_ERR_INVALID_VALUE,
-              "lsmgpu_workspace_set_fp64_band: the band half-width is a number of cells >= 0");
+              "lsmgpu_workspace_set_fp64_band: cells >= 0 and widen 0 or 1");
     return LSMGPU_ERR_INVALID_VALUE;
   }
   ws->band_cells = cells;
+  ws->band_widen = widen;
   return LSMGPU_SUCCESS;
 }
 

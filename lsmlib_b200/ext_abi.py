@@ -18,7 +18,7 @@ SIGNATURES = {
     "lsmgpu_workspace_set_host_async": (I, [P, I]),
     "lsmgpu_workspace_sync": (I, [P]),
     "lsmgpu_workspace_set_fp64_policy": (I, [P, I]),
-    "lsmgpu_workspace_set_fp64_band": (I, [P, D]),
+    "lsmgpu_workspace_set_fp64_band": (I, [P, D, I]),
     "lsmgpu_workspace_set_time": (I, [P, D]),
     "lsmgpu_workspace_get_time": (I, [P, DA, DA]),
     "lsmgpu_workspace_device_scalars": (P, [P]),

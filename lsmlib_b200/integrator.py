@@ -74,10 +74,12 @@ class Workspace:
         gpu.check_rc(gpu.load().lsmgpu_workspace_set_fp64_policy(self.h, int(policy)),
                      "set_fp64_policy")
 
-    def set_fp64_band(self, cells):
+    def set_fp64_band(self, cells, widen=1):
         """Half-width in cells of the FP64 band (FP64_BAND): tiles holding a
-        cell with |phi| < cells * min(dx), and their neighbours, run in FP64."""
-        gpu.check_rc(gpu.load().lsmgpu_workspace_set_fp64_band(self.h, float(cells)),
+        cell with |phi| < cells * min(dx), and their neighbours when widen
+        is 1, run in FP64."""
+        gpu.check_rc(gpu.load().lsmgpu_workspace_set_fp64_band(self.h, float(cells),
+                                                               int(widen)),
                      "set_fp64_band")
 
     def set_time(self, t):
