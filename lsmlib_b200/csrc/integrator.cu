@@ -28,6 +28,9 @@ using namespace lsmgpu;
 #define LSMGPU_HOST_SLABS 4
 #endif
 constexpr int kHostSlabs = LSMGPU_HOST_SLABS;
+// speed buffers of queued host-array calls: up to kMaxSpeedBufs, as many as
+// fit in 1 GiB (at least 2)
+constexpr int kMaxSpeedBufs = 8;
 
 struct lsmgpu_workspace {
   Box gb;
@@ -38,17 +41,24 @@ struct lsmgpu_workspace {
   void* rhs = nullptr;
   void* phi0 = nullptr;
   // lsmgpu_normal_tvdrk3_host: device copies of the host level set and of
-  // the speed (two buffers, alternating between queued calls), the streams
-  // of the slab copies to and from the host, and per slab: copied in, final
-  // stage done, copied out; per speed buffer: last read (created on first
-  // use)
+  // the speed (nspeed buffers, taken in turn by queued calls), the streams
+  // of the slab copies to and from the host and of the queued calls' speed
+  // uploads, and per slab: copied in, final stage done, copied out; per
+  // speed buffer: last read, upload done (created on first use)
   void* dphi = nullptr;
-  void* dF[2] = {nullptr, nullptr};
+  void* dF[kMaxSpeedBufs] = {};
+  int nspeed = 0;
   cudaStream_t copy_stream = nullptr;       // host -> device
   cudaStream_t copy_stream_out = nullptr;   // device -> host
+  cudaStream_t copy_stream_F = nullptr;     // host -> device, queued calls' speed
   cudaEvent_t slab_ev[2 * kHostSlabs] = {};  // [q] in, [kHostSlabs + q] final stage
   cudaEvent_t out_ev[kHostSlabs] = {};
-  cudaEvent_t F_ev[2] = {};
+  cudaEvent_t F_ev[kMaxSpeedBufs] = {};
+  cudaEvent_t Fin_ev[kMaxSpeedBufs] = {};
+  // per call (ring of nspeed): its level set uploaded; and the last queued
+  // call that ran a reinitialization (-1: none)
+  cudaEvent_t up_ev[kMaxSpeedBufs] = {};
+  long long last_reinit_call = -1;
   cudaEvent_t start_ev = nullptr;
   int host_async = 0;       // lsmgpu_workspace_set_host_async
   int host_pending = 0;     // a queued host call has not been waited for
@@ -534,10 +544,17 @@ int lsmgpu_workspace_destroy(lsmgpu_workspace* ws) {
   if (!ws) return LSMGPU_SUCCESS;
   if (ws->host_pending) lsmgpu_workspace_sync(ws);
   void* ps[] = {ws->phi1,      ws->phi2,      ws->rhs,       ws->phi0,      ws->defo_tab,
-                ws->scal,      ws->partials,  ws->dphi,      ws->dF[0],     ws->dF[1],
-                ws->band64[0], ws->band64[1], ws->band64[2], ws->band_flags};
+                ws->scal,      ws->partials,  ws->dphi,      ws->band64[0], ws->band64[1],
+                ws->band64[2], ws->band_flags};
   for (void* p : ps)
     if (p) cudaFree(p);
+  for (void* p : ws->dF)
+    if (p) cudaFree(p);
+  for (cudaEvent_t e : ws->Fin_ev)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : ws->up_ev)
+    if (e) cudaEventDestroy(e);
+  if (ws->copy_stream_F) cudaStreamDestroy(ws->copy_stream_F);
   for (cudaEvent_t e : ws->slab_ev)
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : ws->out_ev)
@@ -572,7 +589,8 @@ int lsmgpu_workspace_sync(lsmgpu_workspace* ws) {
   // the copies back to the host are the last work of a host call; the
   // speed buffers' events close its kernels
   if (!cuda_ok(cudaStreamSynchronize(ws->copy_stream_out), R) ||
-      !cuda_ok(cudaStreamSynchronize(ws->copy_stream), R))
+      !cuda_ok(cudaStreamSynchronize(ws->copy_stream), R) ||
+      !cuda_ok(cudaStreamSynchronize(ws->copy_stream_F), R))
     return LSMGPU_ERR_CUDA;
   for (cudaEvent_t e : ws->F_ev)
     if (!cuda_ok(cudaEventSynchronize(e), R)) return LSMGPU_ERR_CUDA;
@@ -933,8 +951,17 @@ int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
         !cuda_ok(cudaMalloc(&ws->dF[0], ws->bytes), R) ||
         !cuda_ok(cudaStreamCreateWithFlags(&ws->copy_stream, cudaStreamNonBlocking), R) ||
         !cuda_ok(cudaStreamCreateWithFlags(&ws->copy_stream_out, cudaStreamNonBlocking), R) ||
+        !cuda_ok(cudaStreamCreateWithFlags(&ws->copy_stream_F, cudaStreamNonBlocking), R) ||
         !cuda_ok(cudaEventCreateWithFlags(&ws->start_ev, cudaEventDisableTiming), R))
       return LSMGPU_ERR_CUDA;
+    const size_t fit = ((size_t)1 << 30) / ws->bytes;
+    ws->nspeed = fit < 2 ? 2 : fit > (size_t)kMaxSpeedBufs ? kMaxSpeedBufs : (int)fit;
+    for (cudaEvent_t& e : ws->Fin_ev)
+      if (!cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), R))
+        return LSMGPU_ERR_CUDA;
+    for (cudaEvent_t& e : ws->up_ev)
+      if (!cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), R))
+        return LSMGPU_ERR_CUDA;
     for (cudaEvent_t& e : ws->slab_ev)
       if (!cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), R))
         return LSMGPU_ERR_CUDA;
@@ -945,11 +972,14 @@ int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
       if (!cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), R))
         return LSMGPU_ERR_CUDA;
   }
-  // queued calls alternate between the two speed buffers
-  const int fbuf = ws->host_async ? (int)(ws->host_calls & 1u) : 0;
+  // queued calls take the speed buffers in turn and upload the speed on a
+  // stream of its own (see the anchor below)
+  const unsigned call = ws->host_calls;
+  const int fbuf = ws->host_async ? (int)(call % (unsigned)ws->nspeed) : 0;
   if (!ws->dF[fbuf] && !cuda_ok(cudaMalloc(&ws->dF[fbuf], ws->bytes), R)) return LSMGPU_ERR_CUDA;
   void* dF = ws->dF[fbuf];
   cudaStream_t ci = ws->copy_stream, co = ws->copy_stream_out;
+  cudaStream_t cf = ws->host_async ? ws->copy_stream_F : ci;
   const Box& gb = ws->gb;
   const size_t esz = (size_t)ws->prec;
   const size_t plane = (size_t)gb.sz() * esz;
@@ -978,24 +1008,38 @@ int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
   };
   // host -> device.  After a waited-for call: behind all the work queued on
   // st.  Behind a queued call: the speed behind the last kernels that read
-  // this buffer (two calls back), each phi slab behind that call's copy of
-  // the slab back to the host (which followed every kernel writing it).
+  // this buffer (nspeed calls back), each phi slab behind that call's copy
+  // of the slab back to the host (which followed every kernel writing it).
   const bool pending = ws->host_pending != 0;
   if (!pending) {
     if (!cuda_ok(cudaEventRecord(ws->start_ev, st), R) ||
-        !cuda_ok(cudaStreamWaitEvent(ci, ws->start_ev, 0), R))
+        !cuda_ok(cudaStreamWaitEvent(ci, ws->start_ev, 0), R) ||
+        (cf != ci && !cuda_ok(cudaStreamWaitEvent(cf, ws->start_ev, 0), R)))
       return LSMGPU_ERR_CUDA;
-  } else if (ws->host_calls >= 2 && !cuda_ok(cudaStreamWaitEvent(ci, ws->F_ev[fbuf], 0), R)) {
-    return LSMGPU_ERR_CUDA;
+  } else {
+    // The speed of a queued call crosses the link after the previous call's
+    // level set, so that it never delays a level-set upload (the next step
+    // waits for it).  Behind a call that runs a reinitialization, the link
+    // is idle while the level set is reinitialized: the speeds of the next
+    // nspeed - 1 calls go right after that call's level set.
+    const long long r = ws->last_reinit_call;
+    const long long anchor = r >= 0 && (long long)call - r < ws->nspeed ? r : (long long)call - 1;
+    if (!cuda_ok(cudaStreamWaitEvent(cf, ws->F_ev[fbuf], 0), R) ||
+        (cf != ci && !cuda_ok(cudaStreamWaitEvent(cf, ws->up_ev[anchor % ws->nspeed], 0), R)))
+      return LSMGPU_ERR_CUDA;
   }
   for (int q = 0; q < ns; q++)
-    if (!cuda_ok(copy(dF, F, q, cudaMemcpyHostToDevice, ci), R)) return LSMGPU_ERR_CUDA;
+    if (!cuda_ok(copy(dF, F, q, cudaMemcpyHostToDevice, cf), R)) return LSMGPU_ERR_CUDA;
+  if (cf != ci && (!cuda_ok(cudaEventRecord(ws->Fin_ev[fbuf], cf), R) ||
+                   !cuda_ok(cudaStreamWaitEvent(st, ws->Fin_ev[fbuf], 0), R)))
+    return LSMGPU_ERR_CUDA;
   for (int q = 0; q < ns; q++) {
     if ((pending && !cuda_ok(cudaStreamWaitEvent(ci, ws->out_ev[q], 0), R)) ||
         !cuda_ok(copy(ws->dphi, phi, q, cudaMemcpyHostToDevice, ci), R) ||
         !cuda_ok(cudaEventRecord(ws->slab_ev[q], ci), R))
       return LSMGPU_ERR_CUDA;
   }
+  if (!cuda_ok(cudaEventRecord(ws->up_ev[call % ws->nspeed], ci), R)) return LSMGPU_ERR_CUDA;
   const double tiny = ws->prec == 8 ? Consts<double>::tiny : (double)Consts<float>::tiny;
   const int nblk = stage_blocks(f);
   void* dphi = ws->dphi;
@@ -1032,6 +1076,7 @@ int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
     if (!cuda_ok(stage(kStageNormal, ws->prec, a, st, ws), R)) return LSMGPU_ERR_CUDA;
     a.out = dphi; a.phi_s = ws->phi2; a.rk_kind = 33;
     const bool reinit_now = reinit_interval > 0 && (step0 + s + 1) % reinit_interval == 0;
+    if (reinit_now && reinit_iters > 0) ws->last_reinit_call = call;
     if (s == nsteps - 1 && !reinit_now) {
       // the final stage slab by slab, each slab's planes copied back at once
       for (int q = 0; q < ns; q++) {
