@@ -929,10 +929,11 @@ int lsmgpu_normal_tvdrk3(lsmgpu_workspace* ws, void* phi, const void* F,
 // last step's final stage runs slab by slab, each slab copied back while the
 // next is computed.  By default the call returns when phi is back in host
 // memory.  With lsmgpu_workspace_set_host_async(ws, 1) it returns once its
-// work is queued, and successive calls overlap: the speed goes to the other
-// of two device buffers while the previous call still computes, and each
+// work is queued, and successive calls overlap: the speed goes to the next
+// of nspeed device buffers while the previous call still computes, and each
 // slab of phi is copied in as soon as the previous call's copy of that slab
-// back to the host has landed (copies in and out on two streams).
+// back to the host has landed (copies in, out and of the speed on three
+// streams).
 int lsmgpu_normal_tvdrk3_host(lsmgpu_workspace* ws, void* phi, const void* F,
                               const int fb[6], const double dx[3], double cfl, int nsteps,
                               int step0, int reinit_interval, int reinit_iters,
