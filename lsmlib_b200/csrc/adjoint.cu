@@ -35,7 +35,15 @@ using namespace lsmgpu;
 
 namespace {
 
-constexpr int kTX = 32, kTY = 8, kTZ = 32;
+// tile of k_adjoint_stage: kTX x kTY cells per block, kTZ planes per block
+// (build-time setting).  Short tiles balance the SMs: at 128^3 with two
+// blocks per SM, 32-plane tiles make 256 blocks (108 SMs with two, 40 with
+// one); 8-plane tiles make 1024 (about 7 per SM).  Measured reverse sweep of
+// the 128^3 problem: 207.1 ms (32 planes), 201.9 (16), 200.8 (8).
+#ifndef LSMGPU_ADJ_TZ
+#define LSMGPU_ADJ_TZ 8
+#endif
+constexpr int kTX = 32, kTY = 8, kTZ = LSMGPU_ADJ_TZ;
 
 // ---------------------------------------------------------------------------
 // one-sided WENO5 value and its gradient with respect to v1..v5
