@@ -54,8 +54,8 @@ WORKLOAD = ("256^3 normal-velocity level set (6 spheres, F = 1 + 0.2 sin sin sin
 # DRAM bytes (read + write) per launch and FP64-pipe utilisation of the fused
 # stage kernels on the 256^3 workload, from the ncu capture summarised in
 # profiles/k_stage_pairs_config2_256.md (distinct phi_s and phi^n)
-NCU_TRAFFIC = {"stage_reinit_rk32": 395.0e6, "stage_normal_rk32": 541.1e6}
-NCU_FP64_PIPE = {"stage_reinit_rk32": 63.2, "stage_normal_rk32": 64.0}
+NCU_TRAFFIC = {"stage_reinit_rk32": 394.9e6, "stage_normal_rk32": 541.5e6}
+NCU_FP64_PIPE = {"stage_reinit_rk32": 62.5, "stage_normal_rk32": 63.5}
 # FP64 thread instructions per cell of the same kernels (ncu op counters
 # smsp__sass_thread_inst_executed_op_fp64_pred_on, the same capture's
 # profile command) and the B200's FP64 lanes per SM
