@@ -580,7 +580,9 @@ int lsmgpu_workspace_set_fp64_policy(lsmgpu_workspace *ws, int policy);
  * a cell whose copy no longer rounds to the caller's value (first call, or
  * phi changed by the caller) is reloaded from phi.  Default 16 cells; a large
  * value puts every tile in FP64 (the result is then the FP64 run's, rounded
- * to FP32).  No reference counterpart. */
+ * to FP32).  Ghost boxes of 2^31 cells or more, and axes of fewer than 3
+ * cells with a boundary kind, run the plain FP32 form.  No reference
+ * counterpart. */
 int lsmgpu_workspace_set_fp64_band(lsmgpu_workspace *ws, double cells, int widen);
 int lsmgpu_workspace_set_time(lsmgpu_workspace *ws, double t);
 /* waits for the stream; t and the dt of the last step */

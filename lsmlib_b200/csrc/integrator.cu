@@ -323,6 +323,20 @@ cudaError_t stage(int kind, int prec, StageArgs a, cudaStream_t st,
                                      : launch_stage_strict(kind, prec, a, st);
 }
 
+// The band form runs the two-cells-per-thread upwind kernels, which need
+// offsets below 2^31 and the boundary values stored in the ghost cells
+// (3 domain cells on every axis with a boundary kind); elsewhere the plain
+// FP32 form runs.
+bool band_applies(const lsmgpu_workspace* ws, const FillBox& f) {
+  if (ws->gb.count() >= (1L << 31)) return false;
+  for (int d = 0; d < 3; d++) {
+    const unsigned face_bits = 3u << (2 * d);
+    const bool any = (ws->bc_mask & (face_bits | face_bits << 8 | face_bits << 16)) != 0u;
+    if (any && f.n(d) < 3) return false;
+  }
+  return true;
+}
+
 // FP64 band form: the FP64 copies and flag arrays for fill box f, and the
 // FP64 copy of phi brought in line with the caller's phi
 bool band_setup(lsmgpu_workspace* ws, const void* phi, const FillBox& f, cudaStream_t st,
@@ -829,7 +843,7 @@ int lsmgpu_deformation_tvdrk3(lsmgpu_workspace* ws, void* phi, const int fb[6],
   // FP64 band form: the tiles near the interface in FP64, with the dt of the
   // FP64 velocity, as an FP64 workspace computes them
   const bool band = ws->prec == 4 && (ws->fp64_policy & kFp64Band) &&
-                    fp_mode() == LSMGPU_FP_FAST;
+                    fp_mode() == LSMGPU_FP_FAST && band_applies(ws, f);
   if (band && !band_setup(ws, phi, f, st, R)) return lsmgpu_peek_last_error();
   const double tiny =
       ws->prec == 8 || band ? Consts<double>::tiny : (double)Consts<float>::tiny;

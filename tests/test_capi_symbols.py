@@ -54,3 +54,15 @@ def _load_fresh(path):
         return gpu.load(path)
     finally:
         gpu._lib = saved
+
+
+def test_workspace_calls_reject_a_null_workspace():
+    """The workspace setters check their handle on the host before any CUDA
+    call, so a null workspace is an error code, not a crash."""
+    lib = gpu.load()
+    null = ctypes.c_void_p()
+    err_null = 2   # LSMGPU_ERR_NULL_POINTER
+    assert lib.lsmgpu_workspace_set_fp64_policy(null, 8) == err_null
+    assert lib.lsmgpu_workspace_set_fp64_band(null, 16.0, 1) == err_null
+    assert lib.lsmgpu_workspace_set_host_async(null, 1) == err_null
+    assert lib.lsmgpu_workspace_sync(null) == err_null
