@@ -212,7 +212,12 @@ class Grid:
 class LevelSetIntegrator:
     """TVD-RK3 time stepping of level-set fields on ``grid`` (WENO5 spatial
     derivatives, the reference integrator's call order,
-    LevelSetFunctionIntegrator.cc:1319-1510)."""
+    LevelSetFunctionIntegrator.cc:1319-1510).
+
+    ``fp32_policy`` (torch.float32 only) picks the FP64 parts of the FP32
+    form from lsmlib_b200.integrator's FP64_KINKS, FP64_SIGN, STOCH_ROUND
+    and FP64_BAND (the tiles within 16 cells of the interface in FP64, for
+    ``advance_deformation``)."""
 
     def __init__(self, grid, dtype=torch.float64, boundary="linear", cfl=0.5,
                  reinit_interval=10, reinit_iters=20, use_phi0_for_sgn=False,
