@@ -364,6 +364,7 @@ bool band_setup(lsmgpu_workspace* ws, const void* phi, const FillBox& f, cudaStr
     if (!(ws->band_flags = (unsigned char*)ws_alloc(2 * (size_t)tiles, R))) return false;
     ws->band_tiles = tiles;
   }
+  // a grid-stride pass: four 256-thread blocks per SM of a B200 (148 SMs)
   k_band_sync<<<4 * 148, 256, 0, st>>>((const float*)phi, ws->band64[0], ws->gb.count());
   ++launch_counter();
   return cuda_ok(cudaGetLastError(), R);
