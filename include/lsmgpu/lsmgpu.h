@@ -571,16 +571,16 @@ int lsmgpu_workspace_set_fp64_policy(lsmgpu_workspace *ws, int policy);
  * effect elsewhere): the workspace keeps FP64 copies of phi and of its stage
  * buffers.  Before each step the stage tiles (32 x 8 x 16 cells) that hold a
  * cell with |phi| < cells * min(dx) are flagged, with their 26 neighbours
- * when widen is 1;
- * each stage computes the flagged tiles in FP64 from the FP64 copies (on a
- * second, high-priority stream, beside the FP32 launch) and the others in
- * FP32, and writes every cell in both precisions, so phi stays the
- * FP32 array the caller owns (the FP64 results rounded to nearest there).
- * dt is that of the FP64 velocity.  The copy of phi persists between calls:
- * a cell whose copy no longer rounds to the caller's value (first call, or
- * phi changed by the caller) is reloaded from phi.  Default 16 cells; a large
- * value puts every tile in FP64 (the result is then the FP64 run's, rounded
- * to FP32).  Ghost boxes of 2^31 cells or more, and axes of fewer than 3
+ * when widen is 1 (without them the band's error is that of plain FP32: a
+ * flagged tile's halo lies in FP32 tiles).  Each stage computes the flagged
+ * tiles in FP64 from the FP64 copies (on a second, high-priority stream,
+ * beside the FP32 launch) and the others in FP32, and writes every cell in
+ * both precisions, so phi stays the FP32 array the caller owns (the FP64
+ * results rounded to nearest there).  dt is that of the FP64 velocity.  The
+ * copy of phi persists between calls: a cell whose copy no longer rounds to
+ * the caller's value (first call, or phi changed by the caller) is reloaded
+ * from phi.  Defaults: 16 cells, widen 1; a large cells value puts every
+ * tile in FP64 (the result is then the FP64 run's, rounded to FP32).  Ghost boxes of 2^31 cells or more, and axes of fewer than 3
  * cells with a boundary kind, run the plain FP32 form.  No reference
  * counterpart. */
 int lsmgpu_workspace_set_fp64_band(lsmgpu_workspace *ws, double cells, int widen);
